@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""NTT throughput on B200: the 24-limb RNS negacyclic batch.
+
+Workload (one step): 24 distinct 31-bit primes q == 1 mod 2^17, N = 2^16 per
+limb, uint32 residues uniform in [0, q); a negacyclic forward NTT over the
+whole batch followed by the inverse, through the C ABI (nttb_rns_transform).
+`value` counts coefficient-transforms per second over all ranks
+(2 transforms x 24 limbs x 2^16 coefficients per step and GPU).
+
+Inputs rotate through a pool of batches larger than twice the 126 MB L2, so
+no step finds its input in L2.  Multi-GPU runs are independent replicas
+(the path shards by limb and polynomial with no exchange); the timing is the
+max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--engine auto|int8|dmma|scalar]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ntt-tensorcore_b200"))
+sys.path.insert(0, ROOT)
+
+LOG_N = 16
+N_LIMBS = 24
+TWO_ADICITY = 17
+L2_BYTES = 126 * 2 ** 20
+METRIC = "NTT coeffs/s + HBM GB/s, INT8-limb vs FP64-DMMA (bit-exact); serve p50/p99"
+UNIT = "coeff-transforms/s"
+WORKLOAD = "rns_negacyclic_24x2^16_fwd+inv"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "int8", "dmma", "scalar"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def moduli():
+    import ntt_b200 as nb
+    return nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
+
+
+def make_batch(qs, seed):
+    rng = np.random.default_rng(seed)
+    x = np.empty((N_LIMBS, 1 << LOG_N), dtype=np.uint32)
+    for l, q in enumerate(qs):
+        x[l] = rng.integers(0, q, 1 << LOG_N, dtype=np.uint64).astype(np.uint32)
+    return x
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sms) if sms else None,
+                "sm_max_mhz": max(maxes) if maxes else None,
+                "samples": len(sms),
+                "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------- reference arm
+def cpu_reference(qs, steps, warmup, threads=0):
+    """The reference's ntt_host (oracle/_ref, compiled from the reference
+    sources) over the same batch on all host threads; one step = the full
+    batch forward + inverse with the driver's psi twist."""
+    from oracle import oracle as O
+    kind = "reference" if O.ref() is not None else "port"
+    x = make_batch(qs, 1).astype(np.uint64)
+    coeffs = 2 * N_LIMBS * (1 << LOG_N)
+
+    def one():
+        y = x.copy()
+        if kind == "reference":
+            used = O.ref_host_batch(y, qs, inverse=False, negacyclic=True, threads=threads)
+            O.ref_host_batch(y, qs, inverse=True, negacyclic=True, threads=threads)
+        else:
+            y = O.rns(y, qs, negacyclic=True)
+            y = O.rns(y, qs, negacyclic=True, inverse=True)
+            used = 1
+        return used, y
+
+    for _ in range(warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        used, y = one()
+    dt = time.perf_counter() - t0
+    assert (y == x).all(), "reference round trip failed"
+    return {"value": coeffs * steps / dt, "unit": UNIT, "cores": used, "kind": kind,
+            "sample": "%d x (24 limbs x 2^16 negacyclic forward+inverse)" % steps, "seconds": dt}
+
+
+def bounded_cpu_baseline(qs, budget_s=10.0):
+    """cpu_baseline: the reference CPU NTT on a bounded sample (~budget_s of wall time)."""
+    probe = cpu_reference(qs, 1, 0)
+    steps = max(1, int(budget_s / max(probe["seconds"], 1e-3)))
+    steps = min(steps, 200)
+    r = cpu_reference(qs, steps, 0)
+    r.pop("seconds")
+    return r
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, world, rank, local):
+    import torch
+    import ntt_b200 as nb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    qs = moduli()
+    plan = nb.RnsPlan(LOG_N, qs, negacyclic=True)
+    batch_bytes = N_LIMBS * (1 << LOG_N) * 4
+    pool_n = max(8, int(np.ceil(2.4 * L2_BYTES / batch_bytes)))
+    host = [make_batch(qs, 1000 + i) for i in range(4)]
+    pool = torch.empty((pool_n, N_LIMBS << LOG_N), dtype=torch.int32, device=dev)
+    for i in range(pool_n):
+        pool[i].copy_(torch.from_numpy(host[i % 4].reshape(-1).view(np.int32)))
+    torch.cuda.synchronize()
+    coeffs_per_step = 2 * N_LIMBS * (1 << LOG_N)
+
+    def step(i, engine):
+        buf = pool[i % pool_n]
+        plan.transform(buf, buf, 1, inverse=False, engine=engine, stream=stream)
+        plan.transform(buf, buf, 1, inverse=True, engine=engine, stream=stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def timed(engine, steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = nb.launch_count()
+        e0.record(stream)
+        for i in range(steps):
+            step(i, engine)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = nb.launch_count() - c0
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        barrier()
+        return ms, launches
+
+    engine = args.engine
+    # warm-up (also brings the clocks up before the sampled region)
+    for i in range(max(3, args.warmup)):
+        step(i, engine)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_end = time.time() + 1.0
+    i = 0
+    while time.time() < t_end:  # ~1 s of load so the sampler sees the clocks under load
+        step(i, engine)
+        i += 1
+        if i % 50 == 0:
+            torch.cuda.synchronize()
+    ms, launches = timed(engine, args.steps)
+    clk = clocks.stop()
+    # round trip leaves every buffer unchanged: check the data is intact
+    for i in range(min(pool_n, 4)):
+        got = pool[i].cpu().numpy().view(np.uint32)
+        assert (got == host[i % 4].reshape(-1)).all(), "round trip mismatch in buffer %d" % i
+    value = world * coeffs_per_step * args.steps / (ms / 1e3)
+
+    # per-kernel device time over the same steps (events around each library launch)
+    nb.profile_start()
+    for i in range(args.steps):
+        step(i, engine)
+    torch.cuda.synchronize()
+    prof = nb.profile_stop()
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    k_name, (k_launches, k_ms) = top
+    k_avg_s = k_ms / k_launches / 1e3
+    coeffs_per_launch = N_LIMBS * (1 << LOG_N)
+    alg_bytes = 8 * coeffs_per_launch  # 4 B read + 4 B write per coefficient per pass
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / k_avg_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(k_name)
+
+    # end to end: pinned host buffers, H2D + forward + inverse + D2H per step
+    h_in = torch.from_numpy(host[0].reshape(-1).view(np.int32)).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    dbuf = torch.empty(N_LIMBS << LOG_N, dtype=torch.int32, device=dev)
+    e_steps = max(3, min(args.steps, 50))
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            dbuf.copy_(h_in, non_blocking=True)
+            plan.transform(dbuf, dbuf, 1, inverse=False, engine=engine, stream=stream)
+            plan.transform(dbuf, dbuf, 1, inverse=True, engine=engine, stream=stream)
+            h_out.copy_(dbuf, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    assert (h_out.numpy().view(np.uint32) == host[0].reshape(-1)).all(), "e2e round trip mismatch"
+    e2e = {"value": world * coeffs_per_step * e_steps / (e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": batch_bytes, "d2h_bytes_per_step": batch_bytes}
+
+    # engine comparison on the same workload (information; the headline is `engine`)
+    compare = {}
+    if not args.no_compare:
+        for eng in ("int8", "dmma", "scalar"):
+            if eng == engine:
+                continue
+            try:
+                step(0, eng)
+                torch.cuda.synchronize()
+            except nb.NTTError:
+                compare[eng] = None
+                continue
+            for i in range(3):
+                step(i, eng)
+            m, _ = timed(eng, max(10, args.steps // 2))
+            compare[eng] = world * coeffs_per_step * max(10, args.steps // 2) / (m / 1e3)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded uniform residues",
+        "config": {"workload": WORKLOAD, "n": 1 << LOG_N, "limbs": N_LIMBS, "moduli": "31-bit, q == 1 mod 2^17",
+                   "negacyclic": True, "engine": engine, "l2": "rotating %d batches (%d MB) > 2x L2"
+                   % (pool_n, pool_n * batch_bytes >> 20), "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "hbm", "kernel": k_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
+                     "kernel_avg_us": k_avg_s * 1e6, "alg_bytes_per_launch": alg_bytes},
+        "kernels": {k: {"launches": v[0], "total_ms": v[1]} for k, v in prof.items()},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        "engines_coeffs_per_s": dict(compare, **{engine: value}),
+    }
+    return result, qs
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        qs = moduli()
+        r = cpu_reference(qs, args.steps, args.warmup)
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u64", "data": "synthetic: seeded uniform residues",
+                "config": {"workload": WORKLOAD, "n": 1 << LOG_N, "limbs": N_LIMBS, "negacyclic": True,
+                           "parallelism": "host threads"},
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    result, qs = run_ours(args, world, rank, local)
+    if rank == 0 and world == 1:
+        result["cpu_baseline"] = bounded_cpu_baseline(qs)
+    if rank == 0:
+        print(json.dumps(result))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * ntt_b200.h -- C ABI of libntt_b200.so, the B200 (sm_100a) four-step NTT.
+ *
+ * Plain C: fixed-width integers, pointers and sizes, no CUDA or torch types.
+ * Device pointers are device-memory addresses; `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  Every entry point returns
+ * an int status (NTTB_OK == 0); nttb_last_error() gives a one-line reason
+ * for the last failure on the calling thread.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the ntt-tensorcore project root).  The C++ drop-in headers in this
+ * directory (ntt.cuh, modular_arith.cuh, ntt_arbitrary.cuh,
+ * ntt_arbitrary_radix64.cuh) are thin wrappers over these symbols.
+ */
+#ifndef NTT_B200_H
+#define NTT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NTTB_API __attribute__((visibility("default")))
+#else
+#define NTTB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    NTTB_OK = 0,
+    NTTB_ERR_INVALID_ARG = 1, /* size, modulus, pointer or alignment rejected */
+    NTTB_ERR_UNSUPPORTED = 2, /* valid request outside what this build serves */
+    NTTB_ERR_CUDA = 3,        /* a CUDA runtime call or kernel launch failed */
+    NTTB_ERR_NO_MEMORY = 4,   /* a device or host allocation failed */
+    NTTB_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out */
+    NTTB_ERR_BUDGET = 6       /* serving admission refused: HBM budget exceeded */
+};
+
+/* Inner-DFT engines.  AUTO picks the fastest one that serves the request. */
+enum {
+    NTTB_ENGINE_AUTO = 0,
+    NTTB_ENGINE_SCALAR = 1, /* CUDA-core radix-2 in shared memory */
+    NTTB_ENGINE_DMMA = 2,   /* FP64 mma.sync m8n8k4 radix-8 contractions (the plain drop-in form) */
+    NTTB_ENGINE_INT8 = 3    /* tcgen05 kind::i8, byte-plane radix-64 contractions, INT32 in TMEM */
+};
+
+NTTB_API const char* nttb_version(void);
+NTTB_API const char* nttb_status_string(int status);
+NTTB_API const char* nttb_last_error(void);
+
+/* ------------------------------------------------ modular parameters (host)
+ * Field-for-field the reference's ModularParams
+ * (include/modular_arith.cuh:11-19). */
+typedef struct {
+    uint64_t q, q_twice, barrett_k, barrett_m, omega, omega_inv, n_inv;
+} nttb_modular_params;
+
+/* Replaces create_params (include/modular_arith.cuh:153-170). */
+NTTB_API int nttb_create_params(uint64_t q, uint64_t n, nttb_modular_params* out);
+/* Replaces find_primitive_root (include/modular_arith.cuh:130-151). */
+NTTB_API int nttb_find_primitive_root(uint64_t q, uint64_t n, uint64_t* omega);
+/* psi = g^((q-1)/(2n)) with the same generator: primitive 2n-th root, psi^2 = omega. */
+NTTB_API int nttb_find_psi(uint64_t q, uint64_t n, uint64_t* psi);
+/* Replaces ntt_host (src/ntt_basic.cu:412-463): CPU NTT, natural order in place. */
+NTTB_API int nttb_host_ntt(uint64_t* data, uint64_t n, const nttb_modular_params* params, int inverse);
+/* Descending primes q < 2^bits with q == 1 mod 2^two_adicity (bits <= 62). */
+NTTB_API int nttb_generate_primes(uint32_t bits, uint32_t two_adicity, uint32_t count, uint64_t* out);
+
+/* ---------------------------------- single-modulus plan over uint64 words
+ * Backs NTTConfig (include/ntt.cuh:11-24).  q < 2^31 runs the 31-bit
+ * engines; 2^31 <= q < 2^62 runs the 64-bit Montgomery path. */
+typedef struct nttb_plan nttb_plan;
+typedef struct {
+    uint64_t n, log_n, q, mu;
+    uint64_t* d_twiddles;     /* omega^k, k < n (the reference's table layout) */
+    uint64_t* d_twiddles_inv; /* omega^-k, k < n */
+    nttb_modular_params params;
+} nttb_plan_info;
+
+/* Replaces ntt_init (src/ntt_basic.cu:217-249). */
+NTTB_API int nttb_plan_create(uint64_t n, uint64_t q, nttb_plan** out);
+/* Replaces ntt_cleanup (src/ntt_basic.cu:251-257). */
+NTTB_API int nttb_plan_destroy(nttb_plan* plan);
+NTTB_API int nttb_plan_get_info(const nttb_plan* plan, nttb_plan_info* out);
+
+/* Natural-order cyclic NTT over `batch` contiguous polynomials of n words,
+ * in place.  Replaces ntt_forward/inverse_{basic,tlmop,optimized}
+ * (src/ntt_basic.cu:268-334, src/ntt_optimized.cu:515-613) and
+ * ntt_forward/inverse_batch (src/ntt_basic.cu:337-389). */
+NTTB_API int nttb_u64_transform(const nttb_plan* plan, uint64_t* d_data, uint64_t batch, int inverse, int engine,
+                       void* stream);
+/* The reference's four-step map, in place.  Replaces
+ * ntt_forward/inverse_four_step (src/ntt_four_step.cu:244-392). */
+NTTB_API int nttb_u64_four_step(const nttb_plan* plan, uint64_t* d_data, int inverse, void* stream);
+/* Pre-transposed forward NTT for n == 4096, plain forward otherwise.
+ * Replaces ntt_forward_rowmaj (src/ntt_optimized.cu:940-965). */
+NTTB_API int nttb_u64_rowmaj_forward(const nttb_plan* plan, uint64_t* d_data, void* stream);
+/* d_dst[c*rows + r] = d_src[r*cols + c].  Replaces rowmaj_to_pretransposed
+ * (rows=N1, cols=N2) and rowmaj_from_pretransposed (rows=N2, cols=N1),
+ * src/ntt_optimized.cu:922-934.  d_dst may equal d_src only for a square matrix. */
+NTTB_API int nttb_u64_transpose(uint64_t* d_dst, const uint64_t* d_src, uint64_t rows, uint64_t cols, void* stream);
+/* d_out[i] = d_a[i] * d_b[i] mod q, i < n.  Replaces poly_multiply_ntt
+ * (src/ntt_basic.cu:391-409). */
+NTTB_API int nttb_u64_pointwise_mul(const nttb_plan* plan, uint64_t* d_out, const uint64_t* d_a, const uint64_t* d_b,
+                           void* stream);
+/* In-place bit-reversal permutation.  Replaces bit_reverse_permute
+ * (src/ntt_basic.cu:259-265). */
+NTTB_API int nttb_u64_bit_reverse(uint64_t* d_data, uint64_t n, void* stream);
+
+/* ------------------------------------------ RNS batches of uint32 residues
+ * No single reference counterpart: the reference batches only one modulus by
+ * a host loop (ntt_forward_batch, src/ntt_basic.cu:337-389).  Data layout is
+ * [poly][limb][n] uint32, limb l reduced mod moduli[l] (q < 2^31). */
+typedef struct nttb_rns_plan nttb_rns_plan;
+#define NTTB_NEGACYCLIC 1u
+
+NTTB_API int nttb_rns_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, uint32_t flags,
+                         nttb_rns_plan** out);
+NTTB_API int nttb_rns_plan_destroy(nttb_rns_plan* plan);
+/* d_dst = NTT(d_src) (forward) or NTT^-1 (inverse); d_dst may equal d_src.
+ * Negacyclic plans twist by psi^j before the forward and by n^-1 psi^-j
+ * after the inverse. */
+NTTB_API int nttb_rns_transform(const nttb_rns_plan* plan, uint32_t* d_dst, const uint32_t* d_src, uint32_t n_polys,
+                       int inverse, int engine, void* stream);
+/* d_out = d_a * d_b pointwise per limb (NTT domain). */
+NTTB_API int nttb_rns_pointwise_mul(const nttb_rns_plan* plan, uint32_t* d_out, const uint32_t* d_a,
+                           const uint32_t* d_b, uint32_t n_polys, void* stream);
+
+/* ------------------------------------------- 64-bit moduli (q < 2^62)
+ * The multi-limb big-prime path: residues stored as uint64 (two 32-bit
+ * words).  Replaces the K-limb run_forward_ct_tcu path for primes near 2^60
+ * (include/ntt_arbitrary.cuh:2599-2646) and adds the inverse it lacks. */
+typedef struct nttb_wide_plan nttb_wide_plan;
+NTTB_API int nttb_wide_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, uint32_t flags,
+                          nttb_wide_plan** out);
+NTTB_API int nttb_wide_plan_destroy(nttb_wide_plan* plan);
+NTTB_API int nttb_wide_transform(const nttb_wide_plan* plan, uint64_t* d_dst, const uint64_t* d_src, uint32_t n_polys,
+                        int inverse, void* stream);
+
+/* ------------------------------------------------------------ accounting
+ * No reference counterpart (the reference times with ad-hoc cudaEvents,
+ * tests/benchmark.cu:52-99).  nttb_launch_count counts every kernel launch
+ * the library has issued.  Between nttb_profile_start and nttb_profile_stop
+ * the library brackets each of its launches with CUDA events on the
+ * launching stream; nttb_profile_stop synchronizes those events and
+ * aggregates device time per kernel name, read back by index. */
+NTTB_API int nttb_launch_count(uint64_t* out);
+NTTB_API int nttb_profile_start(void);
+NTTB_API int nttb_profile_stop(uint32_t* n_kernels);
+NTTB_API int nttb_profile_read(uint32_t index, char* name, uint32_t name_len, uint64_t* launches,
+                               double* total_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NTT_B200_H */

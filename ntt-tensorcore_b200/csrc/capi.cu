@@ -1,0 +1,464 @@
+// capi.cu -- the extern "C" boundary of libntt_b200.so (declared in
+// include/ntt_b200.h).  Host-side validation, plan ownership and dispatch to
+// the engines; no arithmetic lives here beyond the small elementwise kernels.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ntt_b200.h"
+#include "engines.hpp"
+#include "plan.hpp"
+#include "profiler.hpp"
+
+namespace nttb {
+
+static thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+int cuda_status(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(NTTB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return NTTB_OK;
+}
+
+uint64_t reference_generator(uint64_t q);
+
+// ---- small elementwise kernels ---------------------------------------------
+__global__ void transpose_u64_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t rows,
+                                     uint64_t cols) {
+    __shared__ uint64_t tile[32][33];
+    const uint64_t c0 = (uint64_t)blockIdx.x * 32, r0 = (uint64_t)blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        uint64_t r = r0 + i, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[i][threadIdx.x] = src[r * cols + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        uint64_t c = c0 + i, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) dst[c * rows + r] = tile[threadIdx.x][i];
+    }
+}
+
+// In-place transpose of a square matrix: each (r, c) with r < c swaps once.
+__global__ void transpose_square_inplace_kernel(uint64_t* data, uint64_t n) {
+    const uint64_t total = n * n;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = i / n, c = i % n;
+        if (r < c) {
+            uint64_t t = data[r * n + c];
+            data[r * n + c] = data[c * n + r];
+            data[c * n + r] = t;
+        }
+    }
+}
+
+__global__ void bitrev_u64_kernel(uint64_t* data, uint64_t n, int log_n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t r = log_n ? (__brevll(i) >> (64 - log_n)) : 0;
+        if (i < r) {
+            uint64_t t = data[i];
+            data[i] = data[r];
+            data[r] = t;
+        }
+    }
+}
+
+// out = a * b mod q with one Montgomery product and one correction by R^2.
+__global__ void pointwise_u64_kernel(uint64_t* out, const uint64_t* a, const uint64_t* b, uint64_t n, M64 ar,
+                                     uint64_t r2) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = ar.mul(ar.mul(a[i], b[i]), r2);
+}
+
+__global__ void pointwise_rns_kernel(uint32_t* out, const uint32_t* a, const uint32_t* b, uint32_t log_n,
+                                     uint32_t n_limbs, uint64_t total, const LimbDev<M32>* limbs,
+                                     const uint32_t* r2s) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t limb = (uint32_t)((i >> log_n) % n_limbs);
+        const M32 ar = limbs[limb].ar;
+        out[i] = ar.mul(ar.mul(a[i], b[i]), r2s[limb]);
+    }
+}
+
+static unsigned grid_for(uint64_t n) {
+    uint64_t g = (n + 255) / 256;
+    return (unsigned)(g > 148 * 32 ? 148 * 32 : (g ? g : 1));
+}
+
+}  // namespace nttb
+
+using namespace nttb;
+
+// ---- opaque handle types ------------------------------------------------------
+struct nttb_plan {
+    uint64_t n = 0, log_n = 0, q = 0, mu = 0;
+    nttb_modular_params params{};
+    uint64_t* d_twiddles = nullptr;
+    uint64_t* d_twiddles_inv = nullptr;
+    uint64_t* d_scratch = nullptr;  // n words: four-step / rowmaj staging
+    bool wide = false;              // q >= 2^31
+    Plan32 p32;
+    Plan64 p64;
+    M64 ar64{};
+    uint64_t r2_64 = 0;
+};
+
+struct nttb_rns_plan {
+    Plan32 p;
+    uint32_t* d_r2 = nullptr;  // R^2 mod q per limb (pointwise products)
+};
+
+struct nttb_wide_plan {
+    Plan64 p;
+};
+
+extern "C" {
+
+const char* nttb_version(void) { return "ntt_b200 0.1 (sm_100a)"; }
+
+const char* nttb_status_string(int s) {
+    switch (s) {
+        case NTTB_OK: return "ok";
+        case NTTB_ERR_INVALID_ARG: return "invalid argument";
+        case NTTB_ERR_UNSUPPORTED: return "unsupported";
+        case NTTB_ERR_CUDA: return "CUDA error";
+        case NTTB_ERR_NO_MEMORY: return "out of memory";
+        case NTTB_ERR_TIMEOUT: return "device wait timed out";
+        case NTTB_ERR_BUDGET: return "HBM budget exceeded";
+        default: return "unknown status";
+    }
+}
+
+const char* nttb_last_error(void) { return g_last_error.c_str(); }
+
+static bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
+static uint32_t ilog2(uint64_t n) { uint32_t l = 0; while ((1ull << l) < n) l++; return l; }
+
+int nttb_create_params(uint64_t q, uint64_t n, nttb_modular_params* out) {
+    if (!out || q < 3 || !pow2(n)) return fail(NTTB_ERR_INVALID_ARG, "create_params: bad q or n");
+    // barrett_k / barrett_m exactly as include/modular_arith.cuh:158-162 stores them
+    int k = 64;
+    while ((1ULL << (k - 64)) < q && k < 96) k++;
+    out->q = q;
+    out->q_twice = 2 * q;
+    out->barrett_k = (uint64_t)k;
+    out->barrett_m = (uint64_t)(((unsigned __int128)1 << k) / q);
+    uint64_t g = reference_generator(q);
+    out->omega = h_powmod(g, (q - 1) / n, q);
+    out->omega_inv = h_invmod(out->omega, q);
+    out->n_inv = h_invmod(n % q, q);
+    return NTTB_OK;
+}
+
+int nttb_find_primitive_root(uint64_t q, uint64_t n, uint64_t* omega) {
+    if (!omega || q < 3 || !pow2(n)) return fail(NTTB_ERR_INVALID_ARG, "find_primitive_root: bad q or n");
+    *omega = h_powmod(reference_generator(q), (q - 1) / n, q);
+    return NTTB_OK;
+}
+
+int nttb_find_psi(uint64_t q, uint64_t n, uint64_t* psi) {
+    if (!psi || q < 3 || !pow2(n) || (q - 1) % (2 * n)) return fail(NTTB_ERR_INVALID_ARG, "find_psi: 2n must divide q-1");
+    *psi = h_powmod(reference_generator(q), (q - 1) / (2 * n), q);
+    return NTTB_OK;
+}
+
+// CPU NTT (natural order): iterative decimation-in-frequency into a
+// bit-reversed temporary, then an unscrambling copy; n^-1 applied for the
+// inverse.  Exact with unsigned __int128 for q < 2^63.
+int nttb_host_ntt(uint64_t* data, uint64_t n, const nttb_modular_params* p, int inverse) {
+    if (!data || !p || !pow2(n) || p->q >= (1ull << 63)) return fail(NTTB_ERR_INVALID_ARG, "host_ntt: bad arguments");
+    const uint64_t q = p->q;
+    const uint64_t root = inverse ? p->omega_inv : p->omega;
+    const int lg = (int)ilog2(n);
+    std::vector<uint64_t> w(n / 2 + 1);
+    w[0] = 1;
+    for (uint64_t i = 1; i < n / 2; i++) w[i] = h_mulmod(w[i - 1], root, q);
+    for (uint64_t half = n / 2; half >= 1; half >>= 1) {
+        const uint64_t step = n / (2 * half);
+        for (uint64_t g = 0; g < n; g += 2 * half)
+            for (uint64_t j = 0; j < half; j++) {
+                uint64_t u = data[g + j], v = data[g + j + half];
+                uint64_t s = u + v;
+                if (s >= q || s < u) s -= q;
+                uint64_t d = u >= v ? u - v : u + (q - v);
+                data[g + j] = s;
+                data[g + j + half] = h_mulmod(d, w[j * step], q);
+            }
+        if (half == 1) break;
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t r = 0;
+        for (int b = 0; b < lg; b++) r |= ((i >> b) & 1ull) << (lg - 1 - b);
+        if (i < r) std::swap(data[i], data[r]);
+    }
+    if (inverse)
+        for (uint64_t i = 0; i < n; i++) data[i] = h_mulmod(data[i], p->n_inv, q);
+    return NTTB_OK;
+}
+
+static bool is_prime_u64(uint64_t q) {
+    LimbHost L;
+    std::string why;
+    return q > 2 && (q & 1) && make_limb_host(q, 1, false, &L, &why);
+}
+
+int nttb_generate_primes(uint32_t bits, uint32_t two_adicity, uint32_t count, uint64_t* out) {
+    if (!out || bits < 3 || bits > 62 || two_adicity >= bits) return fail(NTTB_ERR_INVALID_ARG, "generate_primes: bad args");
+    const uint64_t step = 1ull << two_adicity;
+    uint64_t k = ((1ull << bits) - 1) / step;
+    uint32_t found = 0;
+    for (; k > 0 && found < count; k--) {
+        uint64_t q = k * step + 1;
+        if (q >= (1ull << bits)) continue;
+        if (is_prime_u64(q)) out[found++] = q;
+    }
+    if (found < count) return fail(NTTB_ERR_INVALID_ARG, "generate_primes: only %u primes exist", found);
+    return NTTB_OK;
+}
+
+// ---------------------------------------------------------- single-modulus plan
+int nttb_plan_create(uint64_t n, uint64_t q, nttb_plan** out) {
+    if (!out) return fail(NTTB_ERR_INVALID_ARG, "plan_create: null out");
+    *out = nullptr;
+    if (!pow2(n) || n < 2 || n > (1ull << 26)) return fail(NTTB_ERR_INVALID_ARG, "plan_create: n must be a power of two in [2, 2^26]");
+    if (q >= (1ull << 62)) return fail(NTTB_ERR_UNSUPPORTED, "plan_create: q must be < 2^62");
+    auto* P = new nttb_plan();
+    P->n = n;
+    P->log_n = ilog2(n);
+    P->q = q;
+    P->mu = (uint64_t)(((unsigned __int128)1 << 64) / q);
+    std::string why;
+    int rc;
+    uint64_t qs[1] = {q};
+    if (q < (1ull << 31)) {
+        rc = build_plan32(&P->p32, (uint32_t)P->log_n, qs, 1, false, &why);
+    } else {
+        P->wide = true;
+        rc = build_plan64(&P->p64, (uint32_t)P->log_n, qs, 1, false, &why);
+    }
+    if (rc) {
+        free_plan32(&P->p32);
+        free_plan64(&P->p64);
+        delete P;
+        return fail(rc == 4 ? NTTB_ERR_NO_MEMORY : NTTB_ERR_INVALID_ARG, "plan_create: %s", why.c_str());
+    }
+    nttb_create_params(q, n, &P->params);
+    // the reference's twiddle tables: omega^k and omega^-k as uint64 words
+    std::vector<uint64_t> tw(n), twi(n);
+    tw[0] = twi[0] = 1;
+    for (uint64_t i = 1; i < n; i++) {
+        tw[i] = h_mulmod(tw[i - 1], P->params.omega, q);
+        twi[i] = h_mulmod(twi[i - 1], P->params.omega_inv, q);
+    }
+    if (cudaMalloc(&P->d_twiddles, n * 8) != cudaSuccess || cudaMalloc(&P->d_twiddles_inv, n * 8) != cudaSuccess ||
+        cudaMalloc(&P->d_scratch, n * 8) != cudaSuccess) {
+        nttb_plan_destroy(P);
+        return fail(NTTB_ERR_NO_MEMORY, "plan_create: cudaMalloc failed");
+    }
+    cudaMemcpy(P->d_twiddles, tw.data(), n * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(P->d_twiddles_inv, twi.data(), n * 8, cudaMemcpyHostToDevice);
+    P->ar64.q = q;
+    P->ar64.qinv = h_neg_inv64(q);
+    P->r2_64 = h_to_mont64(h_to_mont64(1, q), q);
+    *out = P;
+    return cuda_status("plan_create");
+}
+
+int nttb_plan_destroy(nttb_plan* P) {
+    if (!P) return NTTB_OK;
+    engines_release32(&P->p32);
+    free_plan32(&P->p32);
+    free_plan64(&P->p64);
+    if (P->d_twiddles) cudaFree(P->d_twiddles);
+    if (P->d_twiddles_inv) cudaFree(P->d_twiddles_inv);
+    if (P->d_scratch) cudaFree(P->d_scratch);
+    delete P;
+    return NTTB_OK;
+}
+
+int nttb_plan_get_info(const nttb_plan* P, nttb_plan_info* out) {
+    if (!P || !out) return fail(NTTB_ERR_INVALID_ARG, "plan_get_info: null argument");
+    out->n = P->n;
+    out->log_n = P->log_n;
+    out->q = P->q;
+    out->mu = P->mu;
+    out->d_twiddles = P->d_twiddles;
+    out->d_twiddles_inv = P->d_twiddles_inv;
+    out->params = P->params;
+    return NTTB_OK;
+}
+
+int nttb_u64_transform(const nttb_plan* P, uint64_t* d, uint64_t batch, int inverse, int engine, void* stream) {
+    if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "u64_transform: null argument");
+    if (batch == 0) return NTTB_OK;
+    if (batch > 65535) return fail(NTTB_ERR_UNSUPPORTED, "u64_transform: batch > 65535");
+    if (((uintptr_t)d) & 7) return fail(NTTB_ERR_INVALID_ARG, "u64_transform: misaligned pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc;
+    if (P->wide) {
+        rc = scalar_transform64(P->p64, d, d, (uint32_t)batch, inverse != 0, s);
+    } else {
+        rc = run_transform32(const_cast<Plan32&>(P->p32), d, d, true, (uint32_t)batch, inverse != 0, engine, s);
+    }
+    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "u64_transform: size not served");
+    if (rc) return cuda_status("u64_transform");
+    return cuda_status("u64_transform");
+}
+
+int nttb_u64_four_step(const nttb_plan* P, uint64_t* d, int inverse, void* stream) {
+    if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "four_step: null argument");
+    if (P->wide) return fail(NTTB_ERR_UNSUPPORTED, "four_step: q must be < 2^31");
+    int rc = scalar_four_step32(P->p32, d, P->d_scratch, inverse != 0, (cudaStream_t)stream);
+    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "four_step: size not served");
+    return cuda_status("four_step");
+}
+
+int nttb_u64_transpose(uint64_t* dst, const uint64_t* src, uint64_t rows, uint64_t cols, void* stream) {
+    if (!dst || !src || rows == 0 || cols == 0) return fail(NTTB_ERR_INVALID_ARG, "transpose: bad arguments");
+    if (dst == src) {
+        // The reference's helpers are called in place on square matrices
+        // (tests/debug_rowmaj.cu:122-124); serve that race-free.
+        if (rows != cols) return fail(NTTB_ERR_INVALID_ARG, "transpose: in place only for square matrices");
+        ProfScope prof("transpose_square_inplace", (cudaStream_t)stream);
+        transpose_square_inplace_kernel<<<grid_for(rows * cols), 256, 0, (cudaStream_t)stream>>>(dst, rows);
+        return cuda_status("transpose");
+    }
+    dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+    if (grid.y > 65535) return fail(NTTB_ERR_UNSUPPORTED, "transpose: too many rows");
+    ProfScope prof("transpose_u64", (cudaStream_t)stream);
+    transpose_u64_kernel<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(dst, src, rows, cols);
+    return cuda_status("transpose");
+}
+
+int nttb_u64_rowmaj_forward(const nttb_plan* P, uint64_t* d, void* stream) {
+    if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "rowmaj_forward: null argument");
+    if (P->n != 4096) return nttb_u64_transform(P, d, 1, 0, NTTB_ENGINE_AUTO, stream);
+    // pre-transposed (64 x 64) in -> canonical -> forward -> pre-transposed out
+    int rc = nttb_u64_transpose(P->d_scratch, d, 64, 64, stream);
+    if (rc) return rc;
+    rc = nttb_u64_transform(P, P->d_scratch, 1, 0, NTTB_ENGINE_AUTO, stream);
+    if (rc) return rc;
+    return nttb_u64_transpose(d, P->d_scratch, 64, 64, stream);
+}
+
+int nttb_u64_pointwise_mul(const nttb_plan* P, uint64_t* out, const uint64_t* a, const uint64_t* b, void* stream) {
+    if (!P || !out || !a || !b) return fail(NTTB_ERR_INVALID_ARG, "pointwise_mul: null argument");
+    ProfScope prof("pointwise_u64", (cudaStream_t)stream);
+    pointwise_u64_kernel<<<grid_for(P->n), 256, 0, (cudaStream_t)stream>>>(out, a, b, P->n, P->ar64, P->r2_64);
+    return cuda_status("pointwise_mul");
+}
+
+int nttb_u64_bit_reverse(uint64_t* d, uint64_t n, void* stream) {
+    if (!d || !pow2(n)) return fail(NTTB_ERR_INVALID_ARG, "bit_reverse: n must be a power of two");
+    ProfScope prof("bitrev_u64", (cudaStream_t)stream);
+    bitrev_u64_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d, n, (int)ilog2(n));
+    return cuda_status("bit_reverse");
+}
+
+// ------------------------------------------------------------------ RNS plans
+int nttb_rns_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, uint32_t flags,
+                         nttb_rns_plan** out) {
+    if (!out || !moduli || n_limbs == 0) return fail(NTTB_ERR_INVALID_ARG, "rns_plan_create: bad arguments");
+    *out = nullptr;
+    if (log_n < 1 || log_n > 24) return fail(NTTB_ERR_UNSUPPORTED, "rns_plan_create: log_n must be in [1, 24]");
+    auto* P = new nttb_rns_plan();
+    std::string why;
+    int rc = build_plan32(&P->p, log_n, moduli, n_limbs, (flags & NTTB_NEGACYCLIC) != 0, &why);
+    if (rc) {
+        free_plan32(&P->p);
+        delete P;
+        return fail(rc == 4 ? NTTB_ERR_NO_MEMORY : NTTB_ERR_INVALID_ARG, "rns_plan_create: %s", why.c_str());
+    }
+    std::vector<uint32_t> r2(n_limbs);
+    for (uint32_t l = 0; l < n_limbs; l++) r2[l] = h_to_mont32(h_to_mont32(1, moduli[l]), moduli[l]);
+    if (cudaMalloc(&P->d_r2, n_limbs * 4) != cudaSuccess) {
+        nttb_rns_plan_destroy(P);
+        return fail(NTTB_ERR_NO_MEMORY, "rns_plan_create: cudaMalloc failed");
+    }
+    cudaMemcpy(P->d_r2, r2.data(), n_limbs * 4, cudaMemcpyHostToDevice);
+    *out = P;
+    return cuda_status("rns_plan_create");
+}
+
+int nttb_rns_plan_destroy(nttb_rns_plan* P) {
+    if (!P) return NTTB_OK;
+    engines_release32(&P->p);
+    free_plan32(&P->p);
+    if (P->d_r2) cudaFree(P->d_r2);
+    delete P;
+    return NTTB_OK;
+}
+
+int nttb_rns_transform(const nttb_rns_plan* P, uint32_t* dst, const uint32_t* src, uint32_t n_polys, int inverse,
+                       int engine, void* stream) {
+    if (!P || !dst || !src) return fail(NTTB_ERR_INVALID_ARG, "rns_transform: null argument");
+    if (n_polys == 0) return NTTB_OK;
+    if ((((uintptr_t)dst) | ((uintptr_t)src)) & 15) return fail(NTTB_ERR_INVALID_ARG, "rns_transform: pointers must be 16-byte aligned");
+    int rc = run_transform32(const_cast<Plan32&>(P->p), src, dst, false, n_polys, inverse != 0, engine,
+                             (cudaStream_t)stream);
+    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_transform: shape not served by the requested engine");
+    return cuda_status("rns_transform");
+}
+
+int nttb_rns_pointwise_mul(const nttb_rns_plan* P, uint32_t* out, const uint32_t* a, const uint32_t* b,
+                           uint32_t n_polys, void* stream) {
+    if (!P || !out || !a || !b) return fail(NTTB_ERR_INVALID_ARG, "rns_pointwise_mul: null argument");
+    uint64_t total = (uint64_t)n_polys * P->p.n_limbs * P->p.n;
+    ProfScope prof("pointwise_rns", (cudaStream_t)stream);
+    pointwise_rns_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(out, a, b, P->p.log_n, P->p.n_limbs,
+                                                                            total, P->p.d_limbs, P->d_r2);
+    return cuda_status("rns_pointwise_mul");
+}
+
+// ---------------------------------------------------------------- wide plans
+int nttb_wide_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, uint32_t flags,
+                          nttb_wide_plan** out) {
+    if (!out || !moduli || n_limbs == 0) return fail(NTTB_ERR_INVALID_ARG, "wide_plan_create: bad arguments");
+    *out = nullptr;
+    if (log_n < 1 || log_n > 24) return fail(NTTB_ERR_UNSUPPORTED, "wide_plan_create: log_n must be in [1, 24]");
+    auto* P = new nttb_wide_plan();
+    std::string why;
+    int rc = build_plan64(&P->p, log_n, moduli, n_limbs, (flags & NTTB_NEGACYCLIC) != 0, &why);
+    if (rc) {
+        free_plan64(&P->p);
+        delete P;
+        return fail(rc == 4 ? NTTB_ERR_NO_MEMORY : NTTB_ERR_INVALID_ARG, "wide_plan_create: %s", why.c_str());
+    }
+    *out = P;
+    return cuda_status("wide_plan_create");
+}
+
+int nttb_wide_plan_destroy(nttb_wide_plan* P) {
+    if (!P) return NTTB_OK;
+    free_plan64(&P->p);
+    delete P;
+    return NTTB_OK;
+}
+
+int nttb_wide_transform(const nttb_wide_plan* P, uint64_t* dst, const uint64_t* src, uint32_t n_polys, int inverse,
+                        void* stream) {
+    if (!P || !dst || !src) return fail(NTTB_ERR_INVALID_ARG, "wide_transform: null argument");
+    if (n_polys == 0) return NTTB_OK;
+    int rc = scalar_transform64(P->p, src, dst, n_polys, inverse != 0, (cudaStream_t)stream);
+    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "wide_transform: shape not served");
+    return cuda_status("wide_transform");
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// engines.cu -- engine selection for 31-bit plans.
+#include <cstdlib>
+#include <cstring>
+
+#include "../../include/ntt_b200.h"
+#include "engines.hpp"
+
+namespace nttb {
+
+static int env_engine() {
+    const char* e = std::getenv("NTT_B200_ENGINE");
+    if (!e) return NTTB_ENGINE_AUTO;
+    if (!std::strcmp(e, "scalar")) return NTTB_ENGINE_SCALAR;
+    if (!std::strcmp(e, "dmma")) return NTTB_ENGINE_DMMA;
+    if (!std::strcmp(e, "int8")) return NTTB_ENGINE_INT8;
+    return NTTB_ENGINE_AUTO;
+}
+
+int auto_engine32(const Plan32& p, bool src_u64) {
+    (void)p;
+    (void)src_u64;
+    return NTTB_ENGINE_SCALAR;
+}
+
+int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
+                    int engine, cudaStream_t s) {
+    if (engine == NTTB_ENGINE_AUTO) engine = env_engine();
+    if (engine == NTTB_ENGINE_AUTO) engine = auto_engine32(p, src_u64);
+    switch (engine) {
+        case NTTB_ENGINE_SCALAR:
+            return scalar_transform32(p, src, dst, src_u64, n_polys, inverse, s);
+        default:
+            return 1;
+    }
+}
+
+void engines_release32(Plan32* p) {
+    for (void*& d : p->engine_data) {
+        if (d) cudaFree(d);
+        d = nullptr;
+    }
+}
+
+}  // namespace nttb

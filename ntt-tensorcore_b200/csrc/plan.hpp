@@ -1,0 +1,98 @@
+// plan.hpp -- host-side plan structures shared by the engines and the C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "arith.cuh"
+
+namespace nttb {
+
+// Per-limb constants handed to the kernels (one array entry per limb).
+template <class A>
+struct LimbDev {
+    A ar;                              // modulus + Montgomery constant
+    typename A::elem ninv_m;           // n^-1 * R mod q
+    typename A::elem pad_;
+    const typename A::elem* tw;        // omega^e * R,   e < n
+    const typename A::elem* tw_inv;    // omega^-e * R,  e < n
+    const typename A::elem* psi;       // psi^e * R,     e < n (negacyclic only)
+    const typename A::elem* psi_inv;   // n^-1 psi^-e R, e < n (negacyclic only)
+};
+
+// Host view of one modulus at one transform size.
+struct LimbHost {
+    uint64_t q = 0, g = 0, omega = 0, omega_inv = 0, psi = 0, psi_inv = 0, n_inv = 0;
+};
+
+// Fills LimbHost with the generator rule of the reference
+// (include/modular_arith.cuh:130-151) plus psi = g^((q-1)/2n).
+bool make_limb_host(uint64_t q, uint64_t n, bool need_psi, LimbHost* out, std::string* why);
+
+// Transform direction / twist flags.
+enum : uint32_t {
+    F_PRE_PSI = 1u,       // multiply input element n by psi^n           (negacyclic forward)
+    F_PRE_TW = 2u,        // multiply input (row a, col b) by root^(a*b)  (four-step inverse)
+    F_POST_TW = 4u,       // multiply output (row d, col b) by root^(d*b) (four-step pass 1)
+    F_POST_SCALE = 8u,    // multiply output by n^-1                      (cyclic inverse)
+    F_POST_PSI_INV = 16u, // multiply output element n by n^-1 psi^-n    (negacyclic inverse)
+};
+
+// Pass geometries of the scalar engine.
+enum PassMode : int {
+    MODE_COL = 0,          // vectors = columns of [N1 x N2]; out in place (row k, col b)
+    MODE_ROW_NAT = 1,      // vectors = rows d; out X[d + N1*k] (natural order)
+    MODE_GATHER_T = 2,     // vectors = chunks of the N1 x N2 -> N2 x N1 transpose; out in place
+    MODE_ROW_SCATTER_T = 3 // vectors = contiguous chunks; out through the transpose back
+};
+
+struct PassArgs {
+    const void* src;
+    void* dst;
+    uint64_t poly_stride;  // elements between consecutive polynomials
+    uint32_t n, log_n;
+    uint32_t n1, n2;       // matrix view of one transform
+    uint32_t len, log_len; // DFT length of this pass
+    uint32_t vec_per_tile;
+    uint32_t n_limbs;
+    uint32_t flags;
+    int inverse;
+};
+
+// A u32-residue plan (q < 2^31 for every limb).
+struct Plan32 {
+    uint32_t log_n = 0, n = 0, n_limbs = 0;
+    bool negacyclic = false;
+    std::vector<LimbHost> limbs;
+    LimbDev<M32>* d_limbs = nullptr;  // device array, n_limbs entries
+    std::vector<void*> allocations;   // device memory owned by the plan
+    void* engine_data[4] = {nullptr, nullptr, nullptr, nullptr};  // per-engine caches
+};
+
+// A u64-residue plan (q < 2^62).
+struct Plan64 {
+    uint32_t log_n = 0, n = 0, n_limbs = 0;
+    bool negacyclic = false;
+    std::vector<LimbHost> limbs;
+    LimbDev<M64>* d_limbs = nullptr;
+    std::vector<void*> allocations;
+};
+
+int build_plan32(Plan32* p, uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, bool negacyclic,
+                 std::string* why);
+int build_plan64(Plan64* p, uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, bool negacyclic,
+                 std::string* why);
+void free_plan32(Plan32* p);
+void free_plan64(Plan64* p);
+
+// Scalar engine entry points (scalar_engine.cu).  Storage is u32 or u64
+// words; data layout is [poly][limb][n].
+int scalar_transform32(const Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys,
+                       bool inverse, cudaStream_t s);
+int scalar_transform64(const Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse,
+                       cudaStream_t s);
+int scalar_four_step32(const Plan32& p, uint64_t* data, uint64_t* scratch, bool inverse, cudaStream_t s);
+
+}  // namespace nttb

@@ -1,0 +1,285 @@
+// scalar_engine.cu -- CUDA-core engine: each pass computes a batch of DFTs of
+// length `len` entirely in shared memory (radix-2, DIT after a bit-reversed
+// load or DIF before a bit-reversed store, whichever keeps the shared-memory
+// traffic conflict-free for the pass's global access order), with the
+// four-step twiddles and the negacyclic twists fused into the load/store.
+//
+// It serves every size and modulus width and is the engine of the 60-bit
+// path; the tensor-core engines replace it for the hot 31-bit sizes.
+//
+// Two-pass decomposition for n = N1 * N2 (input index a*N2 + b):
+//   pass A (MODE_COL):     U[d][b] = DFT_N1(x[.][b])[d] * root^(d*b)
+//   pass B (MODE_ROW_NAT): X[d + N1*c] = DFT_N2(U[d][.])[c]
+#include <cuda_runtime.h>
+
+#include "plan.hpp"
+#include "profiler.hpp"
+
+namespace nttb {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <class S, class A, int MODE>
+__global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, const LimbDev<A>* limbs) {
+    using E = typename A::elem;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t L = args.len, V = args.vec_per_tile, lgL = args.log_len;
+    const uint32_t stride = L >= 32 ? L + 1 : L;
+    E* t = reinterpret_cast<E*>(smem_raw);
+    E* tws = t + (size_t)V * stride;
+
+    const uint32_t limb = blockIdx.y, poly = blockIdx.z;
+    const uint32_t v0 = blockIdx.x * V;  // first vector of this tile
+    const LimbDev<A> ld = limbs[limb];
+    const A ar = ld.ar;
+    const uint64_t off = (uint64_t)poly * args.poly_stride + (uint64_t)limb * args.n;
+    const S* src = reinterpret_cast<const S*>(args.src) + off;
+    S* dst = reinterpret_cast<S*>(args.dst) + off;
+    const E* tw = args.inverse ? ld.tw_inv : ld.tw;
+    const uint32_t nmask = args.n - 1, N1 = args.n1, N2 = args.n2;
+    const uint32_t total = V * L;
+    const uint32_t flags = args.flags;
+
+    // powers of the length-L root: tws[k] = root_L^k, k < L/2
+    {
+        const uint32_t step = args.n >> lgL;
+        for (uint32_t k = threadIdx.x; k < (L >> 1); k += blockDim.x) tws[k] = tw[(uint64_t)k * step];
+    }
+
+    constexpr bool kDIT = (MODE == MODE_COL || MODE == MODE_GATHER_T);
+
+    // ---- load ----
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        uint32_t v, j;
+        uint64_t pos;
+        if (kDIT) { v = idx % V; j = idx / V; } else { v = idx / L; j = idx % L; }
+        const uint32_t vec = v0 + v;
+        if (MODE == MODE_COL) {
+            pos = (uint64_t)j * N2 + vec;
+        } else if (MODE == MODE_ROW_NAT) {
+            pos = (uint64_t)vec * N2 + j;
+        } else if (MODE == MODE_GATHER_T) {
+            const uint64_t m = (uint64_t)vec * L + j;  // index into the transposed view
+            pos = (m % N1) * N2 + m / N1;
+        } else {
+            pos = (uint64_t)vec * L + j;
+        }
+        E x = (E)src[pos];
+        if (flags & F_PRE_PSI) x = ar.mul(x, ld.psi[pos]);
+        if (flags & F_PRE_TW) x = ar.mul(x, tw[((uint64_t)j * vec) & nmask]);
+        const uint32_t jj = kDIT ? bitrev(j, (int)lgL) : j;
+        t[(size_t)v * stride + jj] = x;
+    }
+    __syncthreads();
+
+    // ---- radix-2 stages ----
+    const uint32_t half_total = total >> 1, Lh = L >> 1;
+    if (kDIT) {
+        for (uint32_t s = 0; s < lgL; s++) {
+            const uint32_t half = 1u << s;
+            for (uint32_t bf = threadIdx.x; bf < half_total; bf += blockDim.x) {
+                const uint32_t v = bf / Lh, j = bf % Lh;
+                const uint32_t p = j & (half - 1);
+                const uint32_t i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+                E* row = t + (size_t)v * stride;
+                const E w = tws[p << (lgL - 1 - s)];
+                const E u = row[i0], y = ar.mul(row[i1], w);
+                row[i0] = ar.add(u, y);
+                row[i1] = ar.sub(u, y);
+            }
+            __syncthreads();
+        }
+    } else {
+        for (int s = (int)lgL - 1; s >= 0; s--) {
+            const uint32_t half = 1u << s;
+            for (uint32_t bf = threadIdx.x; bf < half_total; bf += blockDim.x) {
+                const uint32_t v = bf / Lh, j = bf % Lh;
+                const uint32_t p = j & (half - 1);
+                const uint32_t i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+                E* row = t + (size_t)v * stride;
+                const E w = tws[p << (lgL - 1 - s)];
+                const E u = row[i0], y = row[i1];
+                row[i0] = ar.add(u, y);
+                row[i1] = ar.mul(ar.sub(u, y), w);
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---- store ----
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        uint32_t v, k;
+        if (MODE == MODE_GATHER_T) { v = idx / L; k = idx % L; } else { v = idx % V; k = idx / V; }
+        const uint32_t vec = v0 + v;
+        const uint32_t kk = kDIT ? k : bitrev(k, (int)lgL);
+        E x = t[(size_t)v * stride + kk];
+        uint64_t pos;
+        if (MODE == MODE_COL) {
+            pos = (uint64_t)k * N2 + vec;
+            if (flags & F_POST_TW) x = ar.mul(x, tw[((uint64_t)k * vec) & nmask]);
+        } else if (MODE == MODE_ROW_NAT) {
+            pos = (uint64_t)vec + (uint64_t)N1 * k;
+        } else if (MODE == MODE_GATHER_T) {
+            pos = (uint64_t)vec * L + k;
+        } else {
+            const uint64_t m = (uint64_t)vec * L + k;
+            pos = (m % N1) * N2 + m / N1;  // transpose n2 x n1 -> n1 x n2
+        }
+        if (flags & F_POST_PSI_INV) x = ar.mul(x, ld.psi_inv[pos]);
+        else if (flags & F_POST_SCALE) x = ar.mul(x, ld.ninv_m);
+        dst[pos] = (S)x;
+    }
+}
+
+template <class S, class A>
+int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t n_vectors,
+                uint32_t n_polys, cudaStream_t s) {
+    using E = typename A::elem;
+    const uint32_t stride = a.len >= 32 ? a.len + 1 : a.len;
+    const size_t smem = ((size_t)a.vec_per_tile * stride + (a.len >> 1) + 1) * sizeof(E);
+    dim3 grid(n_vectors / a.vec_per_tile, a.n_limbs, n_polys);
+    if (grid.x == 0 || n_polys > 65535 || a.n_limbs > 65535) return 1;
+    void (*k)(PassArgs, const LimbDev<A>*) = nullptr;
+    switch (mode) {
+        case MODE_COL: k = scalar_pass_kernel<S, A, MODE_COL>; break;
+        case MODE_ROW_NAT: k = scalar_pass_kernel<S, A, MODE_ROW_NAT>; break;
+        case MODE_GATHER_T: k = scalar_pass_kernel<S, A, MODE_GATHER_T>; break;
+        default: k = scalar_pass_kernel<S, A, MODE_ROW_SCATTER_T>; break;
+    }
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static const char* names[4] = {"scalar_pass_col", "scalar_pass_row", "scalar_pass_gather_t",
+                                   "scalar_pass_scatter_t"};
+    ProfScope prof(names[mode & 3], s);
+    k<<<grid, kThreads, smem, s>>>(a, d_limbs);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+inline uint32_t ilog2u(uint64_t x) { uint32_t l = 0; while ((1ull << l) < x) l++; return l; }
+
+// Two-pass (or single-pass) forward/inverse over a plan.  E_max bounds the
+// shared-memory tile in elements.
+template <class S, class A>
+int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const LimbDev<A>* d_limbs,
+                      const void* src, void* dst, uint32_t n_polys, bool inverse, uint32_t e_max,
+                      cudaStream_t s) {
+    const uint32_t n = 1u << log_n;
+    PassArgs a{};
+    a.poly_stride = (uint64_t)n_limbs * n;
+    a.n = n;
+    a.log_n = log_n;
+    a.n_limbs = n_limbs;
+    a.inverse = inverse ? 1 : 0;
+    uint32_t pre = (!inverse && negacyclic) ? F_PRE_PSI : 0u;
+    uint32_t post = inverse ? (negacyclic ? F_POST_PSI_INV : F_POST_SCALE) : 0u;
+    if (n <= e_max) {
+        // single pass: one row of length n per (poly, limb)
+        a.src = src;
+        a.dst = dst;
+        a.n1 = 1;
+        a.n2 = n;
+        a.len = n;
+        a.log_len = log_n;
+        a.vec_per_tile = 1;
+        a.flags = pre | post;
+        return launch_pass<S, A>(MODE_ROW_NAT, a, d_limbs, 1, n_polys, s);
+    }
+    const uint32_t lg1 = (log_n + 1) / 2, lg2 = log_n - lg1;
+    const uint32_t N1 = 1u << lg1, N2 = 1u << lg2;
+    if (N1 > e_max) return 1;
+    // pass A: column DFTs of length N1 + four-step twiddle
+    a.src = src;
+    a.dst = dst;
+    a.n1 = N1;
+    a.n2 = N2;
+    a.len = N1;
+    a.log_len = lg1;
+    a.vec_per_tile = e_max / N1 < N2 ? e_max / N1 : N2;
+    a.flags = pre | F_POST_TW;
+    int rc = launch_pass<S, A>(MODE_COL, a, d_limbs, N2, n_polys, s);
+    if (rc) return rc;
+    // pass B: row DFTs of length N2, natural-order scatter
+    a.src = dst;
+    a.len = N2;
+    a.log_len = lg2;
+    a.vec_per_tile = e_max / N2 < N1 ? e_max / N2 : N1;
+    a.flags = post;
+    return launch_pass<S, A>(MODE_ROW_NAT, a, d_limbs, N1, n_polys, s);
+}
+
+}  // namespace
+
+int scalar_transform32(const Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys,
+                       bool inverse, cudaStream_t s) {
+    if (src_u64)
+        return transform_generic<uint64_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, n_polys,
+                                                inverse, 8192, s);
+    return transform_generic<uint32_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, n_polys,
+                                            inverse, 8192, s);
+}
+
+int scalar_transform64(const Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse,
+                       cudaStream_t s) {
+    return transform_generic<uint64_t, M64>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, n_polys,
+                                            inverse, 4096, s);
+}
+
+// The reference's four-step map (src/ntt_four_step.cu:244-392), race-free:
+//   forward: column DFT-n1 + Hadamard root^(r*c)  [data -> scratch, in place layout]
+//            transpose + chunked DFT-n2           [scratch -> data, one fused pass]
+//   inverse: chunked DFT-n2 + transpose back      [data -> scratch]
+//            Hadamard root^-(r*c) + column DFT-n1 + n^-1 [scratch -> data]
+// with n1 = 2^max(6, log_n/2) capped at n, n2 = n / n1.
+int scalar_four_step32(const Plan32& p, uint64_t* data, uint64_t* scratch, bool inverse, cudaStream_t s) {
+    const uint32_t log_n = p.log_n, n = p.n;
+    uint32_t lg1 = log_n / 2;
+    if (lg1 < 6) lg1 = 6;
+    if (lg1 > log_n) lg1 = log_n;
+    const uint32_t lg2 = log_n - lg1, n1 = 1u << lg1, n2 = 1u << lg2;
+    const uint32_t e_max = 8192;
+    if (n1 > e_max || n2 > e_max) return 1;
+    PassArgs a{};
+    a.poly_stride = n;
+    a.n = n;
+    a.log_n = log_n;
+    a.n_limbs = 1;
+    a.n1 = n1;
+    a.n2 = n2;
+    a.inverse = inverse ? 1 : 0;
+    int rc;
+    if (!inverse) {
+        a.src = data;
+        a.dst = scratch;
+        a.len = n1;
+        a.log_len = lg1;
+        a.vec_per_tile = e_max / n1 < n2 ? e_max / n1 : n2;
+        a.flags = F_POST_TW;
+        rc = launch_pass<uint64_t, M32>(MODE_COL, a, p.d_limbs, n2, 1, s);
+        if (rc) return rc;
+        a.src = scratch;
+        a.dst = data;
+        a.len = n2;
+        a.log_len = lg2;
+        a.vec_per_tile = e_max / n2 < n1 ? e_max / n2 : n1;
+        a.flags = 0;
+        return launch_pass<uint64_t, M32>(MODE_GATHER_T, a, p.d_limbs, n1, 1, s);
+    }
+    a.src = data;
+    a.dst = scratch;
+    a.len = n2;
+    a.log_len = lg2;
+    a.vec_per_tile = e_max / n2 < n1 ? e_max / n2 : n1;
+    a.flags = 0;
+    rc = launch_pass<uint64_t, M32>(MODE_ROW_SCATTER_T, a, p.d_limbs, n1, 1, s);
+    if (rc) return rc;
+    a.src = scratch;
+    a.dst = data;
+    a.len = n1;
+    a.log_len = lg1;
+    a.vec_per_tile = e_max / n1 < n2 ? e_max / n1 : n2;
+    a.flags = F_PRE_TW | F_POST_SCALE;
+    return launch_pass<uint64_t, M32>(MODE_COL, a, p.d_limbs, n2, 1, s);
+}
+
+}  // namespace nttb

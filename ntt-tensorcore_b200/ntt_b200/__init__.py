@@ -1,0 +1,294 @@
+"""Python binding of libntt_b200.so (the C ABI in include/ntt_b200.h).
+
+The library is the product: every call here goes through the C ABI to the
+sm_100a kernels.  There is no CPU fallback -- if the shared library is missing
+or no GPU is present, the calls raise.
+
+Device buffers are passed as torch tensors (their data_ptr) or raw integer
+addresses; torch is used only for device memory and streams.
+"""
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libntt_b200.so")
+HEADER = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "ntt_b200.h")
+
+OK = 0
+ENGINE_AUTO, ENGINE_SCALAR, ENGINE_DMMA, ENGINE_INT8 = 0, 1, 2, 3
+ENGINES = {"auto": ENGINE_AUTO, "scalar": ENGINE_SCALAR, "dmma": ENGINE_DMMA, "int8": ENGINE_INT8}
+NEGACYCLIC = 1
+
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+_vp = ctypes.c_void_p
+_int = ctypes.c_int
+
+
+class NTTError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("ntt_b200 status %d: %s" % (status, msg))
+        self.status = status
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [(n, _u64) for n in ("q", "q_twice", "barrett_k", "barrett_m", "omega", "omega_inv", "n_inv")]
+
+
+class _PlanInfo(ctypes.Structure):
+    _fields_ = [("n", _u64), ("log_n", _u64), ("q", _u64), ("mu", _u64),
+                ("d_twiddles", _vp), ("d_twiddles_inv", _vp), ("params", _Params)]
+
+
+_lib = None
+
+
+def header_symbols():
+    """Function names declared in include/ntt_b200.h."""
+    with open(HEADER) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"NTTB_API\s+(?:const\s+char\s*\*|int)\s+(nttb_\w+)\s*\(", text)))
+
+
+def lib():
+    """Loads libntt_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libntt_b200.so missing: run `python ntt-tensorcore_b200/build.py`")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "nttb_version": (ctypes.c_char_p, []),
+        "nttb_status_string": (ctypes.c_char_p, [_int]),
+        "nttb_last_error": (ctypes.c_char_p, []),
+        "nttb_create_params": (_int, [_u64, _u64, ctypes.POINTER(_Params)]),
+        "nttb_find_primitive_root": (_int, [_u64, _u64, ctypes.POINTER(_u64)]),
+        "nttb_find_psi": (_int, [_u64, _u64, ctypes.POINTER(_u64)]),
+        "nttb_host_ntt": (_int, [_vp, _u64, ctypes.POINTER(_Params), _int]),
+        "nttb_generate_primes": (_int, [_u32, _u32, _u32, _vp]),
+        "nttb_plan_create": (_int, [_u64, _u64, ctypes.POINTER(_vp)]),
+        "nttb_plan_destroy": (_int, [_vp]),
+        "nttb_plan_get_info": (_int, [_vp, ctypes.POINTER(_PlanInfo)]),
+        "nttb_u64_transform": (_int, [_vp, _vp, _u64, _int, _int, _vp]),
+        "nttb_u64_four_step": (_int, [_vp, _vp, _int, _vp]),
+        "nttb_u64_rowmaj_forward": (_int, [_vp, _vp, _vp]),
+        "nttb_u64_transpose": (_int, [_vp, _vp, _u64, _u64, _vp]),
+        "nttb_u64_pointwise_mul": (_int, [_vp, _vp, _vp, _vp, _vp]),
+        "nttb_u64_bit_reverse": (_int, [_vp, _u64, _vp]),
+        "nttb_rns_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
+        "nttb_rns_plan_destroy": (_int, [_vp]),
+        "nttb_rns_transform": (_int, [_vp, _vp, _vp, _u32, _int, _int, _vp]),
+        "nttb_rns_pointwise_mul": (_int, [_vp, _vp, _vp, _vp, _u32, _vp]),
+        "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
+        "nttb_wide_plan_destroy": (_int, [_vp]),
+        "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
+        "nttb_launch_count": (_int, [ctypes.POINTER(_u64)]),
+        "nttb_profile_start": (_int, []),
+        "nttb_profile_stop": (_int, [ctypes.POINTER(_u32)]),
+        "nttb_profile_read": (_int, [_u32, ctypes.c_char_p, _u32, ctypes.POINTER(_u64),
+                                     ctypes.POINTER(ctypes.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(status):
+    if status != OK:
+        msg = lib().nttb_last_error().decode()
+        raise NTTError(status, msg)
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()  # torch tensor
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream  # torch.cuda.Stream
+
+
+def _engine(e):
+    return ENGINES[e] if isinstance(e, str) else int(e)
+
+
+def version():
+    return lib().nttb_version().decode()
+
+
+# ------------------------------------------------------------- accounting
+def launch_count():
+    """Kernel launches issued by the library so far."""
+    c = _u64()
+    _check(lib().nttb_launch_count(ctypes.byref(c)))
+    return int(c.value)
+
+
+def profile_start():
+    _check(lib().nttb_profile_start())
+
+
+def profile_stop():
+    """Stops per-launch event timing; returns {kernel: (launches, total_ms)}."""
+    n = _u32()
+    _check(lib().nttb_profile_stop(ctypes.byref(n)))
+    out = {}
+    buf = ctypes.create_string_buffer(128)
+    for i in range(n.value):
+        la, ms = _u64(), ctypes.c_double()
+        _check(lib().nttb_profile_read(i, buf, 128, ctypes.byref(la), ctypes.byref(ms)))
+        out[buf.value.decode()] = (int(la.value), float(ms.value))
+    return out
+
+
+# ----------------------------------------------------------------- host math
+def create_params(q, n):
+    p = _Params()
+    _check(lib().nttb_create_params(q, n, ctypes.byref(p)))
+    return {k: int(getattr(p, k)) for k, _ in _Params._fields_}
+
+
+def find_primitive_root(q, n):
+    w = _u64()
+    _check(lib().nttb_find_primitive_root(q, n, ctypes.byref(w)))
+    return int(w.value)
+
+
+def find_psi(q, n):
+    w = _u64()
+    _check(lib().nttb_find_psi(q, n, ctypes.byref(w)))
+    return int(w.value)
+
+
+def host_ntt(data_np, q, inverse=False):
+    """ntt_host equivalent on a numpy uint64 array (in place, returns it)."""
+    import numpy as np
+    assert data_np.dtype == np.uint64 and data_np.flags.c_contiguous
+    p = _Params()
+    _check(lib().nttb_create_params(q, data_np.size, ctypes.byref(p)))
+    _check(lib().nttb_host_ntt(data_np.ctypes.data, data_np.size, ctypes.byref(p), int(inverse)))
+    return data_np
+
+
+def generate_primes(bits, two_adicity, count):
+    import numpy as np
+    out = np.zeros(count, dtype=np.uint64)
+    _check(lib().nttb_generate_primes(bits, two_adicity, count, out.ctypes.data))
+    return [int(x) for x in out]
+
+
+# ------------------------------------------------------------------- plans
+class Plan:
+    """Single-modulus plan over uint64 words (backs the drop-in NTTConfig)."""
+
+    def __init__(self, n, q):
+        h = _vp()
+        _check(lib().nttb_plan_create(n, q, ctypes.byref(h)))
+        self._h = h
+        self.n, self.q = n, q
+
+    def info(self):
+        i = _PlanInfo()
+        _check(lib().nttb_plan_get_info(self._h, ctypes.byref(i)))
+        return i
+
+    def transform(self, data, batch=1, inverse=False, engine="auto", stream=None):
+        _check(lib().nttb_u64_transform(self._h, _ptr(data), batch, int(inverse), _engine(engine), _stream(stream)))
+
+    def four_step(self, data, inverse=False, stream=None):
+        _check(lib().nttb_u64_four_step(self._h, _ptr(data), int(inverse), _stream(stream)))
+
+    def rowmaj_forward(self, data, stream=None):
+        _check(lib().nttb_u64_rowmaj_forward(self._h, _ptr(data), _stream(stream)))
+
+    def pointwise_mul(self, out, a, b, stream=None):
+        _check(lib().nttb_u64_pointwise_mul(self._h, _ptr(out), _ptr(a), _ptr(b), _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nttb_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def transpose_u64(dst, src, rows, cols, stream=None):
+    _check(lib().nttb_u64_transpose(_ptr(dst), _ptr(src), rows, cols, _stream(stream)))
+
+
+def bit_reverse_u64(data, n, stream=None):
+    _check(lib().nttb_u64_bit_reverse(_ptr(data), n, _stream(stream)))
+
+
+class RnsPlan:
+    """Batched RNS plan over uint32 residues, layout [poly][limb][n]."""
+
+    def __init__(self, log_n, moduli, negacyclic=False):
+        import numpy as np
+        m = np.ascontiguousarray(moduli, dtype=np.uint64)
+        h = _vp()
+        _check(lib().nttb_rns_plan_create(log_n, m.ctypes.data, m.size, NEGACYCLIC if negacyclic else 0,
+                                          ctypes.byref(h)))
+        self._h = h
+        self.log_n, self.n, self.moduli, self.negacyclic = log_n, 1 << log_n, [int(x) for x in m], negacyclic
+
+    def transform(self, dst, src, n_polys, inverse=False, engine="auto", stream=None):
+        _check(lib().nttb_rns_transform(self._h, _ptr(dst), _ptr(src), n_polys, int(inverse), _engine(engine),
+                                        _stream(stream)))
+
+    def pointwise_mul(self, out, a, b, n_polys, stream=None):
+        _check(lib().nttb_rns_pointwise_mul(self._h, _ptr(out), _ptr(a), _ptr(b), n_polys, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nttb_rns_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class WidePlan:
+    """Plan for moduli below 2^62, residues stored as uint64."""
+
+    def __init__(self, log_n, moduli, negacyclic=False):
+        import numpy as np
+        m = np.ascontiguousarray(moduli, dtype=np.uint64)
+        h = _vp()
+        _check(lib().nttb_wide_plan_create(log_n, m.ctypes.data, m.size, NEGACYCLIC if negacyclic else 0,
+                                           ctypes.byref(h)))
+        self._h = h
+        self.log_n, self.n, self.moduli = log_n, 1 << log_n, [int(x) for x in m]
+
+    def transform(self, dst, src, n_polys, inverse=False, stream=None):
+        _check(lib().nttb_wide_transform(self._h, _ptr(dst), _ptr(src), n_polys, int(inverse), _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nttb_wide_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,96 @@
+"""CPU: the C-ABI library loads, exports every declared symbol, and its host
+math matches the oracle.  No device work is issued here."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import BABYBEAR, Q60, ROOT
+from oracle import oracle as O
+import ntt_b200 as nb
+
+
+def test_library_exports_every_header_symbol():
+    L = nb.lib()
+    syms = nb.header_symbols()
+    assert len(syms) >= 24
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_library_exports_dropin_cpp_api():
+    out = subprocess.run(["nm", "-DC", "--defined-only", nb.LIB_PATH], capture_output=True, text=True).stdout
+    for name in ["ntt::ntt_init", "ntt::ntt_cleanup", "ntt::ntt_forward_basic", "ntt::ntt_inverse_basic",
+                 "ntt::ntt_forward_four_step", "ntt::ntt_inverse_four_step", "ntt::ntt_forward_tlmop",
+                 "ntt::ntt_inverse_tlmop", "ntt::ntt_forward_optimized", "ntt::ntt_inverse_optimized",
+                 "ntt::ntt_forward_rowmaj", "ntt::rowmaj_to_pretransposed", "ntt::rowmaj_from_pretransposed",
+                 "ntt::ntt_forward_batch", "ntt::ntt_inverse_batch", "ntt::poly_multiply_ntt",
+                 "ntt::bit_reverse_permute", "ntt::ntt_host"]:
+        assert name + "(" in out, name
+
+
+def test_version_and_status_strings():
+    assert "sm_100a" in nb.version()
+    assert nb.lib().nttb_status_string(0) == b"ok"
+
+
+@pytest.mark.parametrize("q,n", [(BABYBEAR, 1 << 16), (BABYBEAR, 2), (1073479681, 1 << 20), (Q60, 1 << 20),
+                                 (4293918721, 1 << 12), (2147352577, 1 << 17)])
+def test_create_params_matches_oracle(q, n):
+    keys = ["q", "q_twice", "barrett_k", "barrett_m", "omega", "omega_inv", "n_inv"]
+    assert nb.create_params(q, n) == dict(zip(keys, O.params(q, n)))
+    assert nb.find_primitive_root(q, n) == O.primitive_root(q, n)
+
+
+def test_psi_squares_to_omega():
+    for q in (BABYBEAR, 2147352577, Q60):
+        n = 1 << 12
+        psi = nb.find_psi(q, n)
+        assert psi == O.psi(q, n)
+        assert pow(psi, 2, q) == nb.find_primitive_root(q, n)
+        assert pow(psi, n, q) == q - 1
+
+
+@pytest.mark.parametrize("lg", [1, 2, 6, 10, 12])
+def test_host_ntt_matches_oracle(lg):
+    rng = np.random.default_rng(lg)
+    for q in (BABYBEAR, Q60):
+        x = rng.integers(0, q, 1 << lg, dtype=np.uint64)
+        for inv in (False, True):
+            y = x.copy()
+            nb.host_ntt(y, q, inv)
+            assert (y == O.ntt(x, q, inv)).all()
+
+
+def test_generate_primes():
+    ps = nb.generate_primes(31, 17, 24)
+    assert len(set(ps)) == 24 and all(p < 2 ** 31 and (p - 1) % (1 << 17) == 0 for p in ps)
+    assert ps == sorted(ps, reverse=True)
+    for p in ps[:4]:
+        assert pow(3, p - 1, p) == 1
+
+
+def test_invalid_arguments_rejected_without_device():
+    h = ctypes.c_void_p()
+    L = nb.lib()
+    assert L.nttb_plan_create(1000, BABYBEAR, ctypes.byref(h)) == 1      # not a power of two
+    assert b"power of two" in L.nttb_last_error()
+    assert L.nttb_plan_create(1 << 10, 1 << 62, ctypes.byref(h)) == 2    # modulus too wide
+    assert L.nttb_rns_plan_create(30, None, 0, 0, ctypes.byref(h)) == 1  # no moduli
+    assert L.nttb_u64_transform(None, None, 1, 0, 0, None) == 1
+    assert L.nttb_rns_transform(None, None, None, 1, 0, 0, None) == 1
+
+
+def test_dropin_headers_compile_reference_test_programs():
+    """The reference's own test sources compile against include/ntt.cuh (drop-in)."""
+    ref = "/root/reference/tests/test_ntt.cu"
+    if not os.path.exists(ref):
+        pytest.skip("reference tree not present")
+    out = os.path.join(ROOT, "_work", "dropin_compile_check.o")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    r = subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I" + os.path.join(ROOT, "include"), "-c", ref, "-o", out],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -1,0 +1,186 @@
+"""GPU parity of the uint64-word drop-in path (the reference's include/ntt.cuh
+entry points) against the oracle, the golden fixtures and the reference's own
+GPU kernels.  Tolerance: zero mismatches (exact integer arithmetic)."""
+import numpy as np
+import pytest
+
+from conftest import BABYBEAR, Q60, golden, to_dev, to_host
+from oracle import oracle as O
+import ntt_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+ENGINES = ["scalar", "auto"]
+
+
+def rand(n, q, seed):
+    return np.random.default_rng(seed).integers(0, q, n, dtype=np.uint64)
+
+
+def run_u64(torch, plan, x, inverse=False, engine="auto", batch=1):
+    d = to_dev(torch, x)
+    plan.transform(d, batch=batch, inverse=inverse, engine=engine)
+    torch.cuda.synchronize()
+    return to_host(d, np.uint64)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("lg", [1, 2, 5, 6, 7, 10, 12, 13, 14, 16, 17, 20])
+def test_forward_inverse_vs_oracle(torch_cuda, engine, lg):
+    n = 1 << lg
+    x = rand(n, BABYBEAR, lg)
+    plan = nb.Plan(n, BABYBEAR)
+    y = run_u64(torch_cuda, plan, x, False, engine)
+    ref = O.ntt(x, BABYBEAR)
+    assert (y == ref).all(), "forward mismatches: %d" % int((y != ref).sum())
+    z = run_u64(torch_cuda, plan, y, True, engine)
+    assert (z == x).all()
+    if lg <= 16:
+        assert (run_u64(torch_cuda, plan, x, True, engine) == O.ntt(x, BABYBEAR, True)).all()
+
+
+@pytest.mark.parametrize("n", [64, 256, 1024, 4096])
+def test_golden_seed42(torch_cuda, n):
+    g = golden("babybear_seed42.npz")
+    plan = nb.Plan(n, BABYBEAR)
+    assert (run_u64(torch_cuda, plan, g["in_%d" % n]) == g["fwd_%d" % n]).all()
+    assert (run_u64(torch_cuda, plan, g["in_%d" % n], True) == g["inv_%d" % n]).all()
+
+
+@pytest.mark.parametrize("n", [64, 128, 4096])
+def test_golden_iplus1(torch_cuda, n):
+    g = golden("babybear_iplus1.npz")
+    plan = nb.Plan(n, BABYBEAR)
+    assert (run_u64(torch_cuda, plan, np.arange(1, n + 1, dtype=np.uint64)) == g["fwd_%d" % n]).all()
+
+
+@pytest.mark.parametrize("q", [1073479681, 1073610753, 2147352577])
+def test_other_31bit_primes(torch_cuda, q):
+    for lg in (4, 11, 15):
+        n = 1 << lg
+        x = rand(n, q, lg + 100)
+        plan = nb.Plan(n, q)
+        assert (run_u64(torch_cuda, plan, x) == O.ntt(x, q)).all()
+
+
+def test_batch_matches_per_poly(torch_cuda):
+    n, b = 1 << 12, 7
+    x = np.stack([rand(n, BABYBEAR, 300 + i) for i in range(b)])
+    plan = nb.Plan(n, BABYBEAR)
+    y = run_u64(torch_cuda, plan, x.reshape(-1), batch=b).reshape(b, n)
+    for i in range(b):
+        assert (y[i] == O.ntt(x[i], BABYBEAR)).all()
+
+
+def test_wide_modulus_through_u64_plan(torch_cuda):
+    g = golden("q60.npz")
+    q = int(g["q"])
+    plan = nb.Plan(1024, q)
+    assert (run_u64(torch_cuda, plan, g["inp"]) == g["fwd"]).all()
+    assert (run_u64(torch_cuda, plan, g["inp"], True) == g["inv"]).all()
+    plan2 = nb.Plan(1 << 12, 4293918721)  # 32-bit modulus (>= 2^31) runs the 64-bit path
+    x = rand(1 << 12, 4293918721, 9)
+    assert (run_u64(torch_cuda, plan2, x) == O.ntt(x, 4293918721)).all()
+
+
+@pytest.mark.parametrize("n", [128, 4096, 8192, 16384, 1 << 16])
+def test_four_step_matches_reference_map(torch_cuda, n):
+    x = rand(n, BABYBEAR, n)
+    plan = nb.Plan(n, BABYBEAR)
+    d = to_dev(torch_cuda, x)
+    plan.four_step(d)
+    torch_cuda.cuda.synchronize()
+    y = to_host(d, np.uint64)
+    assert (y == O.four_step(x, BABYBEAR)).all()
+    plan.four_step(d, inverse=True)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == x).all()
+
+
+def test_rowmaj_forward(torch_cuda):
+    n = 4096
+    x = rand(n, BABYBEAR, 77)
+    pre = O.to_pretransposed(x, 64, 64)
+    plan = nb.Plan(n, BABYBEAR)
+    d = to_dev(torch_cuda, pre)
+    plan.rowmaj_forward(d)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == O.rowmaj_forward(pre, BABYBEAR)).all()
+    # other sizes: plain forward on the buffer as given (src/ntt_optimized.cu:944-948)
+    plan2 = nb.Plan(1024, BABYBEAR)
+    x2 = rand(1024, BABYBEAR, 78)
+    d2 = to_dev(torch_cuda, x2)
+    plan2.rowmaj_forward(d2)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d2, np.uint64) == O.ntt(x2, BABYBEAR)).all()
+
+
+def test_transpose_helpers(torch_cuda):
+    x = rand(64 * 128, BABYBEAR, 5)
+    src = to_dev(torch_cuda, x)
+    dst = torch_cuda.empty_like(src)
+    nb.transpose_u64(dst, src, 64, 128)  # rowmaj_to_pretransposed(N1=64, N2=128)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(dst, np.uint64) == O.to_pretransposed(x, 64, 128)).all()
+    back = torch_cuda.empty_like(src)
+    nb.transpose_u64(back, dst, 128, 64)  # rowmaj_from_pretransposed(N1=64, N2=128)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(back, np.uint64) == x).all()
+
+
+def test_pointwise_and_bitrev(torch_cuda):
+    n = 1 << 12
+    for q in (BABYBEAR, Q60):
+        a, b = rand(n, q, 1), rand(n, q, 2)
+        plan = nb.Plan(n, q)
+        da, db = to_dev(torch_cuda, a), to_dev(torch_cuda, b)
+        out = torch_cuda.empty_like(da)
+        plan.pointwise_mul(out, da, db)
+        torch_cuda.cuda.synchronize()
+        assert (to_host(out, np.uint64) == O.pointwise(a, b, q)).all()
+    nb.bit_reverse_u64(da, n)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(da, np.uint64) == O.bit_reverse(a)).all()
+
+
+def test_negacyclic_polymul_through_dropin_ops(torch_cuda):
+    """Cyclic drop-in ops compose to a cyclic convolution (the reference's
+    test_polynomial_multiplication is negacyclic and skipped; see RNS tests)."""
+    n, q = 256, BABYBEAR
+    a, b = rand(n, q, 11), rand(n, q, 12)
+    plan = nb.Plan(n, q)
+    da, db = to_dev(torch_cuda, a), to_dev(torch_cuda, b)
+    plan.transform(da)
+    plan.transform(db)
+    out = torch_cuda.empty_like(da)
+    plan.pointwise_mul(out, da, db)
+    plan.transform(out, inverse=True)
+    torch_cuda.cuda.synchronize()
+    cyc = np.zeros(n, dtype=object)
+    for i in range(n):
+        cyc[(i + np.arange(n)) % n] += int(a[i]) * b.astype(object)
+    assert (to_host(out, np.uint64) == np.array([int(v) % q for v in cyc], dtype=np.uint64)).all()
+
+
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.parametrize("n,op", [(4096, 4), (1 << 16, 4), (4096, 5), (1 << 16, 5), (1024, 0), (1024, 1),
+                                  (4096, 2), (4096, 3)])
+def test_vs_reference_gpu_kernels(torch_cuda, n, op):
+    """Same bytes in, same bytes out as the reference's own kernels (compiled for sm_100a).
+    op: 0/1 basic fwd/inv, 2/3 four-step fwd/inv (n=4096: the reference's race-free size),
+    4/5 optimized fwd/inv."""
+    R = O.ref()
+    x = O.ref_random_polynomial(n, BABYBEAR, 42)
+    cfg = R.ref_ntt_init(n, BABYBEAR)
+    d_ref = to_dev(torch_cuda, x)
+    R.ref_ntt_run(cfg, d_ref.data_ptr(), op)
+    torch_cuda.cuda.synchronize()
+    R.ref_ntt_cleanup(cfg)
+    plan = nb.Plan(n, BABYBEAR)
+    d = to_dev(torch_cuda, x)
+    if op in (2, 3):
+        plan.four_step(d, inverse=(op == 3))
+    else:
+        plan.transform(d, inverse=(op % 2 == 1), engine="scalar" if op < 2 else "auto")
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == to_host(d_ref, np.uint64)).all()
