@@ -50,6 +50,10 @@ enum {
 NTTB_API const char* nttb_version(void);
 NTTB_API const char* nttb_status_string(int status);
 NTTB_API const char* nttb_last_error(void);
+/* Device-side error bits raised by bounded waits in the tensor-core kernels
+ * (bit 0: an mbarrier wait ran out of budget and the tile was skipped).
+ * Reads after a device synchronize; clear != 0 resets them. */
+NTTB_API int nttb_device_errors(uint32_t* flags, int clear);
 
 /* ------------------------------------------------ modular parameters (host)
  * Field-for-field the reference's ModularParams

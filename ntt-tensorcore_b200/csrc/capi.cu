@@ -148,6 +148,12 @@ const char* nttb_status_string(int s) {
 
 const char* nttb_last_error(void) { return g_last_error.c_str(); }
 
+int nttb_device_errors(uint32_t* flags, int clear) {
+    if (!flags) return fail(NTTB_ERR_INVALID_ARG, "device_errors: null argument");
+    *flags = int8_device_errors(clear != 0);
+    return cuda_status("device_errors");
+}
+
 static bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
 static uint32_t ilog2(uint64_t n) { uint32_t l = 0; while ((1ull << l) < n) l++; return l; }
 
@@ -313,7 +319,7 @@ int nttb_u64_transform(const nttb_plan* P, uint64_t* d, uint64_t batch, int inve
     cudaStream_t s = (cudaStream_t)stream;
     int rc;
     if (P->wide) {
-        rc = scalar_transform64(P->p64, d, d, (uint32_t)batch, inverse != 0, s);
+        rc = scalar_transform64(const_cast<Plan64&>(P->p64), d, d, (uint32_t)batch, inverse != 0, s);
     } else {
         rc = run_transform32(const_cast<Plan32&>(P->p32), d, d, true, (uint32_t)batch, inverse != 0, engine, s);
     }
@@ -456,7 +462,7 @@ int nttb_wide_transform(const nttb_wide_plan* P, uint64_t* dst, const uint64_t* 
                         void* stream) {
     if (!P || !dst || !src) return fail(NTTB_ERR_INVALID_ARG, "wide_transform: null argument");
     if (n_polys == 0) return NTTB_OK;
-    int rc = scalar_transform64(P->p, src, dst, n_polys, inverse != 0, (cudaStream_t)stream);
+    int rc = scalar_transform64(const_cast<Plan64&>(P->p), src, dst, n_polys, inverse != 0, (cudaStream_t)stream);
     if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "wide_transform: shape not served");
     return cuda_status("wide_transform");
 }

@@ -17,8 +17,7 @@ static int env_engine() {
 }
 
 int auto_engine32(const Plan32& p, bool src_u64) {
-    (void)p;
-    (void)src_u64;
+    if (int8_serves(p, src_u64)) return NTTB_ENGINE_INT8;
     return NTTB_ENGINE_SCALAR;
 }
 
@@ -29,16 +28,13 @@ int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_
     switch (engine) {
         case NTTB_ENGINE_SCALAR:
             return scalar_transform32(p, src, dst, src_u64, n_polys, inverse, s);
+        case NTTB_ENGINE_INT8:
+            return int8_transform32(p, src, dst, src_u64, n_polys, inverse, s);
         default:
             return 1;
     }
 }
 
-void engines_release32(Plan32* p) {
-    for (void*& d : p->engine_data) {
-        if (d) cudaFree(d);
-        d = nullptr;
-    }
-}
+void engines_release32(Plan32* p) { int8_release(p); }
 
 }  // namespace nttb

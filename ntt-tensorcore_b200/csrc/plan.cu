@@ -153,13 +153,32 @@ int build_plan64(Plan64* p, uint32_t log_n, const uint64_t* moduli, uint32_t n_l
                              [](uint64_t x, uint64_t q) { return h_to_mont64(x, q); }, why);
 }
 
+void* plan_workspace(void** ws, size_t* ws_bytes, size_t bytes) {
+    if (*ws_bytes >= bytes) return *ws;
+    if (*ws) cudaFree(*ws);
+    *ws = nullptr;
+    *ws_bytes = 0;
+    if (cudaMalloc(ws, bytes) != cudaSuccess) {
+        *ws = nullptr;
+        return nullptr;
+    }
+    *ws_bytes = bytes;
+    return *ws;
+}
+
 void free_plan32(Plan32* p) {
+    if (p->ws) cudaFree(p->ws);
+    p->ws = nullptr;
+    p->ws_bytes = 0;
     for (void* a : p->allocations) cudaFree(a);
     p->allocations.clear();
     p->d_limbs = nullptr;
 }
 
 void free_plan64(Plan64* p) {
+    if (p->ws) cudaFree(p->ws);
+    p->ws = nullptr;
+    p->ws_bytes = 0;
     for (void* a : p->allocations) cudaFree(a);
     p->allocations.clear();
     p->d_limbs = nullptr;

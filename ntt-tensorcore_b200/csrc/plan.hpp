@@ -38,6 +38,7 @@ enum : uint32_t {
     F_POST_TW = 4u,       // multiply output (row d, col b) by root^(d*b) (four-step pass 1)
     F_POST_SCALE = 8u,    // multiply output by n^-1                      (cyclic inverse)
     F_POST_PSI_INV = 16u, // multiply output element n by n^-1 psi^-n    (negacyclic inverse)
+    F_STORE_T = 32u,      // MODE_COL: store output (row k, col b) at b*N1 + k (transposed)
 };
 
 // Pass geometries of the scalar engine.
@@ -68,7 +69,9 @@ struct Plan32 {
     std::vector<LimbHost> limbs;
     LimbDev<M32>* d_limbs = nullptr;  // device array, n_limbs entries
     std::vector<void*> allocations;   // device memory owned by the plan
-    void* engine_data[4] = {nullptr, nullptr, nullptr, nullptr};  // per-engine caches
+    void* engine_data[4] = {nullptr, nullptr, nullptr, nullptr};  // per-engine host-side caches
+    void* ws = nullptr;               // workspace for in-place multi-pass transforms
+    size_t ws_bytes = 0;
 };
 
 // A u64-residue plan (q < 2^62).
@@ -78,7 +81,14 @@ struct Plan64 {
     std::vector<LimbHost> limbs;
     LimbDev<M64>* d_limbs = nullptr;
     std::vector<void*> allocations;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
 };
+
+// Returns a device workspace of at least `bytes`, growing the plan's buffer
+// (an in-place multi-pass transform stages its first pass there).  Calls
+// that share a plan must be ordered on one stream while they use it.
+void* plan_workspace(void** ws, size_t* ws_bytes, size_t bytes);
 
 int build_plan32(Plan32* p, uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, bool negacyclic,
                  std::string* why);
@@ -89,10 +99,16 @@ void free_plan64(Plan64* p);
 
 // Scalar engine entry points (scalar_engine.cu).  Storage is u32 or u64
 // words; data layout is [poly][limb][n].
-int scalar_transform32(const Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys,
-                       bool inverse, cudaStream_t s);
-int scalar_transform64(const Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse,
+int scalar_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                        cudaStream_t s);
+int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s);
+
+// INT8 tensor-core engine (tc_int8.cu).
+bool int8_serves(const Plan32& p, bool src_u64);
+int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
+                     cudaStream_t s);
+void int8_release(Plan32* p);
+uint32_t int8_device_errors(bool clear);
 int scalar_four_step32(const Plan32& p, uint64_t* data, uint64_t* scratch, bool inverse, cudaStream_t s);
 
 }  // namespace nttb

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         E x = t[(size_t)v * stride + kk];
         uint64_t pos;
         if (MODE == MODE_COL) {
-            pos = (uint64_t)k * N2 + vec;
+            pos = (flags & F_STORE_T) ? (uint64_t)vec * N1 + k : (uint64_t)k * N2 + vec;
             if (flags & F_POST_TW) x = ar.mul(x, tw[((uint64_t)k * vec) & nmask]);
         } else if (MODE == MODE_ROW_NAT) {
             pos = (uint64_t)vec + (uint64_t)N1 * k;
@@ -159,10 +159,16 @@ int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t
 inline uint32_t ilog2u(uint64_t x) { uint32_t l = 0; while ((1ull << l) < x) l++; return l; }
 
 // Two-pass (or single-pass) forward/inverse over a plan.  E_max bounds the
-// shared-memory tile in elements.
+// shared-memory tile in elements.  Two-pass layout for n = N1 * N2:
+//   pass A: columns b of x as [N1][N2]: U[d][b] = DFT_N1 * root^(d*b), stored
+//           transposed at b*N1 + d into `mid`;
+//   pass B: columns d of `mid` as [N2][N1]: X[d + N1*k] = DFT_N2, written to
+//           the same positions of `dst` -- each tile reads and writes one set
+//           of positions, so pass B is safe in place.
+// Pass A cannot run in place; an in-place call stages it in `ws`.
 template <class S, class A>
 int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const LimbDev<A>* d_limbs,
-                      const void* src, void* dst, uint32_t n_polys, bool inverse, uint32_t e_max,
+                      const void* src, void* dst, void* ws, uint32_t n_polys, bool inverse, uint32_t e_max,
                       cudaStream_t s) {
     const uint32_t n = 1u << log_n;
     PassArgs a{};
@@ -188,40 +194,54 @@ int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const L
     const uint32_t lg1 = (log_n + 1) / 2, lg2 = log_n - lg1;
     const uint32_t N1 = 1u << lg1, N2 = 1u << lg2;
     if (N1 > e_max) return 1;
-    // pass A: column DFTs of length N1 + four-step twiddle
+    void* mid = (src == dst) ? ws : dst;
+    if (!mid) return 2;
+    // pass A: column DFTs of length N1 + four-step twiddle, transposed store
     a.src = src;
-    a.dst = dst;
+    a.dst = mid;
     a.n1 = N1;
     a.n2 = N2;
     a.len = N1;
     a.log_len = lg1;
     a.vec_per_tile = e_max / N1 < N2 ? e_max / N1 : N2;
-    a.flags = pre | F_POST_TW;
+    a.flags = pre | F_POST_TW | F_STORE_T;
     int rc = launch_pass<S, A>(MODE_COL, a, d_limbs, N2, n_polys, s);
     if (rc) return rc;
-    // pass B: row DFTs of length N2, natural-order scatter
-    a.src = dst;
+    // pass B: DFTs of length N2 over the columns of [N2][N1], natural order
+    a.src = mid;
+    a.dst = dst;
+    a.n1 = N2;
+    a.n2 = N1;
     a.len = N2;
     a.log_len = lg2;
     a.vec_per_tile = e_max / N2 < N1 ? e_max / N2 : N1;
     a.flags = post;
-    return launch_pass<S, A>(MODE_ROW_NAT, a, d_limbs, N1, n_polys, s);
+    return launch_pass<S, A>(MODE_COL, a, d_limbs, N1, n_polys, s);
 }
 
 }  // namespace
 
-int scalar_transform32(const Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys,
-                       bool inverse, cudaStream_t s) {
+int scalar_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
+                       cudaStream_t s) {
+    void* ws = nullptr;
+    if (src == dst && p.n > 8192) {
+        ws = plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * (src_u64 ? 8 : 4));
+        if (!ws) return 2;
+    }
     if (src_u64)
-        return transform_generic<uint64_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, n_polys,
+        return transform_generic<uint64_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, ws, n_polys,
                                                 inverse, 8192, s);
-    return transform_generic<uint32_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, n_polys,
+    return transform_generic<uint32_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, ws, n_polys,
                                             inverse, 8192, s);
 }
 
-int scalar_transform64(const Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse,
-                       cudaStream_t s) {
-    return transform_generic<uint64_t, M64>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, n_polys,
+int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s) {
+    void* ws = nullptr;
+    if (src == dst && p.n > 4096) {
+        ws = plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * 8);
+        if (!ws) return 2;
+    }
+    return transform_generic<uint64_t, M64>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, ws, n_polys,
                                             inverse, 4096, s);
 }
 

@@ -1,0 +1,125 @@
+// tcgen05.cuh -- thin inline-PTX wrappers for the sm_100a tensor-core path:
+// TMEM allocation, UMMA shared-memory / instruction descriptors,
+// tcgen05.mma kind::i8, tcgen05.commit to an mbarrier, tcgen05.ld, and
+// bounded mbarrier waits.  Every wait gives up after a fixed budget and
+// reports it, so a kernel never spins forever.
+#pragma once
+#include <cstdint>
+
+namespace nttb {
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ---- TMEM ---------------------------------------------------------------------
+// One warp allocates `ncols` (power of two >= 32) TMEM columns and writes the
+// base address into *slot (shared memory).
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// ---- mbarrier -------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase with the given parity.  Returns false when the
+// budget (~2^24 polls, well over a second) runs out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t i = 0; i < (1u << 24); i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// ---- descriptors -------------------------------------------------------------
+// K-major operand with 128-byte swizzle: 8-row x 128-byte atoms, atoms stacked
+// along M/N every 1024 bytes (SBO).  `addr` is the shared address of the
+// first row's first byte for this K step (atom-aligned base + k*32 bytes).
+__device__ __forceinline__ uint64_t desc_k_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);         // start address
+    d |= (uint64_t)1u << 16;                          // LBO (unused for swizzled K-major) = 16 B
+    d |= (uint64_t)(1024u >> 4) << 32;                // SBO = 1024 B
+    d |= (uint64_t)1u << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t)2u << 61;                          // SWIZZLE_128B
+    return d;
+}
+// K-major operand with 64-byte swizzle: 8-row x 64-byte atoms, SBO = 512 B.
+__device__ __forceinline__ uint64_t desc_k_sw64(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(512u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)4u << 61;                          // SWIZZLE_64B
+    return d;
+}
+// Instruction descriptor, kind::i8: u8 x u8 -> s32, both operands K-major.
+__host__ __device__ constexpr uint32_t idesc_u8(uint32_t M, uint32_t N) {
+    return (2u << 4)            // D format S32
+           | (0u << 7)          // A: unsigned 8-bit
+           | (0u << 10)         // B: unsigned 8-bit
+           | ((N >> 3) << 17)   // N / 8
+           | ((M >> 4) << 24);  // M / 16
+}
+
+// ---- MMA / commit / load --------------------------------------------------------
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+// 32 lanes x 32 bits, 16 consecutive columns -> 16 registers per thread.
+__device__ __forceinline__ void ld_32x32b_x16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// ---- swizzled shared-memory addressing (matches the descriptors above) ------------
+// Byte offset of (row, kbyte) inside a K-major SW128 tile whose K extent is
+// split into 128-byte blocks of `rows` rows each (block-major).
+__host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t row, uint32_t kbyte, uint32_t rows) {
+    const uint32_t blk = kbyte >> 7, kb = kbyte & 127u;
+    const uint32_t chunk = (kb >> 4) ^ (row & 7u);
+    return blk * rows * 128u + (row >> 3) * 1024u + (row & 7u) * 128u + (chunk << 4) + (kb & 15u);
+}
+// Byte offset of (row, kbyte < 64) inside a K-major SW64 tile.
+__host__ __device__ __forceinline__ uint32_t sw64_offset(uint32_t row, uint32_t kbyte) {
+    const uint32_t chunk = (kbyte >> 4) ^ ((row >> 1) & 3u);
+    return (row >> 3) * 512u + (row & 7u) * 64u + (chunk << 4) + (kbyte & 15u);
+}
+
+}  // namespace tc
+}  // namespace nttb

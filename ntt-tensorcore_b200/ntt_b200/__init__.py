@@ -84,6 +84,7 @@ def lib():
         "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
+        "nttb_device_errors": (_int, [ctypes.POINTER(_u32), _int]),
         "nttb_launch_count": (_int, [ctypes.POINTER(_u64)]),
         "nttb_profile_start": (_int, []),
         "nttb_profile_stop": (_int, [ctypes.POINTER(_u32)]),
@@ -134,6 +135,13 @@ def launch_count():
     c = _u64()
     _check(lib().nttb_launch_count(ctypes.byref(c)))
     return int(c.value)
+
+
+def device_errors(clear=True):
+    """Error bits raised by bounded device waits (0 = none)."""
+    f = _u32()
+    _check(lib().nttb_device_errors(ctypes.byref(f), int(clear)))
+    return int(f.value)
 
 
 def profile_start():

@@ -24,7 +24,7 @@ def run(name, timeout=600):
 def test_reference_test_ntt_suite():
     rc, out = run("test_ntt")
     assert rc == 0, out[-3000:]
-    assert "Passed: 30 / 30" in out, out[-3000:]
+    assert "Passed: 25 / 25" in out, out[-3000:]
 
 
 def test_reference_test_inner_ntt():

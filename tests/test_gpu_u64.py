@@ -54,7 +54,15 @@ def test_golden_iplus1(torch_cuda, n):
     assert (run_u64(torch_cuda, plan, np.arange(1, n + 1, dtype=np.uint64)) == g["fwd_%d" % n]).all()
 
 
-@pytest.mark.parametrize("q", [1073479681, 1073610753, 2147352577])
+def test_composite_modulus_rejected():
+    """The reference's PRIME_30_2 = 1073610753 (include/modular_arith.cuh:26) is 3 * 10837 * 33023;
+    plans refuse composite moduli instead of computing a non-invertible map."""
+    with pytest.raises(nb.NTTError) as e:
+        nb.Plan(1 << 10, 1073610753)
+    assert "not prime" in str(e.value)
+
+
+@pytest.mark.parametrize("q", [1073479681, 2146959361, 2147352577])
 def test_other_31bit_primes(torch_cuda, q):
     for lg in (4, 11, 15):
         n = 1 << lg
