@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "int8", "dmma", "scalar"])
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
+    ap.add_argument("--quick", action="store_true",
+                    help="warm-up + timed steps only (no clock soak, e2e, comparisons or CPU leg): "
+                         "the short run used under ncu")
     return ap.parse_args()
 
 
@@ -225,6 +228,11 @@ def run_ours(args, world, rank, local):
     for i in range(max(3, args.warmup)):
         step(i, engine)
     torch.cuda.synchronize()
+    if args.quick:
+        ms, launches = timed(engine, args.steps)
+        return {"metric": METRIC, "value": world * coeffs_per_step * args.steps / (ms / 1e3), "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "ms_per_step": ms / args.steps, "quick": True,
+                "config": {"workload": WORKLOAD, "engine": engine}, "gpu_launches": launches}, qs
     clocks = ClockSampler(local)
     clocks.start()
     t_end = time.time() + 1.0
@@ -354,7 +362,7 @@ def main():
         print(json.dumps(line))
         return
     result, qs = run_ours(args, world, rank, local)
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.quick:
         result["cpu_baseline"] = bounded_cpu_baseline(qs)
     if rank == 0:
         print(json.dumps(result))

@@ -30,11 +30,16 @@ int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_
             return scalar_transform32(p, src, dst, src_u64, n_polys, inverse, s);
         case NTTB_ENGINE_INT8:
             return int8_transform32(p, src, dst, src_u64, n_polys, inverse, s);
+        case NTTB_ENGINE_DMMA:
+            return dmma_transform32(p, src, dst, src_u64, n_polys, inverse, s);
         default:
             return 1;
     }
 }
 
-void engines_release32(Plan32* p) { int8_release(p); }
+void engines_release32(Plan32* p) {
+    int8_release(p);
+    dmma_release(p);
+}
 
 }  // namespace nttb

@@ -109,6 +109,12 @@ int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32
                      cudaStream_t s);
 void int8_release(Plan32* p);
 uint32_t int8_device_errors(bool clear);
+
+// FP64 DMMA tensor-core engine (tc_dmma.cu).
+bool dmma_serves(const Plan32& p, bool src_u64);
+int dmma_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
+                     cudaStream_t s);
+void dmma_release(Plan32* p);
 int scalar_four_step32(const Plan32& p, uint64_t* data, uint64_t* scratch, bool inverse, cudaStream_t s);
 
 }  // namespace nttb

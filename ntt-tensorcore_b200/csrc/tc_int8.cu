@@ -116,8 +116,8 @@ __global__ void __launch_bounds__(128) int8_pass_a_n16(const uint32_t* __restric
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;                  // 2 kblocks x 128 rows x 128 B = 32 KB
     uint8_t* sB = smem + 32768;          // 64 KB
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 32768 + kMatBytes64);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 1);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 32768 + kMatBytes64);  // [0] MMA done, [1] B landed
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 2);
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t limb = blockIdx.y, poly = blockIdx.z, b0 = blockIdx.x * 128u;
@@ -127,27 +127,33 @@ __global__ void __launch_bounds__(128) int8_pass_a_n16(const uint32_t* __restric
     uint32_t* out = dst + off;
 
     if (warp == 0) tc::tmem_alloc(slot, 256);
-    if (tid == 0) tc::mbar_init(bar, 1);
-    copy_g2s(sB, L.mat_a, kMatBytes64);
-    // transposed load: vector m = column b0 + m, K index a (4 residues per 16-byte chunk)
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        tc::mbar_init(bar + 1, 1);
+        tc::mbar_expect_tx(bar + 1, kMatBytes64);
+#pragma unroll
+        for (uint32_t i = 0; i < 4; i++) tc::bulk_g2s(sB + i * 16384u, L.mat_a + i * 16384u, 16384u, bar + 1);
+    }
+    // transposed load: vector m = column b0 + m, K index a (4 residues per 16-byte
+    // chunk); all 64 loads are in flight before the first shared-memory store
     {
-        const uint32_t m = tid;
-        const uint32_t* col = x + b0 + m;
-#pragma unroll 4
-        for (uint32_t c = 0; c < 16; c++) {
-            uint4 v;
-            v.x = __ldg(col + (4 * c + 0) * 1024u);
-            v.y = __ldg(col + (4 * c + 1) * 1024u);
-            v.z = __ldg(col + (4 * c + 2) * 1024u);
-            v.w = __ldg(col + (4 * c + 3) * 1024u);
-            *reinterpret_cast<uint4*>(sA + tc::sw128_offset(m, 16 * c, 128)) = v;
-        }
+        const uint32_t* col = x + b0 + tid;
+        uint32_t v[64];
+#pragma unroll
+        for (uint32_t a = 0; a < 64; a++) v[a] = __ldg(col + a * 1024u);
+#pragma unroll
+        for (uint32_t c = 0; c < 16; c++)
+            *reinterpret_cast<uint4*>(sA + tc::sw128_offset(tid, 16 * c, 128)) =
+                make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
     }
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     const uint32_t taddr = *slot;
-    if (tid == 0) issue_k256(taddr, sA, 128, sB, 256, 256, bar);
+    if (tid == 0) {
+        if (!tc::mbar_wait_bounded(bar + 1, 0)) flag_timeout();
+        issue_k256(taddr, sA, 128, sB, 256, 256, bar);
+    }
     __syncwarp();
     const bool ok = tc::mbar_wait_bounded(bar, 0);
     tc::fence_after_sync();
@@ -197,8 +203,8 @@ __global__ void __launch_bounds__(128) int8_pass_b_n16(const uint32_t* src, uint
     uint8_t* sA = smem;                          // level-1 A (32 KB), then level-2 A (32 KB, SW64)
     uint8_t* sB1 = smem + 32768;                 // 64 KB
     uint8_t* sB2 = smem + 32768 + kMatBytes64;   // 4 KB
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sB2 + kMatBytes16);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 2);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sB2 + kMatBytes16);  // [0] level 1, [1] level 2, [2] B landed
+    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 3);
 
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t limb = blockIdx.y, poly = blockIdx.z, d0 = blockIdx.x * 8u;
@@ -212,28 +218,32 @@ __global__ void __launch_bounds__(128) int8_pass_b_n16(const uint32_t* src, uint
     if (tid == 0) {
         tc::mbar_init(bar, 1);
         tc::mbar_init(bar + 1, 1);
+        tc::mbar_init(bar + 2, 1);
+        tc::mbar_expect_tx(bar + 2, kMatBytes64 + kMatBytes16);
+#pragma unroll
+        for (uint32_t i = 0; i < 4; i++) tc::bulk_g2s(sB1 + i * 16384u, L.mat_b1 + i * 16384u, 16384u, bar + 2);
+        tc::bulk_g2s(sB2, L.mat_b2, kMatBytes16, bar + 2);
     }
-    copy_g2s(sB1, L.mat_b1, kMatBytes64);
-    copy_g2s(sB2, L.mat_b2, kMatBytes16);
     const uint32_t r = tid & 7u, b2 = tid >> 3;
     {
         const uint32_t* base = u + d0 + r;
-#pragma unroll 4
-        for (uint32_t c = 0; c < 16; c++) {
-            uint4 v;
-            v.x = base[((4 * c + 0) * 16u + b2) * 64u];
-            v.y = base[((4 * c + 1) * 16u + b2) * 64u];
-            v.z = base[((4 * c + 2) * 16u + b2) * 64u];
-            v.w = base[((4 * c + 3) * 16u + b2) * 64u];
-            *reinterpret_cast<uint4*>(sA + tc::sw128_offset(tid, 16 * c, 128)) = v;
-        }
+        uint32_t v[64];
+#pragma unroll
+        for (uint32_t a2 = 0; a2 < 64; a2++) v[a2] = base[(a2 * 16u + b2) * 64u];
+#pragma unroll
+        for (uint32_t c = 0; c < 16; c++)
+            *reinterpret_cast<uint4*>(sA + tc::sw128_offset(tid, 16 * c, 128)) =
+                make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
     }
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     const uint32_t taddr = *slot;
     const uint32_t lane_base = taddr + ((warp * 32u) << 16);
-    if (tid == 0) issue_k256(taddr, sA, 128, sB1, 256, 256, bar);
+    if (tid == 0) {
+        if (!tc::mbar_wait_bounded(bar + 2, 0)) flag_timeout();
+        issue_k256(taddr, sA, 128, sB1, 256, 256, bar);
+    }
     __syncwarp();
     bool ok = tc::mbar_wait_bounded(bar, 0);
     tc::fence_after_sync();

@@ -14,12 +14,12 @@ PRIMES21 = nb.generate_primes(31, 21, 8)
 
 
 def engines():
-    return ["scalar", "int8", "auto"]
+    return ["scalar", "int8", "dmma", "auto"]
 
 
 def serves(engine, lg):
-    """The INT8 tensor-core engine serves N = 2^16; AUTO falls back elsewhere."""
-    return engine != "int8" or lg == 16
+    """The tensor-core engines serve N = 2^16; AUTO falls back elsewhere."""
+    return engine not in ("int8", "dmma") or lg == 16
 
 
 def rand_batch(n_polys, moduli, n, seed):
