@@ -129,6 +129,20 @@ NTTB_API int nttb_rns_plan_destroy(nttb_rns_plan* plan);
  * after the inverse. */
 NTTB_API int nttb_rns_transform(const nttb_rns_plan* plan, uint32_t* d_dst, const uint32_t* d_src, uint32_t n_polys,
                        int inverse, int engine, void* stream);
+/* In-place transform that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc while transforming (a
+ * memory manager that owns all device memory, a loop that must never enter
+ * the allocator because cudaMalloc can synchronize the device, a fixed
+ * up-front memory budget).  The first pass is staged in a static device
+ * buffer of NTTB_NOALLOC_SCRATCH_BYTES that every GPU loading the library
+ * holds until exit; batches needing more (n_polys * n_limbs * n * 4 bytes)
+ * are rejected with NTTB_ERR_INVALID_ARG.  The first call on a device looks
+ * up the buffer's address (cudaGetSymbolAddress): make it before any stream
+ * capture.  Calls share the buffer: calls whose work overlaps on the GPU
+ * race.  Runs the CUDA-core engine; same results as nttb_rns_transform. */
+#define NTTB_NOALLOC_SCRATCH_BYTES (8u << 20)
+NTTB_API int nttb_rns_transform_noalloc(const nttb_rns_plan* plan, uint32_t* d_data, uint32_t n_polys, int inverse,
+                                        void* stream);
 /* d_out = d_a * d_b pointwise per limb (NTT domain). */
 NTTB_API int nttb_rns_pointwise_mul(const nttb_rns_plan* plan, uint32_t* d_out, const uint32_t* d_a,
                            const uint32_t* d_b, uint32_t n_polys, void* stream);

@@ -129,6 +129,10 @@ struct nttb_wide_plan {
     Plan64 p;
 };
 
+namespace nttb {
+const Plan32* rns_plan_core(const nttb_rns_plan* p) { return p ? &p->p : nullptr; }
+}  // namespace nttb
+
 extern "C" {
 
 const char* nttb_version(void) { return "ntt_b200 0.1 (sm_100a)"; }

@@ -102,6 +102,10 @@ void free_plan64(Plan64* p);
 int scalar_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                        cudaStream_t s);
 int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s);
+// In-place uint32 transform staging its first pass in a caller-supplied buffer
+// `ws` (n_polys * n_limbs * n words); allocates nothing.
+int scalar_transform32_ws(const Plan32& p, uint32_t* data, void* ws, uint32_t n_polys, bool inverse,
+                          cudaStream_t s);
 
 // INT8 tensor-core engine (tc_int8.cu).
 bool int8_serves(const Plan32& p, bool src_u64);

@@ -235,6 +235,12 @@ int scalar_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint
                                             inverse, 8192, s);
 }
 
+int scalar_transform32_ws(const Plan32& p, uint32_t* data, void* ws, uint32_t n_polys, bool inverse,
+                          cudaStream_t s) {
+    return transform_generic<uint32_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, data, data, ws, n_polys,
+                                            inverse, 8192, s);
+}
+
 int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s) {
     void* ws = nullptr;
     if (src == dst && p.n > 4096) {

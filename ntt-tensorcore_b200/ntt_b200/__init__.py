@@ -81,6 +81,7 @@ def lib():
         "nttb_rns_plan_destroy": (_int, [_vp]),
         "nttb_rns_transform": (_int, [_vp, _vp, _vp, _u32, _int, _int, _vp]),
         "nttb_rns_pointwise_mul": (_int, [_vp, _vp, _vp, _vp, _u32, _vp]),
+        "nttb_rns_transform_noalloc": (_int, [_vp, _vp, _u32, _int, _vp]),
         "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
@@ -262,6 +263,11 @@ class RnsPlan:
 
     def pointwise_mul(self, out, a, b, n_polys, stream=None):
         _check(lib().nttb_rns_pointwise_mul(self._h, _ptr(out), _ptr(a), _ptr(b), n_polys, _stream(stream)))
+
+    def transform_noalloc(self, data, n_polys, inverse=False, stream=None):
+        """In-place transform that allocates no device memory (static scratch;
+        see nttb_rns_transform_noalloc in include/ntt_b200.h)."""
+        _check(lib().nttb_rns_transform_noalloc(self._h, _ptr(data), n_polys, int(inverse), _stream(stream)))
 
     def close(self):
         if getattr(self, "_h", None):
