@@ -129,6 +129,12 @@ NTTB_API int nttb_rns_plan_destroy(nttb_rns_plan* plan);
  * after the inverse. */
 NTTB_API int nttb_rns_transform(const nttb_rns_plan* plan, uint32_t* d_dst, const uint32_t* d_src, uint32_t n_polys,
                        int inverse, int engine, void* stream);
+/* Forward then inverse transform of d_data in place (the round trip of the
+ * reference's test_ntt_inverse, tests/test_ntt.cu:60-123, for a whole RNS
+ * batch).  The INT8 engine runs both in one persistent launch with
+ * per-(poly, limb) stage dependencies; other engines run two transforms. */
+NTTB_API int nttb_rns_forward_inverse(const nttb_rns_plan* plan, uint32_t* d_data, uint32_t n_polys, int engine,
+                                      void* stream);
 /* In-place transform that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc while transforming (a
  * memory manager that owns all device memory, a loop that must never enter

@@ -427,6 +427,24 @@ int nttb_rns_transform(const nttb_rns_plan* P, uint32_t* dst, const uint32_t* sr
     return cuda_status("rns_transform");
 }
 
+int nttb_rns_forward_inverse(const nttb_rns_plan* P, uint32_t* d, uint32_t n_polys, int engine, void* stream) {
+    if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "rns_forward_inverse: null argument");
+    if (n_polys == 0) return NTTB_OK;
+    if (((uintptr_t)d) & 15) return fail(NTTB_ERR_INVALID_ARG, "rns_forward_inverse: pointer must be 16-byte aligned");
+    Plan32& p = const_cast<Plan32&>(P->p);
+    cudaStream_t s = (cudaStream_t)stream;
+    int eng = engine == NTTB_ENGINE_AUTO ? auto_engine32(p, false) : engine;
+    int rc;
+    if (eng == NTTB_ENGINE_INT8) {
+        rc = int8_forward_inverse32(p, d, n_polys, s);
+    } else {
+        rc = run_transform32(p, d, d, false, n_polys, false, eng, s);
+        if (!rc) rc = run_transform32(p, d, d, false, n_polys, true, eng, s);
+    }
+    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_forward_inverse: shape not served by the requested engine");
+    return cuda_status("rns_forward_inverse");
+}
+
 int nttb_rns_pointwise_mul(const nttb_rns_plan* P, uint32_t* out, const uint32_t* a, const uint32_t* b,
                            uint32_t n_polys, void* stream) {
     if (!P || !out || !a || !b) return fail(NTTB_ERR_INVALID_ARG, "rns_pointwise_mul: null argument");

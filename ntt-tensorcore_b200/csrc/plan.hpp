@@ -113,6 +113,8 @@ int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32
                      cudaStream_t s);
 void int8_release(Plan32* p);
 uint32_t int8_device_errors(bool clear);
+// Forward then inverse, in place, in one persistent launch.
+int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStream_t s);
 
 // FP64 DMMA tensor-core engine (tc_dmma.cu).
 bool dmma_serves(const Plan32& p, bool src_u64);

@@ -13,22 +13,34 @@
 // The four INT32 accumulator planes of a vector live in one TMEM lane, so one
 // thread recombines them with three shifted adds -- no cross-thread exchange.
 //
-// N = 2^16 (64 x 64 x 16) runs as two passes; data layout [poly][limb][N]:
-//   pass A: for each column b < 1024 of x viewed as [64][1024]:
-//             U[d][b] = DFT64(x[.][b])[d] * t_A(b, d)
-//           stored transposed (U at b*64 + d) so that each 128-column tile
-//           writes one contiguous 32 KB block.
-//   pass B: for each row d, Z = DFT1024(U[d][.]) as DFT64 (over stride 16,
-//           twiddle t_B1) then DFT16 (contiguous); X[d + 64 k] = Z[k].  A tile
-//           of 8 rows reads and writes exactly the same positions, so pass B
-//           runs in place on its buffer.
-// The four-step twiddles t_A, t_B1 are geometric in the output index and are
-// generated in the epilogue (one Montgomery product to apply, one to advance).
-// Negacyclic twists and n^-1 are folded into the B matrices and the twiddle
-// ratios, so they cost nothing extra.
+// N = 2^16 (64 x 64 x 16) runs as two stages; data layout [poly][limb][N]:
+//   stage A: for each column b < 1024 of x viewed as [64][1024]:
+//              U[d][b] = DFT64(x[.][b])[d] * t_A(b, d)
+//            stored transposed (U at b*64 + d): each 128-column tile writes one
+//            contiguous 32 KB block.
+//   stage B: for each row d, Z = DFT1024(U[d][.]) as DFT64 (over stride 16,
+//            twiddle t_B1) then DFT16 (contiguous); X[d + 64 k] = Z[k].  A tile
+//            of 8 rows reads and writes exactly the same positions.
+// The four-step twiddles are geometric in the output index and are generated
+// in the epilogue: each thread walks two interleaved chains (even and odd
+// outputs, ratio^2 steps) over its 32 outputs.  Negacyclic twists and n^-1
+// are folded into the B matrices and the twiddle tables.
+//
+// Execution: one persistent launch runs a list of stages (one transform = A, B;
+// forward-then-inverse = A, B, A, B).  CTAs draw tiles from a device ticket
+// counter in stage order; a tile of stage s for (poly, limb) first waits,
+// with a bounded spin, until the 8 tiles of stage s-1 of the same (poly, limb)
+// have signalled completion.  Tickets are claimed in order, so every awaited
+// tile belongs to a CTA that is already running: no deadlock.  TMEM, the
+// mbarriers and the last-used B image stay resident across a CTA's tiles.
+//
+// CTA shape: kWorkers workers of 256 threads (8 warps) each.  Warp w of a
+// worker reads TMEM lanes 32*(w%4).. (its TMEM sub-partition) and output half
+// w/4, so each of the 128 vectors of a tile is recombined by two threads.
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -40,23 +52,37 @@
 
 namespace nttb {
 
-__device__ uint32_t g_tc_error;  // bit 0: an mbarrier wait ran out of budget
+// bit 0: an mbarrier wait ran out of budget; bit 1: a stage dependency wait did
+__device__ uint32_t g_tc_error;
 
 namespace {
 
 constexpr uint32_t kMatBytes64 = 64 * 1024;  // DFT-64 byte-plane image (256 rows x 256 B)
 constexpr uint32_t kMatBytes16 = 4 * 1024;   // DFT-16 byte-plane image (64 rows x 64 B)
+constexpr uint32_t kThreads = 256;
+constexpr uint32_t kTilesPerUnit = 8;        // tiles per (poly, limb) per stage
+constexpr uint32_t kWorkers = 1;             // independent tile workers per CTA
+// per worker: A 32 KB, B 64 KB, DFT-16 image 4 KB, generator table 2 KB, 3 mbarriers + ticket
+constexpr size_t kWorkerSmem = 103 * 1024;
+constexpr size_t kSmem = kWorkers * kWorkerSmem + 64 + 1024;
 
 // Device constants of one modulus for one direction.
 struct TcLimb {
     uint32_t q, qinv;        // modulus, -q^-1 mod 2^32
     uint32_t one_m, pad_;    // 2^32 mod q
-    const uint32_t* a_start; // pass A: t_A(b, d) = a_start[b] * a_ratio[b]^d  (Montgomery form)
-    const uint32_t* a_ratio;
-    const uint32_t* b_ratio; // pass B level 1: t_B1(b2, d2) = b_ratio[b2]^d2
-    const uint8_t* mat_a;    // DFT-64 image for pass A
-    const uint8_t* mat_b1;   // DFT-64 image for pass B level 1
-    const uint8_t* mat_b2;   // DFT-16 image for pass B level 2
+    // stage A twiddle t_A(b, d) = a_st2[2b + h] * a_ratio[b]^(d - 32h), d in [32h, 32h + 32)
+    const uint32_t* a_st2;   // 2048 entries (Montgomery form)
+    const uint32_t* a_ratio; // 1024 entries
+    // stage B level-1 twiddle t_B1(b2, d2) = b_st2[2 b2 + h] * b_ratio[b2]^(d2 - 32h)
+    const uint32_t* b_st2;   // 32 entries
+    const uint32_t* b_ratio; // 16 entries
+    // DFT-64 images are generated in shared memory from byte-transposed tables:
+    // gen[a * E + e] packs byte a of (256^p * 2^32 * T[e] mod q) for p = 0..3,
+    // with W[k][j] = T[(j * m_k) mod E], m_k = k (E = 64) or 2k + 1 (E = 128).
+    const uint32_t* gen_a;   // stage A
+    const uint32_t* gen_b1;  // stage B level 1 (E = 64)
+    uint32_t e_a, pad2_;     // stage A table length: 64 (cyclic) or 128 (negacyclic forward)
+    const uint8_t* mat_b2;   // DFT-16 image for stage B level 2 (4 KB, copied as is)
 };
 
 struct Int8Cache {
@@ -64,6 +90,22 @@ struct Int8Cache {
     TcLimb* d_fwd = nullptr;
     TcLimb* d_inv = nullptr;
     void* d_blob = nullptr;
+    uint32_t* d_ctr = nullptr;  // ticket + completion counters
+    size_t ctr_words = 0;
+};
+
+struct StageDesc {
+    const uint32_t* src;
+    uint32_t* dst;
+    const TcLimb* limbs;
+    uint32_t kind;  // 0: stage A, 1: stage B
+    uint32_t pad_;
+};
+
+struct QueueArgs {
+    StageDesc st[4];
+    uint32_t n_stages, n_limbs, units, total;  // units = polys x limbs; total = tiles
+    uint32_t* ctr;                              // [0] ticket, [1 + s * units + u] tiles done
 };
 
 // ---- device arithmetic ------------------------------------------------------------
@@ -73,7 +115,9 @@ __device__ __forceinline__ uint32_t redc64(uint64_t v, uint32_t q, uint32_t qinv
 }
 __device__ __forceinline__ uint32_t combine_redc(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t q,
                                                  uint32_t qinv) {
-    uint64_t v = (uint64_t)c0 + ((uint64_t)c1 << 8) + ((uint64_t)c2 << 16) + ((uint64_t)c3 << 24);
+    uint64_t v = (uint64_t)c1 * 256u + c0;
+    v += (uint64_t)c2 * 65536u;
+    v += (uint64_t)c3 * 16777216u;
     return redc64(v, q, qinv);
 }
 // a < 2q, b < q -> a*b*2^-32 mod q in [0, 2q)
@@ -82,13 +126,20 @@ __device__ __forceinline__ uint32_t mont_lazy(uint32_t a, uint32_t b, uint32_t q
 }
 __device__ __forceinline__ uint32_t canon(uint32_t x, uint32_t q) { return x >= q ? x - q : x; }
 
-__device__ __forceinline__ void flag_timeout() { atomicOr(&g_tc_error, 1u); }
+__device__ __forceinline__ void flag_error(uint32_t bit) { atomicOr(&g_tc_error, bit); }
 
-// Copies `bytes` (multiple of 16) from global to shared with 16-byte loads.
-__device__ __forceinline__ void copy_g2s(uint8_t* s, const uint8_t* g, uint32_t bytes) {
-    const uint4* src = reinterpret_cast<const uint4*>(g);
-    uint4* dst = reinterpret_cast<uint4*>(s);
-    for (uint32_t i = threadIdx.x; i < bytes / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+// Bounded wait until *p >= target (acquire at GPU scope).
+__device__ __forceinline__ bool wait_count(const uint32_t* p, uint32_t target) {
+    for (uint32_t i = 0; i < (1u << 24); i++) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void signal_count(uint32_t* p) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
 }
 
 // Issues the K = 256-byte contraction (8 MMAs of K = 32) into TMEM columns
@@ -107,230 +158,312 @@ __device__ __forceinline__ void issue_k256(uint32_t tmem, const uint8_t* A, uint
     tc::commit(bar);
 }
 
-// ============================================================ pass A (N = 2^16)
-// One CTA: 128 consecutive columns b0.. of one (poly, limb); 128 threads.
-// Input x[a*1024 + b] from `src`; output U[d][b] at (b*64 + d) in `dst`.
-__global__ void __launch_bounds__(128) int8_pass_a_n16(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
-                                                       const TcLimb* __restrict__ limbs, uint32_t n_limbs) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sA = smem;                  // 2 kblocks x 128 rows x 128 B = 32 KB
-    uint8_t* sB = smem + 32768;          // 64 KB
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 32768 + kMatBytes64);  // [0] MMA done, [1] B landed
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 2);
-
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t limb = blockIdx.y, poly = blockIdx.z, b0 = blockIdx.x * 128u;
-    const TcLimb L = limbs[limb];
-    const uint64_t off = ((uint64_t)poly * n_limbs + limb) << 16;
-    const uint32_t* x = src + off;
-    uint32_t* out = dst + off;
-
-    if (warp == 0) tc::tmem_alloc(slot, 256);
-    if (tid == 0) {
-        tc::mbar_init(bar, 1);
-        tc::mbar_init(bar + 1, 1);
-        tc::mbar_expect_tx(bar + 1, kMatBytes64);
-#pragma unroll
-        for (uint32_t i = 0; i < 4; i++) tc::bulk_g2s(sB + i * 16384u, L.mat_a + i * 16384u, 16384u, bar + 1);
-    }
-    // transposed load: vector m = column b0 + m, K index a (4 residues per 16-byte
-    // chunk); all 64 loads are in flight before the first shared-memory store
-    {
-        const uint32_t* col = x + b0 + tid;
-        uint32_t v[64];
-#pragma unroll
-        for (uint32_t a = 0; a < 64; a++) v[a] = __ldg(col + a * 1024u);
-#pragma unroll
-        for (uint32_t c = 0; c < 16; c++)
-            *reinterpret_cast<uint4*>(sA + tc::sw128_offset(tid, 16 * c, 128)) =
-                make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
-    }
-    tc::fence_proxy_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
-    const uint32_t taddr = *slot;
-    if (tid == 0) {
-        if (!tc::mbar_wait_bounded(bar + 1, 0)) flag_timeout();
-        issue_k256(taddr, sA, 128, sB, 256, 256, bar);
-    }
-    __syncwarp();
-    const bool ok = tc::mbar_wait_bounded(bar, 0);
-    tc::fence_after_sync();
-    if (!ok) {
-        if (tid == 0) flag_timeout();
-    } else {
-        const uint32_t q = L.q, qinv = L.qinv;
-        const uint32_t b = b0 + tid;
-        uint32_t tw = L.a_start[b];
-        const uint32_t ratio = L.a_ratio[b];
-        uint4* orow = reinterpret_cast<uint4*>(out + (uint64_t)b * 64u);
-        const uint32_t lane_base = taddr + ((warp * 32u) << 16);
-#pragma unroll 1
-        for (uint32_t dc = 0; dc < 4; dc++) {
-            uint32_t c0[16], c1[16], c2[16], c3[16];
-            tc::ld_32x32b_x16(lane_base + 0 * 64 + dc * 16, c0);
-            tc::ld_32x32b_x16(lane_base + 1 * 64 + dc * 16, c1);
-            tc::ld_32x32b_x16(lane_base + 2 * 64 + dc * 16, c2);
-            tc::ld_32x32b_x16(lane_base + 3 * 64 + dc * 16, c3);
-            tc::ld_wait();
-            uint32_t y[16];
-#pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const uint32_t t = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
-                y[i] = canon(mont_lazy(t, tw, q, qinv), q);
-                tw = canon(mont_lazy(tw, ratio, q, qinv), q);
-            }
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-                orow[dc * 4 + i] = make_uint4(y[4 * i], y[4 * i + 1], y[4 * i + 2], y[4 * i + 3]);
-        }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(taddr, 256);
+// The four 16-column planes (a = 0..3 at columns col + 64a) of this thread's TMEM lane.
+__device__ __forceinline__ void ld_planes64(uint32_t col, uint32_t (&c0)[16], uint32_t (&c1)[16],
+                                            uint32_t (&c2)[16], uint32_t (&c3)[16]) {
+    tc::ld_32x32b_x16(col + 0, c0);
+    tc::ld_32x32b_x16(col + 64, c1);
+    tc::ld_32x32b_x16(col + 128, c2);
+    tc::ld_32x32b_x16(col + 192, c3);
+    tc::ld_wait();
 }
 
-// ============================================================ pass B (N = 2^16)
-// One CTA: 8 rows d0..d0+7 of U (U[d][b] at b*64 + d in `src`).  128 threads.
-// Level 1: vector m = (r = m & 7, b2 = m >> 3), elements a2 at row position
-// a2*16 + b2 -> DFT64 over a2, twiddle b_ratio[b2]^d2 -> A2 (SW64, rows
-// d2*8 + r, K index b2).  Level 2: DFT16 over b2 -> X[d0 + r + 64*d2 + 4096*c2].
-__global__ void __launch_bounds__(128) int8_pass_b_n16(const uint32_t* src, uint32_t* dst,
-                                                       const TcLimb* __restrict__ limbs, uint32_t n_limbs) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sA = smem;                          // level-1 A (32 KB), then level-2 A (32 KB, SW64)
-    uint8_t* sB1 = smem + 32768;                 // 64 KB
-    uint8_t* sB2 = smem + 32768 + kMatBytes64;   // 4 KB
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sB2 + kMatBytes16);  // [0] level 1, [1] level 2, [2] B landed
-    uint32_t* slot = reinterpret_cast<uint32_t*>(bar + 3);
+// Shared state of one persistent CTA.
+struct Ctx {
+    uint8_t* sA;      // 32 KB operand A (stage A / level 1: SW128; level 2: SW64)
+    uint8_t* sB;      // 64 KB DFT-64 image
+    uint8_t* sB2;     // 4 KB DFT-16 image
+    uint32_t* sTab;   // 2 KB generator table
+    uint64_t* bar;    // [1] MMA (level 1), [2] MMA (level 2)
+    uint32_t taddr;   // TMEM base of this worker (256 columns)
+    uint32_t ph_m1, ph_m2;          // mbarrier parities
+    const uint32_t* cached;         // generator table of the image currently in sB
+    uint32_t tid;                   // thread index within the worker (0..255)
+    uint32_t bar_id;                // named barrier of the worker
+};
 
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t limb = blockIdx.y, poly = blockIdx.z, d0 = blockIdx.x * 8u;
-    const TcLimb L = limbs[limb];
-    const uint64_t off = ((uint64_t)poly * n_limbs + limb) << 16;
-    const uint32_t* u = src + off;
-    uint32_t* out = dst + off;
+// Barrier over the 256 threads of one worker.
+__device__ __forceinline__ void wsync(const Ctx& c) {
+    asm volatile("bar.sync %0, %1;" ::"r"(c.bar_id), "r"(kThreads) : "memory");
+}
+
+// Stages the generator table (4 * E words) in shared memory.
+__device__ __forceinline__ void stage_table(Ctx& c, const uint32_t* gtab, uint32_t E) {
+    for (uint32_t i = c.tid; i < 4u * E; i += kThreads) c.sTab[i] = __ldg(gtab + i);
+}
+// Writes the 256-row x 256-byte SW128 DFT-64 image: thread t owns row
+// t = (a, k); its 16-byte chunk cc holds W[k][4cc..4cc+3] byte plane a.
+__device__ __forceinline__ void gen_image64(Ctx& c, uint32_t E) {
+    const uint32_t t = c.tid, a = t >> 6, k = t & 63u;
+    const uint32_t m = (E == 128u) ? 2u * k + 1u : k, mask = E - 1u;
+    const uint32_t* ta = c.sTab + a * E;
+#pragma unroll
+    for (uint32_t cc = 0; cc < 16; cc++) {
+        const uint32_t j = 4u * cc;
+        uint4 w;
+        w.x = ta[(j * m) & mask];
+        w.y = ta[((j + 1u) * m) & mask];
+        w.z = ta[((j + 2u) * m) & mask];
+        w.w = ta[((j + 3u) * m) & mask];
+        *reinterpret_cast<uint4*>(c.sB + tc::sw128_offset(t, 16u * cc, 256)) = w;
+    }
+}
+
+// ---- stage A tile: 128 columns b0.. of one (poly, limb) ------------------------------
+__device__ __forceinline__ void tile_a(Ctx& c, const uint32_t* x, uint32_t* out, const TcLimb& L, uint32_t b0) {
+    const uint32_t tid = c.tid, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t quarter = warp & 3u, half = warp >> 2;
+    const uint32_t b_ep = b0 + quarter * 32u + lane;
     const uint32_t q = L.q, qinv = L.qinv;
-
-    if (warp == 0) tc::tmem_alloc(slot, 256);
-    if (tid == 0) {
-        tc::mbar_init(bar, 1);
-        tc::mbar_init(bar + 1, 1);
-        tc::mbar_init(bar + 2, 1);
-        tc::mbar_expect_tx(bar + 2, kMatBytes64 + kMatBytes16);
+    const uint32_t ratio = L.a_ratio[b_ep];
+    const uint32_t start = L.a_st2[2 * b_ep + half];
+    const uint32_t* gtab = L.gen_a;
+    const uint32_t E = L.e_a;
+    const bool new_img = gtab != c.cached;
+    if (new_img) stage_table(c, gtab, E);
+    {   // transposed load: vector m = column b0 + m, rows a in [32h, 32h + 32);
+        // the image is generated while the loads are in flight
+        const uint32_t m = tid & 127u, h = tid >> 7;
+        const uint32_t* col = x + b0 + m + (32u * h) * 1024u;
+        uint32_t v[32];
 #pragma unroll
-        for (uint32_t i = 0; i < 4; i++) tc::bulk_g2s(sB1 + i * 16384u, L.mat_b1 + i * 16384u, 16384u, bar + 2);
-        tc::bulk_g2s(sB2, L.mat_b2, kMatBytes16, bar + 2);
+        for (uint32_t a = 0; a < 32; a++) v[a] = __ldcg(col + a * 1024u);
+        if (new_img) {
+            wsync(c);
+            gen_image64(c, E);
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < 8; k++)
+            *reinterpret_cast<uint4*>(c.sA + tc::sw128_offset(m, 128u * h + 16u * k, 128)) =
+                make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
     }
-    const uint32_t r = tid & 7u, b2 = tid >> 3;
-    {
-        const uint32_t* base = u + d0 + r;
-        uint32_t v[64];
-#pragma unroll
-        for (uint32_t a2 = 0; a2 < 64; a2++) v[a2] = base[(a2 * 16u + b2) * 64u];
-#pragma unroll
-        for (uint32_t c = 0; c < 16; c++)
-            *reinterpret_cast<uint4*>(sA + tc::sw128_offset(tid, 16 * c, 128)) =
-                make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
-    }
+    c.cached = gtab;
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
-    __syncthreads();
-    const uint32_t taddr = *slot;
-    const uint32_t lane_base = taddr + ((warp * 32u) << 16);
-    if (tid == 0) {
-        if (!tc::mbar_wait_bounded(bar + 2, 0)) flag_timeout();
-        issue_k256(taddr, sA, 128, sB1, 256, 256, bar);
-    }
+    wsync(c);
+    if (tid == 0) issue_k256(c.taddr, c.sA, 128, c.sB, 256, 256, c.bar + 1);
     __syncwarp();
-    bool ok = tc::mbar_wait_bounded(bar, 0);
+    const bool ok = tc::mbar_wait_bounded(c.bar + 1, c.ph_m1);
+    c.ph_m1 ^= 1u;
+    tc::fence_after_sync();
+    if (!ok) {
+        if (lane == 0) flag_error(1u);
+        return;
+    }
+    const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
+    uint32_t tw_e = start;                                      // d = 32h
+    uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
+    uint4* orow = reinterpret_cast<uint4*>(out + (uint64_t)b_ep * 64u + 32u * half);
+    const uint32_t lane_base = c.taddr + ((quarter * 32u) << 16);
+#pragma unroll 1
+    for (uint32_t sub = 0; sub < 2; sub++) {
+        uint32_t c0[16], c1[16], c2[16], c3[16];
+        ld_planes64(lane_base + 32u * half + 16u * sub, c0, c1, c2, c3);
+        uint32_t y[16];
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+            const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
+            const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
+            y[i] = canon(mont_lazy(te, tw_e, q, qinv), q);
+            y[i + 1] = canon(mont_lazy(to, tw_o, q, qinv), q);
+            tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
+            tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            orow[sub * 4 + i] = make_uint4(y[4 * i], y[4 * i + 1], y[4 * i + 2], y[4 * i + 3]);
+    }
+}
+
+// ---- stage B tile: 8 rows d0..d0+7 of U (U[d][b] at b*64 + d) -------------------------
+// Level 1: vector m = (r = m & 7, b2 = m >> 3), elements a2 at row position
+// a2*16 + b2 -> DFT64 over a2, twiddle t_B1 -> A2 (SW64, rows d2*8 + r,
+// K index b2).  Level 2: DFT16 over b2 -> X[d0 + r + 64*d2 + 4096*c2].
+__device__ __forceinline__ void tile_b(Ctx& c, const uint32_t* u, uint32_t* out, const TcLimb& L, uint32_t d0) {
+    const uint32_t tid = c.tid, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t quarter = warp & 3u, h = warp >> 2;
+    const uint32_t mv = quarter * 32u + lane, r_ep = mv & 7u, b2_ep = mv >> 3;
+    const uint32_t q = L.q, qinv = L.qinv;
+    const uint32_t ratio = L.b_ratio[b2_ep];
+    const uint32_t start = L.b_st2[2 * b2_ep + h];
+    const uint32_t* gtab = L.gen_b1;
+    const bool new_img = gtab != c.cached;
+    uint4 img2;
+    if (new_img) {
+        stage_table(c, gtab, 64u);
+        img2 = __ldg(reinterpret_cast<const uint4*>(L.mat_b2) + tid);  // 4 KB = 256 x 16 B
+    }
+    {
+        const uint32_t m = tid & 127u, hh = tid >> 7;
+        const uint32_t r = m & 7u, b2 = m >> 3;
+        const uint32_t* base = u + d0 + r + ((32u * hh) * 16u + b2) * 64u;
+        uint32_t v[32];
+#pragma unroll
+        for (uint32_t a = 0; a < 32; a++) v[a] = __ldcg(base + a * 1024u);
+        if (new_img) {
+            wsync(c);
+            gen_image64(c, 64u);
+            reinterpret_cast<uint4*>(c.sB2)[tid] = img2;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < 8; k++)
+            *reinterpret_cast<uint4*>(c.sA + tc::sw128_offset(m, 128u * hh + 16u * k, 128)) =
+                make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    }
+    c.cached = gtab;
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    wsync(c);
+    const uint32_t lane_base = c.taddr + ((quarter * 32u) << 16);
+    if (tid == 0) issue_k256(c.taddr, c.sA, 128, c.sB, 256, 256, c.bar + 1);
+    __syncwarp();
+    bool ok = tc::mbar_wait_bounded(c.bar + 1, c.ph_m1);
+    c.ph_m1 ^= 1u;
     tc::fence_after_sync();
     if (ok) {
         // level-1 epilogue -> A2 (SW64 layout, 512 rows x 64 B), overwriting level-1 A
-        const uint32_t ratio = L.b_ratio[b2];
-        uint32_t tw = L.one_m;
+        const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
+        uint32_t tw_e = start;
+        uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
 #pragma unroll 1
-        for (uint32_t dc = 0; dc < 4; dc++) {
+        for (uint32_t sub = 0; sub < 2; sub++) {
             uint32_t c0[16], c1[16], c2[16], c3[16];
-            tc::ld_32x32b_x16(lane_base + 0 * 64 + dc * 16, c0);
-            tc::ld_32x32b_x16(lane_base + 1 * 64 + dc * 16, c1);
-            tc::ld_32x32b_x16(lane_base + 2 * 64 + dc * 16, c2);
-            tc::ld_32x32b_x16(lane_base + 3 * 64 + dc * 16, c3);
-            tc::ld_wait();
+            ld_planes64(lane_base + 32u * h + 16u * sub, c0, c1, c2, c3);
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const uint32_t d2 = dc * 16 + i;
-                const uint32_t t = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
-                const uint32_t y = mont_lazy(t, tw, q, qinv);  // [0, 2q): exact input for level 2
-                tw = canon(mont_lazy(tw, ratio, q, qinv), q);
-                *reinterpret_cast<uint32_t*>(sA + tc::sw64_offset(d2 * 8u + r, 4u * b2)) = y;
+            for (int i = 0; i < 16; i += 2) {
+                const uint32_t d2 = 32u * h + 16u * sub + i;
+                const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
+                const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
+                // [0, 2q) values are exact inputs for level 2
+                *reinterpret_cast<uint32_t*>(c.sA + tc::sw64_offset(d2 * 8u + r_ep, 4u * b2_ep)) =
+                    mont_lazy(te, tw_e, q, qinv);
+                *reinterpret_cast<uint32_t*>(c.sA + tc::sw64_offset((d2 + 1u) * 8u + r_ep, 4u * b2_ep)) =
+                    mont_lazy(to, tw_o, q, qinv);
+                tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
+                tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
             }
         }
-    } else if (tid == 0) {
-        flag_timeout();
+    } else if (lane == 0) {
+        flag_error(1u);
     }
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
-    __syncthreads();
+    wsync(c);
     if (ok && tid == 0) {
         tc::fence_after_sync();
         const uint32_t idesc = tc::idesc_u8(128, 64);
-        const uint32_t a0 = tc::smem_u32(sA), bb = tc::smem_u32(sB2);
+        const uint32_t a0 = tc::smem_u32(c.sA), bb = tc::smem_u32(c.sB2);
 #pragma unroll
         for (uint32_t t = 0; t < 4; t++)
 #pragma unroll
             for (uint32_t ks = 0; ks < 2; ks++)
-                tc::mma_i8(taddr + t * 64u, tc::desc_k_sw64(a0 + t * 8192u + ks * 32u),
+                tc::mma_i8(c.taddr + t * 64u, tc::desc_k_sw64(a0 + t * 8192u + ks * 32u),
                            tc::desc_k_sw64(bb + ks * 32u), idesc, ks > 0);
-        tc::commit(bar + 1);
+        tc::commit(c.bar + 2);
     }
     __syncwarp();
-    if (ok) {
-        ok = tc::mbar_wait_bounded(bar + 1, 0);
-        tc::fence_after_sync();
-        if (!ok && tid == 0) flag_timeout();
+    if (!ok) return;
+    ok = tc::mbar_wait_bounded(c.bar + 2, c.ph_m2);
+    c.ph_m2 ^= 1u;
+    tc::fence_after_sync();
+    if (!ok) {
+        if (lane == 0) flag_error(1u);
+        return;
     }
-    if (ok) {
+    // level 2: warp pair h handles M-tiles 2h and 2h + 1
 #pragma unroll 1
-        for (uint32_t t = 0; t < 4; t++) {
-            uint32_t c0[16], c1[16], c2[16], c3[16];
-            const uint32_t col = lane_base + t * 64u;
-            tc::ld_32x32b_x16(col + 0, c0);
-            tc::ld_32x32b_x16(col + 16, c1);
-            tc::ld_32x32b_x16(col + 32, c2);
-            tc::ld_32x32b_x16(col + 48, c3);
-            tc::ld_wait();
-            const uint32_t row2 = t * 128u + tid;
-            const uint32_t d2 = row2 >> 3, rr = row2 & 7u;
-            uint32_t* o = out + d0 + rr + 64u * d2;
+    for (uint32_t tt = 0; tt < 2; tt++) {
+        const uint32_t t = 2u * h + tt;
+        uint32_t c0[16], c1[16], c2[16], c3[16];
+        const uint32_t col = lane_base + t * 64u;
+        tc::ld_32x32b_x16(col + 0, c0);
+        tc::ld_32x32b_x16(col + 16, c1);
+        tc::ld_32x32b_x16(col + 32, c2);
+        tc::ld_32x32b_x16(col + 48, c3);
+        tc::ld_wait();
+        const uint32_t row2 = t * 128u + quarter * 32u + lane;
+        const uint32_t d2 = row2 >> 3, rr = row2 & 7u;
+        uint32_t* o = out + d0 + rr + 64u * d2;
 #pragma unroll
-            for (int c = 0; c < 16; c++)
-                o[4096u * c] = canon(combine_redc(c0[c], c1[c], c2[c], c3[c], q, qinv), q);
-        }
+        for (int k = 0; k < 16; k++) o[4096u * k] = canon(combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv), q);
+    }
+}
+
+// ---- persistent work-queue kernel -------------------------------------------------------
+// One CTA per SM holds kWorkers independent tile workers of 256 threads each
+// (own shared-memory region, TMEM column range, mbarriers, named barrier and
+// ticket stream), so that tiles in different phases overlap on the SM.
+__global__ void __launch_bounds__(kThreads * kWorkers, 1) int8_queue_n16(const __grid_constant__ QueueArgs args) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t worker = threadIdx.x / kThreads;
+    uint8_t* smem = base + worker * kWorkerSmem;
+    Ctx c;
+    c.sA = smem;
+    c.sB = smem + 32768;
+    c.sB2 = smem + 32768 + kMatBytes64;
+    c.sTab = reinterpret_cast<uint32_t*>(c.sB2 + kMatBytes16);
+    c.bar = reinterpret_cast<uint64_t*>(c.sTab + 512);
+    c.tid = threadIdx.x % kThreads;
+    c.bar_id = 1 + worker;
+    uint32_t* slot = reinterpret_cast<uint32_t*>(base + kWorkers * kWorkerSmem);  // CTA-wide TMEM base
+    uint32_t* s_ticket = reinterpret_cast<uint32_t*>(c.bar + 3);
+    const uint32_t tid = c.tid;
+    if (threadIdx.x < 32) tc::tmem_alloc(slot, 256 * kWorkers);
+    if (tid == 0) {
+        tc::mbar_init(c.bar + 1, 1);
+        tc::mbar_init(c.bar + 2, 1);
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(taddr, 256);
+    tc::fence_after_sync();
+    c.taddr = *slot + worker * 256u;
+    c.ph_m1 = c.ph_m2 = 0;
+    c.cached = nullptr;
+    for (;;) {
+        if (tid == 0) *s_ticket = atomicAdd(args.ctr, 1u);
+        wsync(c);
+        const uint32_t t = *s_ticket;
+        if (t >= args.total) break;
+        const uint32_t per_stage = args.units * kTilesPerUnit;
+        const uint32_t s = t / per_stage, rem = t - s * per_stage;
+        const uint32_t unit = rem / kTilesPerUnit, tile = rem % kTilesPerUnit;
+        const uint32_t limb = unit % args.n_limbs;
+        const StageDesc& S = args.st[s];
+        if (s > 0 && tid == 0 && !wait_count(args.ctr + 1 + (s - 1) * args.units + unit, kTilesPerUnit))
+            flag_error(2u);
+        wsync(c);
+        const uint64_t off = (uint64_t)unit << 16;
+        if (S.kind == 0) tile_a(c, S.src + off, S.dst + off, S.limbs[limb], tile * 128u);
+        else tile_b(c, S.src + off, S.dst + off, S.limbs[limb], tile * 8u);
+        __threadfence();
+        tc::fence_before_sync();
+        wsync(c);
+        if (tid == 0) signal_count(args.ctr + 1 + s * args.units + unit);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) tc::tmem_dealloc(*slot, 256 * kWorkers);
 }
-
-constexpr size_t kSmemA = 32768 + kMatBytes64 + 64 + 1024;
-constexpr size_t kSmemB = 32768 + kMatBytes64 + kMatBytes16 + 64 + 1024;
 
 // ---- host: tables and byte-plane images ------------------------------------------------
-// Image of B[(a, k)][(j, p)] = byte a of (256^p * 2^32 * W[k][j] mod q), K-major SW128,
-// 256 rows, two 128-byte K blocks.
-void build_image64(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) {
-    std::memset(img, 0, kMatBytes64);
-    for (uint32_t k = 0; k < 64; k++)
-        for (uint32_t j = 0; j < 64; j++)
-            for (uint32_t p = 0; p < 4; p++) {
-                const uint64_t v = h_mulmod(h_to_mont32(W[k * 64 + j], q), (1ull << (8 * p)) % q, q);
-                for (uint32_t a = 0; a < 4; a++)
-                    img[tc::sw128_offset(a * 64 + k, 4 * j + p, 256)] = (uint8_t)(v >> (8 * a));
-            }
+// The DFT-64 operand B is B[(a, k)][(j, p)] = byte a of (256^p * 2^32 * W[k][j] mod q),
+// K-major SW128, 256 rows, two 128-byte K blocks; gen_image64 writes it on the device.
+// Byte-transposed generator table for DFT-64 images built on the device:
+// g[a*E + e] packs, for p = 0..3 (byte p), byte a of (256^p * 2^32 * root^e mod q).
+void build_gen(uint32_t* g, uint64_t root, uint32_t E, uint64_t q) {
+    uint64_t t = 1;
+    for (uint32_t e = 0; e < E; e++) {
+        uint32_t packed[4] = {0, 0, 0, 0};
+        for (uint32_t p = 0; p < 4; p++) {
+            const uint64_t v = h_mulmod(h_to_mont32(t, q), (1ull << (8 * p)) % q, q);
+            for (uint32_t a = 0; a < 4; a++) packed[a] |= (uint32_t)((v >> (8 * a)) & 255u) << (8 * p);
+        }
+        for (uint32_t a = 0; a < 4; a++) g[a * E + e] = packed[a];
+        t = h_mulmod(t, root, q);
+    }
 }
+
 // Same for a 16-point matrix: 64 rows x 64 bytes, K-major SW64.
 void build_image16(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) {
     std::memset(img, 0, kMatBytes16);
@@ -349,7 +482,7 @@ std::vector<uint64_t> dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t
     std::vector<uint64_t> W((size_t)L * L);
     for (uint32_t k = 0; k < L; k++)
         for (uint32_t j = 0; j < L; j++) {
-            uint64_t v = h_powmod(root, (uint64_t)j * k % (2ull * L * L), q);
+            uint64_t v = h_powmod(root, (uint64_t)j * k, q);
             v = h_mulmod(v, h_powmod(row_twist, k, q), q);
             v = h_mulmod(v, h_powmod(col_twist, j, q), q);
             W[(size_t)k * L + j] = h_mulmod(v, scale, q);
@@ -357,15 +490,33 @@ std::vector<uint64_t> dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t
     return W;
 }
 
+// Twiddle tables of one direction: a_st2 (2048), a_ratio (1024), b_st2 (32), b_ratio (16).
+constexpr size_t kTabWords = 2048 + 1024 + 32 + 16;
+
+void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_t* ratio_a, const uint64_t* ratio_b) {
+    for (uint32_t b = 0; b < 1024; b++) {
+        t[2 * b] = h_to_mont32(start_a[b], q);
+        t[2 * b + 1] = h_to_mont32(h_mulmod(start_a[b], h_powmod(ratio_a[b], 32, q), q), q);
+        t[2048 + b] = h_to_mont32(ratio_a[b], q);
+    }
+    for (uint32_t b2 = 0; b2 < 16; b2++) {
+        t[3072 + 2 * b2] = h_to_mont32(1, q);
+        t[3072 + 2 * b2 + 1] = h_to_mont32(h_powmod(ratio_b[b2], 32, q), q);
+        t[3104 + b2] = h_to_mont32(ratio_b[b2], q);
+    }
+}
+
 int build_cache(Plan32& p, Int8Cache* c) {
     const uint32_t n = p.n, nl = p.n_limbs;
-    // blob layout per limb: 4 DFT-64 images + 2 DFT-16 images + tables
-    const size_t tab_words = 4 * 1024 + 2 * 16;
-    const size_t per_limb = 4 * (size_t)kMatBytes64 + 2 * (size_t)kMatBytes16 + tab_words * 4;
+    // blob layout per limb: 4 generator tables (512 words each: stage A / B1,
+    // forward / inverse) + 2 DFT-16 images + 2 twiddle tables
+    const size_t kGen = 4 * 512 * 4;
+    const size_t per_limb = kGen + 2 * (size_t)kMatBytes16 + 2 * kTabWords * 4;
     std::vector<uint8_t> blob(per_limb * nl);
     uint8_t* d_blob = nullptr;
     if (cudaMalloc(&d_blob, blob.size()) != cudaSuccess) return 4;
     std::vector<TcLimb> fwd(nl), inv(nl);
+    std::vector<uint64_t> st(1024), ra(1024), rb(16);
     for (uint32_t l = 0; l < nl; l++) {
         const LimbHost& H = p.limbs[l];
         const uint64_t q = H.q;
@@ -374,55 +525,61 @@ int build_cache(Plan32& p, Int8Cache* c) {
         const uint64_t w = H.omega, wi = H.omega_inv;
         const uint64_t w64 = h_powmod(w, n / 64, q), w64i = h_powmod(wi, n / 64, q);
         const uint64_t w16 = h_powmod(w, n / 16, q), w16i = h_powmod(wi, n / 16, q);
-        // pass A forward matrix: negacyclic folds psi^(a * n/64) on the input index
-        std::vector<uint64_t> Af = p.negacyclic ? dft_matrix(64, w64, q, 1, h_powmod(H.psi, n / 64, q))
-                                                : dft_matrix(64, w64, q);
-        std::vector<uint64_t> Ai = dft_matrix(64, w64i, q);
-        // pass B level 2 inverse: n^-1 (and psi^-(4096 c2)) folded on the output index
+        // stage A forward: the negacyclic twist psi^(a * n/64) on the input index
+        // makes W[k][j] = psi_128^(j (2k + 1)) (table of 128 powers)
+        uint32_t* gen = reinterpret_cast<uint32_t*>(h);
+        const uint32_t e_af = p.negacyclic ? 128u : 64u;
+        build_gen(gen + 0 * 512, p.negacyclic ? h_powmod(H.psi, n / 64, q) : w64, e_af, q);  // A forward
+        build_gen(gen + 1 * 512, w64i, 64, q);                                                // A inverse
+        build_gen(gen + 2 * 512, w64, 64, q);                                                 // B1 forward
+        build_gen(gen + 3 * 512, w64i, 64, q);                                                // B1 inverse
+        // stage B level 2 inverse: n^-1 (and psi^-(4096 c2)) folded on the output index
         std::vector<uint64_t> B2f = dft_matrix(16, w16, q);
         std::vector<uint64_t> B2i = p.negacyclic ? dft_matrix(16, w16i, q, h_powmod(H.psi_inv, 4096, q), 1, H.n_inv)
                                                  : dft_matrix(16, w16i, q, 1, 1, H.n_inv);
-        build_image64(h + 0 * kMatBytes64, Af, q);
-        build_image64(h + 1 * kMatBytes64, Ai, q);
-        build_image64(h + 2 * kMatBytes64, dft_matrix(64, w64, q), q);  // pass B level 1 forward
-        build_image64(h + 3 * kMatBytes64, Ai, q);                      // pass B level 1 inverse
-        build_image16(h + 4 * kMatBytes64, B2f, q);
-        build_image16(h + 4 * kMatBytes64 + kMatBytes16, B2i, q);
-        uint32_t* tab = reinterpret_cast<uint32_t*>(h + 4 * kMatBytes64 + 2 * kMatBytes16);
-        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + 4 * kMatBytes64 + 2 * kMatBytes16);
-        // pass A twiddles (b < 1024): forward start psi^b (negacyclic) or 1, ratio omega^b;
-        // inverse start 1, ratio omega^-b (times psi^-1 for negacyclic)
+        build_image16(h + kGen, B2f, q);
+        build_image16(h + kGen + kMatBytes16, B2i, q);
+        uint32_t* tab = reinterpret_cast<uint32_t*>(h + kGen + 2 * kMatBytes16);
+        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + kGen + 2 * kMatBytes16);
+        const uint32_t* dgen = reinterpret_cast<const uint32_t*>(d);
+        // forward: t_A(b, d) = psi^b (negacyclic) * omega^(b d); t_B1(b2, d2) = omega^(64 b2 d2)
         for (uint32_t b = 0; b < 1024; b++) {
-            tab[0 * 1024 + b] = h_to_mont32(p.negacyclic ? h_powmod(H.psi, b, q) : 1, q);
-            tab[1 * 1024 + b] = h_to_mont32(h_powmod(w, b, q), q);
-            tab[2 * 1024 + b] = h_to_mont32(1, q);
-            uint64_t ri = h_powmod(wi, b, q);
-            if (p.negacyclic) ri = h_mulmod(ri, H.psi_inv, q);
-            tab[3 * 1024 + b] = h_to_mont32(ri, q);
+            st[b] = p.negacyclic ? h_powmod(H.psi, b, q) : 1;
+            ra[b] = h_powmod(w, b, q);
         }
-        // pass B level-1 ratios (b2 < 16): omega_1024^(+-b2) (times psi^-64 for negacyclic inverse)
+        for (uint32_t b2 = 0; b2 < 16; b2++) rb[b2] = h_powmod(w, 64ull * b2, q);
+        fill_tables(tab, q, st.data(), ra.data(), rb.data());
+        // inverse: t_A(b, d) = omega^-(b d) (* psi^-d); t_B1 = omega^-(64 b2 d2) (* psi^-(64 d2))
+        for (uint32_t b = 0; b < 1024; b++) {
+            st[b] = 1;
+            ra[b] = h_powmod(wi, b, q);
+            if (p.negacyclic) ra[b] = h_mulmod(ra[b], H.psi_inv, q);
+        }
         for (uint32_t b2 = 0; b2 < 16; b2++) {
-            tab[4096 + b2] = h_to_mont32(h_powmod(w, 64ull * b2, q), q);
-            uint64_t ri = h_powmod(wi, 64ull * b2, q);
-            if (p.negacyclic) ri = h_mulmod(ri, h_powmod(H.psi_inv, 64, q), q);
-            tab[4096 + 16 + b2] = h_to_mont32(ri, q);
+            rb[b2] = h_powmod(wi, 64ull * b2, q);
+            if (p.negacyclic) rb[b2] = h_mulmod(rb[b2], h_powmod(H.psi_inv, 64, q), q);
         }
+        fill_tables(tab + kTabWords, q, st.data(), ra.data(), rb.data());
         TcLimb f{}, v{};
         f.q = v.q = (uint32_t)q;
         f.qinv = v.qinv = h_neg_inv32((uint32_t)q);
         f.one_m = v.one_m = h_to_mont32(1, q);
-        f.a_start = dtab;
-        f.a_ratio = dtab + 1024;
-        v.a_start = dtab + 2048;
-        v.a_ratio = dtab + 3072;
-        f.b_ratio = dtab + 4096;
-        v.b_ratio = dtab + 4096 + 16;
-        f.mat_a = d;
-        v.mat_a = d + kMatBytes64;
-        f.mat_b1 = d + 2 * kMatBytes64;
-        v.mat_b1 = d + 3 * kMatBytes64;
-        f.mat_b2 = d + 4 * kMatBytes64;
-        v.mat_b2 = d + 4 * kMatBytes64 + kMatBytes16;
+        f.a_st2 = dtab;
+        f.a_ratio = dtab + 2048;
+        f.b_st2 = dtab + 3072;
+        f.b_ratio = dtab + 3104;
+        v.a_st2 = dtab + kTabWords;
+        v.a_ratio = dtab + kTabWords + 2048;
+        v.b_st2 = dtab + kTabWords + 3072;
+        v.b_ratio = dtab + kTabWords + 3104;
+        f.gen_a = dgen;
+        f.e_a = e_af;
+        v.gen_a = dgen + 512;
+        v.e_a = 64;
+        f.gen_b1 = dgen + 2 * 512;
+        v.gen_b1 = dgen + 3 * 512;
+        f.mat_b2 = d + kGen;
+        v.mat_b2 = d + kGen + kMatBytes16;
         fwd[l] = f;
         inv[l] = v;
     }
@@ -444,6 +601,61 @@ int build_cache(Plan32& p, Int8Cache* c) {
     return 0;
 }
 
+Int8Cache* get_cache(Plan32& p) {
+    auto* c = reinterpret_cast<Int8Cache*>(p.engine_data[1]);
+    if (c) return c;
+    c = new Int8Cache();
+    if (build_cache(p, c)) {
+        delete c;
+        return nullptr;
+    }
+    p.engine_data[1] = c;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(int8_queue_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+        // two CTAs of ~103 KB per SM need the largest shared-memory carveout
+        cudaFuncSetAttribute(int8_queue_n16, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        attr = true;
+    }
+    return c;
+}
+
+int grid_size(uint32_t total) {
+    static int max_blocks = 0;
+    if (!max_blocks) {
+        int dev = 0, sms = 0, occ = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, int8_queue_n16, kThreads * kWorkers, kSmem);
+        // launch-shape knob: CTAs per SM (clamped to the occupancy limit)
+        if (const char* e = std::getenv("NTT_B200_INT8_CTAS_PER_SM")) {
+            const int want = std::atoi(e);
+            if (want > 0 && want < occ) occ = want;
+        }
+        max_blocks = sms * (occ > 0 ? occ : 1);
+    }
+    return (int)((uint32_t)max_blocks < total ? (uint32_t)max_blocks : total);
+}
+
+// Launches the stage list; counters live in the cache and are cleared on the stream.
+int launch_queue(Int8Cache* c, QueueArgs& q, cudaStream_t s) {
+    const size_t words = 1 + (size_t)q.n_stages * q.units;
+    if (c->ctr_words < words) {
+        if (c->d_ctr) cudaFree(c->d_ctr);
+        c->d_ctr = nullptr;
+        c->ctr_words = 0;
+        if (cudaMalloc(&c->d_ctr, words * 4) != cudaSuccess) return 2;
+        c->ctr_words = words;
+    }
+    q.ctr = c->d_ctr;
+    q.total = q.n_stages * q.units * kTilesPerUnit;
+    if (cudaMemsetAsync(c->d_ctr, 0, words * 4, s) != cudaSuccess) return 2;
+    ProfScope prof(q.n_stages == 2 ? "int8_queue_n16_x2" : "int8_queue_n16_x4", s);
+    int8_queue_n16<<<grid_size((q.total + kWorkers - 1) / kWorkers), kThreads * kWorkers, kSmem, s>>>(q);
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
 }  // namespace
 
 bool int8_serves(const Plan32& p, bool src_u64) { return !src_u64 && p.log_n == 16; }
@@ -451,40 +663,42 @@ bool int8_serves(const Plan32& p, bool src_u64) { return !src_u64 && p.log_n == 
 int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                      cudaStream_t s) {
     if (!int8_serves(p, src_u64)) return 1;
-    if (n_polys > 65535 || p.n_limbs > 65535) return 1;
-    auto* c = reinterpret_cast<Int8Cache*>(p.engine_data[1]);
-    if (!c) {
-        c = new Int8Cache();
-        int rc = build_cache(p, c);
-        if (rc) {
-            delete c;
-            return 2;
-        }
-        p.engine_data[1] = c;
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(int8_pass_a_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemA);
-            cudaFuncSetAttribute(int8_pass_b_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemB);
-            attr = true;
-        }
-    }
+    if ((uint64_t)n_polys * p.n_limbs > (1u << 24)) return 1;
+    Int8Cache* c = get_cache(p);
+    if (!c) return 2;
     const uint32_t* in = static_cast<const uint32_t*>(src);
     uint32_t* out = static_cast<uint32_t*>(dst);
     uint32_t* mid = out;
-    if (src == dst) {  // pass A cannot run in place: stage it in the plan's workspace
+    if (src == dst) {  // stage A cannot run in place: stage it in the plan's workspace
         mid = static_cast<uint32_t*>(plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * 4));
         if (!mid) return 2;
     }
     const TcLimb* limbs = inverse ? c->d_inv : c->d_fwd;
-    {
-        ProfScope prof("int8_pass_a_n16", s);
-        int8_pass_a_n16<<<dim3(8, p.n_limbs, n_polys), 128, kSmemA, s>>>(in, mid, limbs, p.n_limbs);
-    }
-    {
-        ProfScope prof("int8_pass_b_n16", s);
-        int8_pass_b_n16<<<dim3(8, p.n_limbs, n_polys), 128, kSmemB, s>>>(mid, out, limbs, p.n_limbs);
-    }
-    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    QueueArgs q{};
+    q.st[0] = {in, mid, limbs, 0, 0};
+    q.st[1] = {mid, out, limbs, 1, 0};
+    q.n_stages = 2;
+    q.n_limbs = p.n_limbs;
+    q.units = n_polys * p.n_limbs;
+    return launch_queue(c, q, s);
+}
+
+int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStream_t s) {
+    if (!int8_serves(p, false)) return 1;
+    if ((uint64_t)n_polys * p.n_limbs > (1u << 24)) return 1;
+    Int8Cache* c = get_cache(p);
+    if (!c) return 2;
+    uint32_t* ws = static_cast<uint32_t*>(plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * 4));
+    if (!ws) return 2;
+    QueueArgs q{};
+    q.st[0] = {data, ws, c->d_fwd, 0, 0};
+    q.st[1] = {ws, data, c->d_fwd, 1, 0};
+    q.st[2] = {data, ws, c->d_inv, 0, 0};
+    q.st[3] = {ws, data, c->d_inv, 1, 0};
+    q.n_stages = 4;
+    q.n_limbs = p.n_limbs;
+    q.units = n_polys * p.n_limbs;
+    return launch_queue(c, q, s);
 }
 
 void int8_release(Plan32* p) {
@@ -492,6 +706,7 @@ void int8_release(Plan32* p) {
     if (!c) return;
     if (c->d_fwd) cudaFree(c->d_fwd);
     if (c->d_blob) cudaFree(c->d_blob);
+    if (c->d_ctr) cudaFree(c->d_ctr);
     delete c;
     p->engine_data[1] = nullptr;
 }

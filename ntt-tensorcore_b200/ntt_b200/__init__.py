@@ -82,6 +82,7 @@ def lib():
         "nttb_rns_transform": (_int, [_vp, _vp, _vp, _u32, _int, _int, _vp]),
         "nttb_rns_pointwise_mul": (_int, [_vp, _vp, _vp, _vp, _u32, _vp]),
         "nttb_rns_transform_noalloc": (_int, [_vp, _vp, _u32, _int, _vp]),
+        "nttb_rns_forward_inverse": (_int, [_vp, _vp, _u32, _int, _vp]),
         "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
@@ -263,6 +264,10 @@ class RnsPlan:
 
     def pointwise_mul(self, out, a, b, n_polys, stream=None):
         _check(lib().nttb_rns_pointwise_mul(self._h, _ptr(out), _ptr(a), _ptr(b), n_polys, _stream(stream)))
+
+    def forward_inverse(self, data, n_polys, engine="auto", stream=None):
+        """Forward then inverse in place (one persistent launch on the INT8 engine)."""
+        _check(lib().nttb_rns_forward_inverse(self._h, _ptr(data), n_polys, _engine(engine), _stream(stream)))
 
     def transform_noalloc(self, data, n_polys, inverse=False, stream=None):
         """In-place transform that allocates no device memory (static scratch;

