@@ -13,30 +13,42 @@
 // The four INT32 accumulator planes of a vector live in one TMEM lane, so one
 // thread recombines them with three shifted adds -- no cross-thread exchange.
 //
-// N = 2^16 (64 x 64 x 16) runs as two stages; data layout [poly][limb][N]:
-//   stage A: for each column b < 1024 of x viewed as [64][1024]:
-//              U[d][b] = DFT64(x[.][b])[d] * t_A(b, d)
-//            stored transposed (U at b*64 + d): each 128-column tile writes one
-//            contiguous 32 KB block.
-//   stage B: for each row d, Z = DFT1024(U[d][.]) as DFT64 (over stride 16,
-//            twiddle t_B1) then DFT16 (contiguous); X[d + 64 k] = Z[k].  A tile
-//            of 8 rows reads and writes exactly the same positions.
+// N = 2^16 (64 x 64 x 16) runs as two stages over x viewed as [64][1024]:
+//   stage A: for each column b, U[d][b] = DFT64(x[.][b])[d] * t_A(b, d).
+//   stage B: for each row d, Z = DFT1024(U[d][.]) as DFT64 over a2 (b = 16 a2
+//            + b2, twiddle t_B1(b2, d2)) then DFT16 over b2; X[d + 64 k] = Z[k].
 // The four-step twiddles are geometric in the output index and are generated
 // in the epilogue: each thread walks two interleaved chains (even and odd
 // outputs, ratio^2 steps) over its 32 outputs.  Negacyclic twists and n^-1
 // are folded into the B matrices and the twiddle tables.
 //
-// Execution: one persistent launch runs a list of stages (one transform = A, B;
-// forward-then-inverse = A, B, A, B).  CTAs draw tiles from a device ticket
-// counter in stage order; a tile of stage s for (poly, limb) first waits,
-// with a bounded spin, until the 8 tiles of stage s-1 of the same (poly, limb)
-// have signalled completion.  Tickets are claimed in order, so every awaited
-// tile belongs to a CTA that is already running: no deadlock.  TMEM, the
-// mbarriers and the last-used B image stay resident across a CTA's tiles.
+// Execution: a cluster of 4 CTAs (one per SM, 512 threads = two 128-vector
+// tiles each) owns one polynomial of one limb -- 256 KB, held in the
+// cluster's distributed shared memory for all stages.  The unit is read from
+// HBM once by stage A of the first transform and written once by stage B of
+// the last.  In between, the four-step transpose is a DSMEM exchange: each
+// epilogue stages its outputs in its own (now free) operand buffer, laid out
+// exactly as the 1 KB pieces of the receivers' next operand buffers, and 64
+// bulk copies per CTA move the pieces, each completing its bytes on the
+// receiver's mbarrier.  A piece for CTA P is staged in the region that P
+// itself overwrites next, so staging never races an outgoing copy.
+// Forward-then-inverse runs four stages on chip.  Clusters are persistent
+// over (poly, limb) units.
 //
-// CTA shape: kWorkers workers of 256 threads (8 warps) each.  Warp w of a
-// worker reads TMEM lanes 32*(w%4).. (its TMEM sub-partition) and output half
-// w/4, so each of the 128 vectors of a tile is recombined by two threads.
+// Operand layouts (K-major, two 128-vector tiles per buffer):
+//   stage A (buffer 0, SW128): row m of tile t holds column b = 128 t + beta(m)
+//     (beta permutes rows so that each source CTA of the B->A exchange owns
+//     whole 8-row atoms), K word a = row of x.
+//   stage B level 1 (buffer 1, SW64, four 64-byte K blocks): row m' = b2 + 16 r
+//     (row d = 8 t + r), K word a2 in block a2 / 16 = the source CTA.
+//   stage B level 2 (in place of level 1, SW64): row r + 8 (d2 / 16) + 32 (d2 % 16),
+//     K word b2.
+//
+// CTA layout: tile w = threadIdx.x / 256 of CTA rank c is tile 2c + w of a
+// stage (columns 128(2c+w).. in stage A, rows 8(2c+w).. in stage B).  Warp
+// v = (threadIdx.x / 32) % 8 of a tile reads TMEM lanes 32*(v%4).. (its TMEM
+// sub-partition) and output half v/4, so each vector is recombined by two
+// threads.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -52,19 +64,29 @@
 
 namespace nttb {
 
-// bit 0: an mbarrier wait ran out of budget; bit 1: a stage dependency wait did
+// bit 0: an mbarrier wait on a local MMA or copy ran out of budget;
+// bit 1: a wait on another CTA of the cluster did
 __device__ uint32_t g_tc_error;
 
 namespace {
 
 constexpr uint32_t kMatBytes64 = 64 * 1024;  // DFT-64 byte-plane image (256 rows x 256 B)
 constexpr uint32_t kMatBytes16 = 4 * 1024;   // DFT-16 byte-plane image (64 rows x 64 B)
-constexpr uint32_t kThreads = 256;
-constexpr uint32_t kTilesPerUnit = 8;        // tiles per (poly, limb) per stage
-constexpr uint32_t kWorkers = 1;             // independent tile workers per CTA
-// per worker: A 32 KB, B 64 KB, DFT-16 image 4 KB, generator table 2 KB, 3 mbarriers + ticket
-constexpr size_t kWorkerSmem = 103 * 1024;
-constexpr size_t kSmem = kWorkers * kWorkerSmem + 64 + 1024;
+constexpr uint32_t kTileBytes = 32 * 1024;   // one 128-vector operand tile (SW128, 256 B rows)
+constexpr uint32_t kClCtas = 4;              // CTAs per cluster
+constexpr uint32_t kClThreads = 512;         // two tiles of 256 threads per CTA
+constexpr uint32_t kGenWords = 512;          // one generator table slot (4 * E words, E <= 128)
+// shared memory map (offsets from a 1024-aligned base)
+constexpr uint32_t kOffBuf0 = 0;                        // operand buffer 0: 2 tiles
+constexpr uint32_t kOffBuf1 = 2 * kTileBytes;           // operand buffer 1: 2 tiles
+constexpr uint32_t kOffImg = 4 * kTileBytes;            // DFT-64 image
+constexpr uint32_t kOffTab = kOffImg + kMatBytes64;     // 4 generator tables (8 KB)
+constexpr uint32_t kOffImg16 = kOffTab + 4 * kGenWords * 4;  // DFT-16 images: forward, inverse
+constexpr uint32_t kLimbConst = 4 * kGenWords * 4 + 2 * kMatBytes16;  // 16 KB per limb, one bulk copy
+constexpr uint32_t kPiece = 1024;            // DSMEM exchange granule
+constexpr uint32_t kBufBytes = 2 * kTileBytes;
+constexpr uint32_t kOffBar = kOffTab + kLimbConst;
+constexpr size_t kClSmem = kOffBar + 128 + 1024;
 
 // Device constants of one modulus for one direction.
 struct TcLimb {
@@ -76,36 +98,33 @@ struct TcLimb {
     // stage B level-1 twiddle t_B1(b2, d2) = b_st2[2 b2 + h] * b_ratio[b2]^(d2 - 32h)
     const uint32_t* b_st2;   // 32 entries
     const uint32_t* b_ratio; // 16 entries
-    // DFT-64 images are generated in shared memory from byte-transposed tables:
-    // gen[a * E + e] packs byte a of (256^p * 2^32 * T[e] mod q) for p = 0..3,
-    // with W[k][j] = T[(j * m_k) mod E], m_k = k (E = 64) or 2k + 1 (E = 128).
-    const uint32_t* gen_a;   // stage A
-    const uint32_t* gen_b1;  // stage B level 1 (E = 64)
-    uint32_t e_a, pad2_;     // stage A table length: 64 (cyclic) or 128 (negacyclic forward)
-    const uint8_t* mat_b2;   // DFT-16 image for stage B level 2 (4 KB, copied as is)
 };
 
 struct Int8Cache {
     uint32_t log_n = 0;
     TcLimb* d_fwd = nullptr;
     TcLimb* d_inv = nullptr;
-    void* d_blob = nullptr;
-    uint32_t* d_ctr = nullptr;  // ticket + completion counters
-    size_t ctr_words = 0;
+    uint8_t* d_blob = nullptr;
+    size_t per_limb = 0;
+    bool negacyclic = false;
 };
 
-struct StageDesc {
-    const uint32_t* src;
-    uint32_t* dst;
-    const TcLimb* limbs;
-    uint32_t kind;  // 0: stage A, 1: stage B
-    uint32_t pad_;
+// One stage of the on-chip stage list.
+struct ClStage {
+    const TcLimb* limbs;  // twiddles of the stage's direction, per limb
+    uint32_t kind;        // 0: stage A (columns), 1: stage B (rows)
+    uint32_t gen;         // generator table slot of the stage's DFT-64 image
+    uint32_t e;           // its length: 64, or 128 (negacyclic forward stage A)
+    uint32_t img16;       // stage B: DFT-16 image 0 (forward) or 1 (inverse)
 };
 
-struct QueueArgs {
-    StageDesc st[4];
-    uint32_t n_stages, n_limbs, units, total;  // units = polys x limbs; total = tiles
-    uint32_t* ctr;                              // [0] ticket, [1 + s * units + u] tiles done
+struct ClArgs {
+    ClStage st[4];
+    const uint32_t* src;    // [units][2^16]
+    uint32_t* dst;          // [units][2^16], may equal src
+    const uint8_t* consts;  // per limb: 4 generator tables, 2 DFT-16 images (kLimbConst bytes)
+    uint64_t const_stride;
+    uint32_t n_stages, n_limbs, units, pad_;
 };
 
 // ---- device arithmetic ------------------------------------------------------------
@@ -113,12 +132,12 @@ __device__ __forceinline__ uint32_t redc64(uint64_t v, uint32_t q, uint32_t qinv
     const uint32_t m = (uint32_t)v * qinv;
     return (uint32_t)((v + (uint64_t)m * q) >> 32);  // [0, 2q) for v < q * 2^32
 }
+// Planes c_a <= 256 * 255^2 (K = 256 byte products), so c0 + 256 c1 and
+// c2 + 256 c3 fit in 32 bits; v = sum_a 256^a c_a < 2^49.
 __device__ __forceinline__ uint32_t combine_redc(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t q,
                                                  uint32_t qinv) {
-    uint64_t v = (uint64_t)c1 * 256u + c0;
-    v += (uint64_t)c2 * 65536u;
-    v += (uint64_t)c3 * 16777216u;
-    return redc64(v, q, qinv);
+    const uint32_t lo = c0 + (c1 << 8), hi = c2 + (c3 << 8);
+    return redc64((uint64_t)lo + ((uint64_t)hi << 16), q, qinv);
 }
 // a < 2q, b < q -> a*b*2^-32 mod q in [0, 2q)
 __device__ __forceinline__ uint32_t mont_lazy(uint32_t a, uint32_t b, uint32_t q, uint32_t qinv) {
@@ -128,34 +147,36 @@ __device__ __forceinline__ uint32_t canon(uint32_t x, uint32_t q) { return x >= 
 
 __device__ __forceinline__ void flag_error(uint32_t bit) { atomicOr(&g_tc_error, bit); }
 
-// Bounded wait until *p >= target (acquire at GPU scope).
-__device__ __forceinline__ bool wait_count(const uint32_t* p, uint32_t target) {
-    for (uint32_t i = 0; i < (1u << 24); i++) {
-        uint32_t v;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-        if (v >= target) return true;
-        __nanosleep(64);
-    }
-    return false;
-}
-__device__ __forceinline__ void signal_count(uint32_t* p) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(p) : "memory");
-}
-
 // Issues the K = 256-byte contraction (8 MMAs of K = 32) into TMEM columns
-// [tmem, tmem + N) and commits to `bar`.
-__device__ __forceinline__ void issue_k256(uint32_t tmem, const uint8_t* A, uint32_t a_rows, const uint8_t* B,
-                                           uint32_t b_rows, uint32_t N, uint64_t* bar) {
-    tc::fence_after_sync();
+// [tmem, tmem + N).  The caller commits.
+__device__ __forceinline__ void issue_k256(uint32_t tmem, uint32_t a0, uint32_t a_rows, uint32_t b0, uint32_t b_rows,
+                                           uint32_t N) {
     const uint32_t idesc = tc::idesc_u8(128, N);
-    const uint32_t a0 = tc::smem_u32(A), b0 = tc::smem_u32(B);
 #pragma unroll
     for (uint32_t ks = 0; ks < 8; ks++) {
         const uint32_t ka = a0 + (ks >> 2) * a_rows * 128u + (ks & 3u) * 32u;
         const uint32_t kb = b0 + (ks >> 2) * b_rows * 128u + (ks & 3u) * 32u;
         tc::mma_i8(tmem, tc::desc_k_sw128(ka), tc::desc_k_sw128(kb), idesc, ks > 0);
     }
-    tc::commit(bar);
+}
+
+// Same contraction with operand A in the stage B level-1 layout: SW64, four
+// 64-byte K blocks of `a_rows` rows each.
+__device__ __forceinline__ void issue_k256_a64(uint32_t tmem, uint32_t a0, uint32_t a_rows, uint32_t b0,
+                                               uint32_t b_rows, uint32_t N) {
+    const uint32_t idesc = tc::idesc_u8(128, N);
+#pragma unroll
+    for (uint32_t ks = 0; ks < 8; ks++) {
+        const uint32_t ka = a0 + (ks >> 1) * a_rows * 64u + (ks & 1u) * 32u;
+        const uint32_t kb = b0 + (ks >> 2) * b_rows * 128u + (ks & 3u) * 32u;
+        tc::mma_i8(tmem, tc::desc_k_sw64(ka), tc::desc_k_sw128(kb), idesc, ks > 0);
+    }
+}
+
+// Column offset (within a 128-column tile) held by stage A operand row m:
+// bits [6][5][4:3][2:0] of m -> bits [6][3][5:4][2:0].
+__device__ __forceinline__ uint32_t beta(uint32_t m) {
+    return ((m >> 3) & 3u) * 16u + ((m >> 5) & 1u) * 8u + (m & 7u) + (m >> 6) * 64u;
 }
 
 // The four 16-column planes (a = 0..3 at columns col + 64a) of this thread's TMEM lane.
@@ -168,287 +189,333 @@ __device__ __forceinline__ void ld_planes64(uint32_t col, uint32_t (&c0)[16], ui
     tc::ld_wait();
 }
 
-// Shared state of one persistent CTA.
-struct Ctx {
-    uint8_t* sA;      // 32 KB operand A (stage A / level 1: SW128; level 2: SW64)
-    uint8_t* sB;      // 64 KB DFT-64 image
-    uint8_t* sB2;     // 4 KB DFT-16 image
-    uint32_t* sTab;   // 2 KB generator table
-    uint64_t* bar;    // [1] MMA (level 1), [2] MMA (level 2)
-    uint32_t taddr;   // TMEM base of this worker (256 columns)
-    uint32_t ph_m1, ph_m2;          // mbarrier parities
-    const uint32_t* cached;         // generator table of the image currently in sB
-    uint32_t tid;                   // thread index within the worker (0..255)
-    uint32_t bar_id;                // named barrier of the worker
-};
-
-// Barrier over the 256 threads of one worker.
-__device__ __forceinline__ void wsync(const Ctx& c) {
-    asm volatile("bar.sync %0, %1;" ::"r"(c.bar_id), "r"(kThreads) : "memory");
-}
-
-// Stages the generator table (4 * E words) in shared memory.
-__device__ __forceinline__ void stage_table(Ctx& c, const uint32_t* gtab, uint32_t E) {
-    for (uint32_t i = c.tid; i < 4u * E; i += kThreads) c.sTab[i] = __ldg(gtab + i);
-}
-// Writes the 256-row x 256-byte SW128 DFT-64 image: thread t owns row
-// t = (a, k); its 16-byte chunk cc holds W[k][4cc..4cc+3] byte plane a.
-__device__ __forceinline__ void gen_image64(Ctx& c, uint32_t E) {
-    const uint32_t t = c.tid, a = t >> 6, k = t & 63u;
+// Writes the 256-row x 256-byte SW128 DFT-64 image from a byte-transposed
+// generator table (tab[a * E + e] packs byte a of 256^p * 2^32 * T[e] mod q,
+// p = 0..3, with W[k][j] = T[(j * m_k) mod E], m_k = k (E = 64) or 2k + 1
+// (E = 128)).  512 threads: row t = (a, k) = tid % 256, chunk half tid / 256.
+__device__ __forceinline__ void gen_image64(uint8_t* img, const uint32_t* tab, uint32_t E, uint32_t tid) {
+    const uint32_t t = tid & 255u, a = t >> 6, k = t & 63u, half = tid >> 8;
     const uint32_t m = (E == 128u) ? 2u * k + 1u : k, mask = E - 1u;
-    const uint32_t* ta = c.sTab + a * E;
+    const uint32_t* ta = tab + a * E;
 #pragma unroll
-    for (uint32_t cc = 0; cc < 16; cc++) {
-        const uint32_t j = 4u * cc;
+    for (uint32_t i = 0; i < 8; i++) {
+        const uint32_t cc = 8u * half + i, j = 4u * cc;
         uint4 w;
         w.x = ta[(j * m) & mask];
         w.y = ta[((j + 1u) * m) & mask];
         w.z = ta[((j + 2u) * m) & mask];
         w.w = ta[((j + 3u) * m) & mask];
-        *reinterpret_cast<uint4*>(c.sB + tc::sw128_offset(t, 16u * cc, 256)) = w;
+        *reinterpret_cast<uint4*>(img + tc::sw128_offset(t, 16u * cc, 256)) = w;
     }
 }
 
-// ---- stage A tile: 128 columns b0.. of one (poly, limb) ------------------------------
-__device__ __forceinline__ void tile_a(Ctx& c, const uint32_t* x, uint32_t* out, const TcLimb& L, uint32_t b0) {
-    const uint32_t tid = c.tid, warp = tid >> 5, lane = tid & 31u;
-    const uint32_t quarter = warp & 3u, half = warp >> 2;
-    const uint32_t b_ep = b0 + quarter * 32u + lane;
+// Shared state of one CTA.
+struct Cl {
+    uint8_t* base;
+    uint32_t rank, tid, w, wt;  // CTA rank in the cluster, thread, tile, thread within tile
+    uint32_t taddr;             // TMEM base (512 columns: tile w at + 256 w)
+    uint64_t* bar;              // [0] MMA, [1] MMA level 2, [2] constants copy,
+                                // [3], [4] inbox of buffer 0 / 1, [5] unit done
+    uint32_t ph_mma, ph_mma2, ph_ld, ph_in0, ph_in1, ph_unit;
+};
+
+__device__ __forceinline__ uint32_t buf_addr(const Cl& c, uint32_t which) {
+    return tc::smem_u32(c.base + (which ? kOffBuf1 : kOffBuf0));
+}
+
+__device__ __forceinline__ void wait_local(uint64_t* bar, uint32_t& ph) {
+    if (!tc::mbar_wait_bounded(bar, ph)) flag_error(1u);
+    ph ^= 1u;
+}
+__device__ __forceinline__ void wait_cluster(uint64_t* bar, uint32_t& ph) {
+    if (!tc::mbar_wait_cluster_bounded(bar, ph)) flag_error(2u);
+    ph ^= 1u;
+}
+// One arrival on barrier `idx` of every CTA of the cluster (thread 0 only).
+__device__ __forceinline__ void arrive_all(const Cl& c, uint32_t idx) {
+    const uint32_t a = tc::smem_u32(c.bar + idx);
+#pragma unroll
+    for (uint32_t r = 0; r < kClCtas; r++) tc::arrive_cluster(tc::mapa(a, r));
+}
+
+// Stage A operand of tile w from HBM: row m = column b = 128(2c+w) + beta(m),
+// elements a (rows of x) -> buffer 0, K-major SW128.
+__device__ __forceinline__ void load_columns(const Cl& c, const uint32_t* x) {
+    const uint32_t m = c.wt & 127u, hh = c.wt >> 7;
+    const uint32_t* col = x + 128u * (2u * c.rank + c.w) + beta(m) + (32u * hh) * 1024u;
+    uint32_t v[32];
+#pragma unroll
+    for (uint32_t a = 0; a < 32; a++) v[a] = __ldcs(col + a * 1024u);
+    uint8_t* t = c.base + kOffBuf0 + c.w * kTileBytes;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; k++)
+        *reinterpret_cast<uint4*>(t + tc::sw128_offset(m, 128u * hh + 16u * k, 128)) =
+            make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+// Stage A epilogue: y_d * t_A(b, d) (in [0, 2q)) for this thread's 32 outputs
+// d, staged in buffer 0 for the A->B exchange.  Output d goes to CTA P = d / 16,
+// tile w' = (d / 8) % 2, level-1 row m' = (b % 16) + 16 (d % 8), K word b / 16
+// (K block = this CTA's rank): piece j = d % 8 of the receiver's K block
+// (rows 16 j..), staged at piece slot (j / 4, 4 (j % 4) + P) of tile w'.
+__device__ __forceinline__ void epilogue_a(const Cl& c, const TcLimb& L) {
+    const uint32_t lane = c.tid & 31u, v = c.wt >> 5, quarter = v & 3u, h = v >> 2;
+    const uint32_t m = quarter * 32u + lane, b = 128u * (2u * c.rank + c.w) + beta(m);
     const uint32_t q = L.q, qinv = L.qinv;
-    const uint32_t ratio = L.a_ratio[b_ep];
-    const uint32_t start = L.a_st2[2 * b_ep + half];
-    const uint32_t* gtab = L.gen_a;
-    const uint32_t E = L.e_a;
-    const bool new_img = gtab != c.cached;
-    if (new_img) stage_table(c, gtab, E);
-    {   // transposed load: vector m = column b0 + m, rows a in [32h, 32h + 32);
-        // the image is generated while the loads are in flight
-        const uint32_t m = tid & 127u, h = tid >> 7;
-        const uint32_t* col = x + b0 + m + (32u * h) * 1024u;
-        uint32_t v[32];
-#pragma unroll
-        for (uint32_t a = 0; a < 32; a++) v[a] = __ldcg(col + a * 1024u);
-        if (new_img) {
-            wsync(c);
-            gen_image64(c, E);
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < 8; k++)
-            *reinterpret_cast<uint4*>(c.sA + tc::sw128_offset(m, 128u * h + 16u * k, 128)) =
-                make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
-    }
-    c.cached = gtab;
-    tc::fence_proxy_async_smem();
-    tc::fence_before_sync();
-    wsync(c);
-    if (tid == 0) issue_k256(c.taddr, c.sA, 128, c.sB, 256, 256, c.bar + 1);
-    __syncwarp();
-    const bool ok = tc::mbar_wait_bounded(c.bar + 1, c.ph_m1);
-    c.ph_m1 ^= 1u;
-    tc::fence_after_sync();
-    if (!ok) {
-        if (lane == 0) flag_error(1u);
-        return;
-    }
+    const uint32_t ratio = L.a_ratio[b];
     const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
-    uint32_t tw_e = start;                                      // d = 32h
+    uint32_t tw_e = L.a_st2[2 * b + h];                         // d = 32h
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
-    uint4* orow = reinterpret_cast<uint4*>(out + (uint64_t)b_ep * 64u + 32u * half);
-    const uint32_t lane_base = c.taddr + ((quarter * 32u) << 16);
+    const uint32_t bl = b & 15u, a2 = (b >> 4) & 15u;
+    // SW64 offset of (row bl, K word a2) inside a 16-row piece
+    const uint32_t inpiece = (bl >> 3) * 512u + (bl & 7u) * 64u + (((a2 >> 2) ^ ((bl >> 1) & 3u)) << 4) + 4u * (a2 & 3u);
+    uint8_t* stage = c.base + kOffBuf0 + inpiece;
+    const uint32_t lane_base = c.taddr + c.w * 256u + ((quarter * 32u) << 16);
 #pragma unroll 1
     for (uint32_t sub = 0; sub < 2; sub++) {
         uint32_t c0[16], c1[16], c2[16], c3[16];
-        ld_planes64(lane_base + 32u * half + 16u * sub, c0, c1, c2, c3);
-        uint32_t y[16];
+        ld_planes64(lane_base + 32u * h + 16u * sub, c0, c1, c2, c3);
+        uint8_t* o = stage + (2u * h + sub) * kPiece;  // P = 2h + sub
 #pragma unroll
-        for (int i = 0; i < 16; i += 2) {
+        for (uint32_t i = 0; i < 16; i += 2) {
             const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
             const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
-            y[i] = canon(mont_lazy(te, tw_e, q, qinv), q);
-            y[i + 1] = canon(mont_lazy(to, tw_o, q, qinv), q);
+            // output i: w' = i / 8, j = i % 8 -> w' * 32 KB + (j / 4) * 16 KB + 4 (j % 4) KB
+            *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u + 4u * (i & 3u) * kPiece) =
+                mont_lazy(te, tw_e, q, qinv);
+            *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u +
+                                         4u * ((i + 1) & 3u) * kPiece) = mont_lazy(to, tw_o, q, qinv);
             tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
             tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
         }
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-            orow[sub * 4 + i] = make_uint4(y[4 * i], y[4 * i + 1], y[4 * i + 2], y[4 * i + 3]);
     }
 }
 
-// ---- stage B tile: 8 rows d0..d0+7 of U (U[d][b] at b*64 + d) -------------------------
-// Level 1: vector m = (r = m & 7, b2 = m >> 3), elements a2 at row position
-// a2*16 + b2 -> DFT64 over a2, twiddle t_B1 -> A2 (SW64, rows d2*8 + r,
-// K index b2).  Level 2: DFT16 over b2 -> X[d0 + r + 64*d2 + 4096*c2].
-__device__ __forceinline__ void tile_b(Ctx& c, const uint32_t* u, uint32_t* out, const TcLimb& L, uint32_t d0) {
-    const uint32_t tid = c.tid, warp = tid >> 5, lane = tid & 31u;
-    const uint32_t quarter = warp & 3u, h = warp >> 2;
-    const uint32_t mv = quarter * 32u + lane, r_ep = mv & 7u, b2_ep = mv >> 3;
+// Stage B level-1 epilogue: row m' = b2 + 16 r, outputs d2; z * t_B1(b2, d2)
+// (in [0, 2q)) -> level-2 operand of the same tile (overwriting level 1):
+// SW64, row r + 8 (d2 / 16) + 32 (d2 % 16), K word b2.
+__device__ __forceinline__ void epilogue_b1(const Cl& c, const TcLimb& L, uint8_t* a2buf) {
+    const uint32_t lane = c.tid & 31u, v = c.wt >> 5, quarter = v & 3u, h = v >> 2;
+    const uint32_t mv = quarter * 32u + lane, b2 = mv & 15u, r = mv >> 4;
     const uint32_t q = L.q, qinv = L.qinv;
-    const uint32_t ratio = L.b_ratio[b2_ep];
-    const uint32_t start = L.b_st2[2 * b2_ep + h];
-    const uint32_t* gtab = L.gen_b1;
-    const bool new_img = gtab != c.cached;
-    uint4 img2;
-    if (new_img) {
-        stage_table(c, gtab, 64u);
-        img2 = __ldg(reinterpret_cast<const uint4*>(L.mat_b2) + tid);  // 4 KB = 256 x 16 B
-    }
-    {
-        const uint32_t m = tid & 127u, hh = tid >> 7;
-        const uint32_t r = m & 7u, b2 = m >> 3;
-        const uint32_t* base = u + d0 + r + ((32u * hh) * 16u + b2) * 64u;
-        uint32_t v[32];
-#pragma unroll
-        for (uint32_t a = 0; a < 32; a++) v[a] = __ldcg(base + a * 1024u);
-        if (new_img) {
-            wsync(c);
-            gen_image64(c, 64u);
-            reinterpret_cast<uint4*>(c.sB2)[tid] = img2;
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < 8; k++)
-            *reinterpret_cast<uint4*>(c.sA + tc::sw128_offset(m, 128u * hh + 16u * k, 128)) =
-                make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
-    }
-    c.cached = gtab;
-    tc::fence_proxy_async_smem();
-    tc::fence_before_sync();
-    wsync(c);
-    const uint32_t lane_base = c.taddr + ((quarter * 32u) << 16);
-    if (tid == 0) issue_k256(c.taddr, c.sA, 128, c.sB, 256, 256, c.bar + 1);
-    __syncwarp();
-    bool ok = tc::mbar_wait_bounded(c.bar + 1, c.ph_m1);
-    c.ph_m1 ^= 1u;
-    tc::fence_after_sync();
-    if (ok) {
-        // level-1 epilogue -> A2 (SW64 layout, 512 rows x 64 B), overwriting level-1 A
-        const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
-        uint32_t tw_e = start;
-        uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
+    const uint32_t ratio = L.b_ratio[b2];
+    const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
+    uint32_t tw_e = L.b_st2[2 * b2 + h];
+    uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
+    // sw64_offset(r + 8 (2h + sub) + 32 i, 4 b2) = off + 512 (2h + sub) + 2048 i
+    const uint32_t off = r * 64u + (((b2 >> 2) ^ ((r >> 1) & 3u)) << 4) + 4u * (b2 & 3u);
+    const uint32_t lane_base = c.taddr + c.w * 256u + ((quarter * 32u) << 16);
 #pragma unroll 1
-        for (uint32_t sub = 0; sub < 2; sub++) {
-            uint32_t c0[16], c1[16], c2[16], c3[16];
-            ld_planes64(lane_base + 32u * h + 16u * sub, c0, c1, c2, c3);
+    for (uint32_t sub = 0; sub < 2; sub++) {
+        uint32_t c0[16], c1[16], c2[16], c3[16];
+        ld_planes64(lane_base + 32u * h + 16u * sub, c0, c1, c2, c3);
+        uint8_t* o = a2buf + off + 512u * (2u * h + sub);
 #pragma unroll
-            for (int i = 0; i < 16; i += 2) {
-                const uint32_t d2 = 32u * h + 16u * sub + i;
-                const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
-                const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
-                // [0, 2q) values are exact inputs for level 2
-                *reinterpret_cast<uint32_t*>(c.sA + tc::sw64_offset(d2 * 8u + r_ep, 4u * b2_ep)) =
-                    mont_lazy(te, tw_e, q, qinv);
-                *reinterpret_cast<uint32_t*>(c.sA + tc::sw64_offset((d2 + 1u) * 8u + r_ep, 4u * b2_ep)) =
-                    mont_lazy(to, tw_o, q, qinv);
-                tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
-                tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
-            }
+        for (uint32_t i = 0; i < 16; i += 2) {
+            const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
+            const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
+            *reinterpret_cast<uint32_t*>(o + 2048u * i) = mont_lazy(te, tw_e, q, qinv);
+            *reinterpret_cast<uint32_t*>(o + 2048u * (i + 1)) = mont_lazy(to, tw_o, q, qinv);
+            tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
+            tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
         }
-    } else if (lane == 0) {
-        flag_error(1u);
     }
-    tc::fence_proxy_async_smem();
-    tc::fence_before_sync();
-    wsync(c);
-    if (ok && tid == 0) {
-        tc::fence_after_sync();
-        const uint32_t idesc = tc::idesc_u8(128, 64);
-        const uint32_t a0 = tc::smem_u32(c.sA), bb = tc::smem_u32(c.sB2);
-#pragma unroll
-        for (uint32_t t = 0; t < 4; t++)
-#pragma unroll
-            for (uint32_t ks = 0; ks < 2; ks++)
-                tc::mma_i8(c.taddr + t * 64u, tc::desc_k_sw64(a0 + t * 8192u + ks * 32u),
-                           tc::desc_k_sw64(bb + ks * 32u), idesc, ks > 0);
-        tc::commit(c.bar + 2);
-    }
-    __syncwarp();
-    if (!ok) return;
-    ok = tc::mbar_wait_bounded(c.bar + 2, c.ph_m2);
-    c.ph_m2 ^= 1u;
-    tc::fence_after_sync();
-    if (!ok) {
-        if (lane == 0) flag_error(1u);
-        return;
-    }
-    // level 2: warp pair h handles M-tiles 2h and 2h + 1
+}
+
+// Stage B level-2 epilogue.  Lane row2 = 128 t2 + 32 quarter + lane holds
+// d2 = 16 (lane / 8) + 4 t2 + quarter, r = lane % 8, outputs c2:
+// X[d + 64 d2 + 4096 c2] with d = 8(2c + w) + r.  The last stage writes HBM
+// (canonical); otherwise X (in [0, 2q)) is staged in buffer 1 for the B->A
+// exchange: element (a, b) goes to CTA P = t2, tile w' = quarter / 2, row
+// 32 g + 8 c + r with g = 2 (quarter % 2) + w, K word a = lane / 8 + 4 c2 --
+// one word of the SW128 atom (g, K block c2 / 8), staged at piece slot
+// w' * 32 + P * 8 + 2 g + c2 / 8 (in KB).
+__device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qinv, uint32_t* gout) {
+    const uint32_t lane = c.tid & 31u, v = c.wt >> 5, quarter = v & 3u, h = v >> 2;
+    const uint32_t lane_base = c.taddr + c.w * 256u + ((quarter * 32u) << 16);
+    const uint32_t r = lane & 7u, d = 8u * (2u * c.rank + c.w) + r;
 #pragma unroll 1
     for (uint32_t tt = 0; tt < 2; tt++) {
-        const uint32_t t = 2u * h + tt;
+        const uint32_t t2 = 2u * h + tt;
         uint32_t c0[16], c1[16], c2[16], c3[16];
-        const uint32_t col = lane_base + t * 64u;
+        const uint32_t col = lane_base + t2 * 64u;
         tc::ld_32x32b_x16(col + 0, c0);
         tc::ld_32x32b_x16(col + 16, c1);
         tc::ld_32x32b_x16(col + 32, c2);
         tc::ld_32x32b_x16(col + 48, c3);
         tc::ld_wait();
-        const uint32_t row2 = t * 128u + quarter * 32u + lane;
-        const uint32_t d2 = row2 >> 3, rr = row2 & 7u;
-        uint32_t* o = out + d0 + rr + 64u * d2;
+        const uint32_t d2 = 16u * (lane >> 3) + 4u * t2 + quarter;
+        if (gout) {
+            uint32_t* o = gout + d + 64u * d2;
 #pragma unroll
-        for (int k = 0; k < 16; k++) o[4096u * k] = canon(combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv), q);
+            for (int k = 0; k < 16; k++)
+                __stcs(o + 4096u * k, canon(combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv), q));
+        } else {
+            const uint32_t g = 2u * (quarter & 1u) + c.w;
+            uint8_t* o = c.base + kOffBuf1 + (quarter >> 1) * kTileBytes + t2 * 8u * kPiece + 2u * g * kPiece +
+                         r * 128u + 4u * (lane >> 3);
+#pragma unroll
+            for (uint32_t k = 0; k < 16; k++)
+                *reinterpret_cast<uint32_t*>(o + (k >> 3) * kPiece + (((k & 7u) ^ r) << 4)) =
+                    combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv);
+        }
     }
 }
 
-// ---- persistent work-queue kernel -------------------------------------------------------
-// One CTA per SM holds kWorkers independent tile workers of 256 threads each
-// (own shared-memory region, TMEM column range, mbarriers, named barrier and
-// ticket stream), so that tiles in different phases overlap on the SM.
-__global__ void __launch_bounds__(kThreads * kWorkers, 1) int8_queue_n16(const __grid_constant__ QueueArgs args) {
+// The 64 piece copies of one exchange (threads 0..63, one each), completing
+// on barrier `bar_idx` of the receiver.
+//   A->B (kind 0): piece (P, w', j) from buffer 0 slot (w', j / 4, 4 (j % 4) + P)
+//     to P's buffer 1, tile w', K block c, rows 16 j.. (offset 8 KB c + 1 KB j).
+//   B->A (kind 1): piece (P, w', g, kb) from buffer 1 slot w' * 32 + P * 8 + 2 g + kb
+//     to P's buffer 0, tile w', K block kb, atom 4 g + c.
+__device__ __forceinline__ void send_pieces(const Cl& c, uint32_t kind, uint32_t bar_idx) {
+    const uint32_t t = c.tid;
+    if (t >= 64) return;
+    const uint32_t P = t >> 4, wp = (t >> 3) & 1u;
+    uint32_t src, dst;
+    if (kind == 0) {
+        const uint32_t j = t & 7u;
+        src = kOffBuf0 + wp * kTileBytes + (j >> 2) * 16384u + (4u * (j & 3u) + P) * kPiece;
+        dst = kOffBuf1 + wp * kTileBytes + c.rank * 8192u + j * kPiece;
+    } else {
+        const uint32_t g = (t >> 1) & 3u, kb = t & 1u;
+        src = kOffBuf1 + wp * kTileBytes + P * 8192u + (2u * g + kb) * kPiece;
+        dst = kOffBuf0 + wp * kTileBytes + kb * 16384u + (4u * g + c.rank) * kPiece;
+    }
+    const uint32_t base = tc::smem_u32(c.base);
+    tc::bulk_s2cluster(tc::mapa(base + dst, P), base + src, kPiece, tc::mapa(tc::smem_u32(c.bar + bar_idx), P));
+}
+
+// ---- the cluster kernel ----------------------------------------------------------------
+// Barriers: [0] MMA, [1] level-2 MMA, [2] per-limb constants copy,
+// [3] buffer 0 inbox, [4] buffer 1 inbox (one arrival: the owner arming the
+// 64 KB the four senders will complete), [5] unit done (one arrival per CTA).
+__global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_constant__ ClArgs args) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const uint32_t worker = threadIdx.x / kThreads;
-    uint8_t* smem = base + worker * kWorkerSmem;
-    Ctx c;
-    c.sA = smem;
-    c.sB = smem + 32768;
-    c.sB2 = smem + 32768 + kMatBytes64;
-    c.sTab = reinterpret_cast<uint32_t*>(c.sB2 + kMatBytes16);
-    c.bar = reinterpret_cast<uint64_t*>(c.sTab + 512);
-    c.tid = threadIdx.x % kThreads;
-    c.bar_id = 1 + worker;
-    uint32_t* slot = reinterpret_cast<uint32_t*>(base + kWorkers * kWorkerSmem);  // CTA-wide TMEM base
-    uint32_t* s_ticket = reinterpret_cast<uint32_t*>(c.bar + 3);
-    const uint32_t tid = c.tid;
-    if (threadIdx.x < 32) tc::tmem_alloc(slot, 256 * kWorkers);
-    if (tid == 0) {
+    Cl c;
+    c.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    c.rank = tc::cluster_rank();
+    c.tid = threadIdx.x;
+    c.w = threadIdx.x >> 8;
+    c.wt = threadIdx.x & 255u;
+    c.bar = reinterpret_cast<uint64_t*>(c.base + kOffBar);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(c.bar + 8);
+    uint8_t* img = c.base + kOffImg;
+    const uint32_t* tab = reinterpret_cast<const uint32_t*>(c.base + kOffTab);
+    const uint32_t img_a = tc::smem_u32(img);
+    const bool four = args.n_stages == 4;
+    if (c.tid < 32) tc::tmem_alloc(slot, 512);
+    if (c.tid == 0) {
+        tc::mbar_init(c.bar + 0, 1);
         tc::mbar_init(c.bar + 1, 1);
         tc::mbar_init(c.bar + 2, 1);
+        tc::mbar_init(c.bar + 3, 1);
+        tc::mbar_init(c.bar + 4, 1);
+        tc::mbar_init(c.bar + 5, kClCtas);
+        // arm the inboxes of the first unit before any peer can send
+        tc::mbar_expect_tx(c.bar + 4, kBufBytes);
+        if (four) tc::mbar_expect_tx(c.bar + 3, kBufBytes);
     }
     tc::fence_before_sync();
     __syncthreads();
+    tc::cluster_sync();  // every CTA's barriers exist and are armed before any remote traffic
     tc::fence_after_sync();
-    c.taddr = *slot + worker * 256u;
-    c.ph_m1 = c.ph_m2 = 0;
-    c.cached = nullptr;
-    for (;;) {
-        if (tid == 0) *s_ticket = atomicAdd(args.ctr, 1u);
-        wsync(c);
-        const uint32_t t = *s_ticket;
-        if (t >= args.total) break;
-        const uint32_t per_stage = args.units * kTilesPerUnit;
-        const uint32_t s = t / per_stage, rem = t - s * per_stage;
-        const uint32_t unit = rem / kTilesPerUnit, tile = rem % kTilesPerUnit;
+    c.taddr = *slot;
+    c.ph_mma = c.ph_mma2 = c.ph_ld = c.ph_in0 = c.ph_in1 = c.ph_unit = 0;
+    uint32_t iter = 0;
+    for (uint32_t unit = tc::cluster_id(); unit < args.units; unit += tc::cluster_count(), iter++) {
         const uint32_t limb = unit % args.n_limbs;
-        const StageDesc& S = args.st[s];
-        if (s > 0 && tid == 0 && !wait_count(args.ctr + 1 + (s - 1) * args.units + unit, kTilesPerUnit))
-            flag_error(2u);
-        wsync(c);
         const uint64_t off = (uint64_t)unit << 16;
-        if (S.kind == 0) tile_a(c, S.src + off, S.dst + off, S.limbs[limb], tile * 128u);
-        else tile_b(c, S.src + off, S.dst + off, S.limbs[limb], tile * 8u);
-        __threadfence();
+        // the previous unit is finished everywhere: peers no longer read their
+        // buffers and every copy out of this CTA's buffers has landed
+        if (iter > 0) wait_cluster(c.bar + 5, c.ph_unit);
+        if (c.tid == 0) {
+            tc::mbar_expect_tx(c.bar + 2, kLimbConst);
+            tc::bulk_g2s(c.base + kOffTab, args.consts + limb * args.const_stride, kLimbConst, c.bar + 2);
+        }
+        load_columns(c, args.src + off);
+        wait_local(c.bar + 2, c.ph_ld);
+        gen_image64(img, tab + args.st[0].gen * kGenWords, args.st[0].e, c.tid);
+        tc::fence_proxy_async_smem();
         tc::fence_before_sync();
-        wsync(c);
-        if (tid == 0) signal_count(args.ctr + 1 + s * args.units + unit);
+        __syncthreads();
+        for (uint32_t s = 0; s < args.n_stages; s++) {
+            const ClStage& S = args.st[s];
+            const bool last = s + 1 == args.n_stages;
+            const uint32_t in = buf_addr(c, s & 1u);
+            if (s > 0) {  // this stage's 64 KB operand arrived from the four CTAs
+                if (s & 1u) wait_cluster(c.bar + 4, c.ph_in1);
+                else wait_cluster(c.bar + 3, c.ph_in0);
+                if (s == 1 && four && c.tid == 0) tc::mbar_expect_tx(c.bar + 4, kBufBytes);  // for stage 3
+            }
+            tc::fence_after_sync();
+            if (c.tid == 0) {
+                if (S.kind == 0) {
+                    issue_k256(c.taddr, in, 128, img_a, 256, 256);
+                    issue_k256(c.taddr + 256u, in + kTileBytes, 128, img_a, 256, 256);
+                } else {
+                    issue_k256_a64(c.taddr, in, 128, img_a, 256, 256);
+                    issue_k256_a64(c.taddr + 256u, in + kTileBytes, 128, img_a, 256, 256);
+                }
+                tc::commit(c.bar + 0);
+            }
+            __syncwarp();
+            wait_local(c.bar + 0, c.ph_mma);
+            tc::fence_after_sync();
+            if (!last && args.st[s + 1].gen != S.gen) {  // the image is free: build the next stage's
+                gen_image64(img, tab + args.st[s + 1].gen * kGenWords, args.st[s + 1].e, c.tid);
+                tc::fence_proxy_async_smem();
+            }
+            const TcLimb& L = S.limbs[limb];
+            if (S.kind == 0) {
+                epilogue_a(c, L);
+            } else {
+                uint8_t* tile = c.base + kOffBuf1 + c.w * kTileBytes;
+                epilogue_b1(c, L, tile);
+                tc::fence_proxy_async_smem();
+                tc::fence_before_sync();
+                __syncthreads();
+                if (c.tid == 0) {
+                    tc::fence_after_sync();
+                    const uint32_t idesc = tc::idesc_u8(128, 64);
+                    const uint32_t bb = tc::smem_u32(c.base + kOffImg16 + S.img16 * kMatBytes16);
+#pragma unroll
+                    for (uint32_t w = 0; w < 2; w++)
+#pragma unroll
+                        for (uint32_t t = 0; t < 4; t++)
+#pragma unroll
+                            for (uint32_t ks = 0; ks < 2; ks++)
+                                tc::mma_i8(c.taddr + w * 256u + t * 64u,
+                                           tc::desc_k_sw64(in + w * kTileBytes + t * 8192u + ks * 32u),
+                                           tc::desc_k_sw64(bb + ks * 32u), idesc, ks > 0);
+                    tc::commit(c.bar + 1);
+                }
+                __syncwarp();
+                wait_local(c.bar + 1, c.ph_mma2);
+                tc::fence_after_sync();
+                if (last && c.tid == 0) {
+                    // this CTA reads its buffers no more in this unit: re-arm the
+                    // inboxes for the next one, then report done to every CTA
+                    tc::mbar_expect_tx(c.bar + 4, kBufBytes);
+                    if (four) tc::mbar_expect_tx(c.bar + 3, kBufBytes);
+                    arrive_all(c, 5);
+                }
+                epilogue_b2(c, L.q, L.qinv, last ? args.dst + off : nullptr);
+            }
+            tc::fence_proxy_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();
+            if (!last) send_pieces(c, S.kind, S.kind == 0 ? 4 : 3);
+        }
     }
+    // the last arrivals aimed at this CTA have landed before it exits
+    if (iter > 0) wait_cluster(c.bar + 5, c.ph_unit);
     tc::fence_before_sync();
     __syncthreads();
-    if (threadIdx.x < 32) tc::tmem_dealloc(*slot, 256 * kWorkers);
+    if (c.tid < 32) tc::tmem_dealloc(c.taddr, 512);
 }
 
 // ---- host: tables and byte-plane images ------------------------------------------------
-// The DFT-64 operand B is B[(a, k)][(j, p)] = byte a of (256^p * 2^32 * W[k][j] mod q),
-// K-major SW128, 256 rows, two 128-byte K blocks; gen_image64 writes it on the device.
 // Byte-transposed generator table for DFT-64 images built on the device:
 // g[a*E + e] packs, for p = 0..3 (byte p), byte a of (256^p * 2^32 * root^e mod q).
 void build_gen(uint32_t* g, uint64_t root, uint32_t E, uint64_t q) {
@@ -464,7 +531,7 @@ void build_gen(uint32_t* g, uint64_t root, uint32_t E, uint64_t q) {
     }
 }
 
-// Same for a 16-point matrix: 64 rows x 64 bytes, K-major SW64.
+// Byte-plane image of a 16-point matrix: 64 rows (a, c) x 64 bytes, K-major SW64.
 void build_image16(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) {
     std::memset(img, 0, kMatBytes16);
     for (uint32_t c = 0; c < 16; c++)
@@ -506,12 +573,13 @@ void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_
     }
 }
 
+// Generator table slots: 0 stage A forward, 1 stage A inverse, 2 stage B
+// level 1 forward, 3 its inverse (same table as slot 1).
 int build_cache(Plan32& p, Int8Cache* c) {
     const uint32_t n = p.n, nl = p.n_limbs;
-    // blob layout per limb: 4 generator tables (512 words each: stage A / B1,
-    // forward / inverse) + 2 DFT-16 images + 2 twiddle tables
-    const size_t kGen = 4 * 512 * 4;
-    const size_t per_limb = kGen + 2 * (size_t)kMatBytes16 + 2 * kTabWords * 4;
+    // blob layout per limb: kLimbConst bytes of device-side constants (4
+    // generator tables + DFT-16 forward / inverse images) then 2 twiddle tables
+    const size_t per_limb = kLimbConst + 2 * kTabWords * 4;
     std::vector<uint8_t> blob(per_limb * nl);
     uint8_t* d_blob = nullptr;
     if (cudaMalloc(&d_blob, blob.size()) != cudaSuccess) return 4;
@@ -528,20 +596,18 @@ int build_cache(Plan32& p, Int8Cache* c) {
         // stage A forward: the negacyclic twist psi^(a * n/64) on the input index
         // makes W[k][j] = psi_128^(j (2k + 1)) (table of 128 powers)
         uint32_t* gen = reinterpret_cast<uint32_t*>(h);
-        const uint32_t e_af = p.negacyclic ? 128u : 64u;
-        build_gen(gen + 0 * 512, p.negacyclic ? h_powmod(H.psi, n / 64, q) : w64, e_af, q);  // A forward
-        build_gen(gen + 1 * 512, w64i, 64, q);                                                // A inverse
-        build_gen(gen + 2 * 512, w64, 64, q);                                                 // B1 forward
-        build_gen(gen + 3 * 512, w64i, 64, q);                                                // B1 inverse
+        build_gen(gen + 0 * kGenWords, p.negacyclic ? h_powmod(H.psi, n / 64, q) : w64, p.negacyclic ? 128 : 64, q);
+        build_gen(gen + 1 * kGenWords, w64i, 64, q);
+        build_gen(gen + 2 * kGenWords, w64, 64, q);
+        build_gen(gen + 3 * kGenWords, w64i, 64, q);
         // stage B level 2 inverse: n^-1 (and psi^-(4096 c2)) folded on the output index
         std::vector<uint64_t> B2f = dft_matrix(16, w16, q);
         std::vector<uint64_t> B2i = p.negacyclic ? dft_matrix(16, w16i, q, h_powmod(H.psi_inv, 4096, q), 1, H.n_inv)
                                                  : dft_matrix(16, w16i, q, 1, 1, H.n_inv);
-        build_image16(h + kGen, B2f, q);
-        build_image16(h + kGen + kMatBytes16, B2i, q);
-        uint32_t* tab = reinterpret_cast<uint32_t*>(h + kGen + 2 * kMatBytes16);
-        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + kGen + 2 * kMatBytes16);
-        const uint32_t* dgen = reinterpret_cast<const uint32_t*>(d);
+        build_image16(h + 4 * kGenWords * 4, B2f, q);
+        build_image16(h + 4 * kGenWords * 4 + kMatBytes16, B2i, q);
+        uint32_t* tab = reinterpret_cast<uint32_t*>(h + kLimbConst);
+        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + kLimbConst);
         // forward: t_A(b, d) = psi^b (negacyclic) * omega^(b d); t_B1(b2, d2) = omega^(64 b2 d2)
         for (uint32_t b = 0; b < 1024; b++) {
             st[b] = p.negacyclic ? h_powmod(H.psi, b, q) : 1;
@@ -572,14 +638,6 @@ int build_cache(Plan32& p, Int8Cache* c) {
         v.a_ratio = dtab + kTabWords + 2048;
         v.b_st2 = dtab + kTabWords + 3072;
         v.b_ratio = dtab + kTabWords + 3104;
-        f.gen_a = dgen;
-        f.e_a = e_af;
-        v.gen_a = dgen + 512;
-        v.e_a = 64;
-        f.gen_b1 = dgen + 2 * 512;
-        v.gen_b1 = dgen + 3 * 512;
-        f.mat_b2 = d + kGen;
-        v.mat_b2 = d + kGen + kMatBytes16;
         fwd[l] = f;
         inv[l] = v;
     }
@@ -597,6 +655,8 @@ int build_cache(Plan32& p, Int8Cache* c) {
     c->d_fwd = d_l;
     c->d_inv = d_l + nl;
     c->d_blob = d_blob;
+    c->per_limb = per_limb;
+    c->negacyclic = p.negacyclic;
     c->log_n = p.log_n;
     return 0;
 }
@@ -610,49 +670,70 @@ Int8Cache* get_cache(Plan32& p) {
         return nullptr;
     }
     p.engine_data[1] = c;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(int8_queue_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-        // two CTAs of ~103 KB per SM need the largest shared-memory carveout
-        cudaFuncSetAttribute(int8_queue_n16, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        attr = true;
-    }
     return c;
 }
 
-int grid_size(uint32_t total) {
-    static int max_blocks = 0;
-    if (!max_blocks) {
-        int dev = 0, sms = 0, occ = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, int8_queue_n16, kThreads * kWorkers, kSmem);
-        // launch-shape knob: CTAs per SM (clamped to the occupancy limit)
-        if (const char* e = std::getenv("NTT_B200_INT8_CTAS_PER_SM")) {
-            const int want = std::atoi(e);
-            if (want > 0 && want < occ) occ = want;
-        }
-        max_blocks = sms * (occ > 0 ? occ : 1);
+ClStage stage(const Int8Cache* c, bool inverse, uint32_t kind) {
+    ClStage s{};
+    s.limbs = inverse ? c->d_inv : c->d_fwd;
+    s.kind = kind;
+    if (kind == 0) {
+        s.gen = inverse ? 1 : 0;
+        s.e = (!inverse && c->negacyclic) ? 128 : 64;
+    } else {
+        // the inverse stage B level-1 table is the inverse stage A table;
+        // cyclic: the forward ones coincide too (slot 0)
+        s.gen = inverse ? 1 : (c->negacyclic ? 2 : 0);
+        s.e = 64;
     }
-    return (int)((uint32_t)max_blocks < total ? (uint32_t)max_blocks : total);
+    s.img16 = inverse ? 1 : 0;
+    return s;
 }
 
-// Launches the stage list; counters live in the cache and are cleared on the stream.
-int launch_queue(Int8Cache* c, QueueArgs& q, cudaStream_t s) {
-    const size_t words = 1 + (size_t)q.n_stages * q.units;
-    if (c->ctr_words < words) {
-        if (c->d_ctr) cudaFree(c->d_ctr);
-        c->d_ctr = nullptr;
-        c->ctr_words = 0;
-        if (cudaMalloc(&c->d_ctr, words * 4) != cudaSuccess) return 2;
-        c->ctr_words = words;
+void launch_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, uint32_t clusters, cudaStream_t s) {
+    std::memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3(kClCtas * clusters);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.dynamicSmemBytes = kClSmem;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+}
+
+// Clusters of 4 that fit on the device at once (one CTA per SM).
+int max_clusters() {
+    static int cached = 0;
+    if (cached) return cached;
+    cudaFuncSetAttribute(int8_cluster_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem);
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute attr[1];
+    launch_config(cfg, attr, 1, 0);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, int8_cluster_n16, &cfg) != cudaSuccess || n < 1) {
+        cudaGetLastError();
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        n = sms / (int)kClCtas / 2 > 0 ? sms / (int)kClCtas / 2 : 1;
     }
-    q.ctr = c->d_ctr;
-    q.total = q.n_stages * q.units * kTilesPerUnit;
-    if (cudaMemsetAsync(c->d_ctr, 0, words * 4, s) != cudaSuccess) return 2;
-    ProfScope prof(q.n_stages == 2 ? "int8_queue_n16_x2" : "int8_queue_n16_x4", s);
-    int8_queue_n16<<<grid_size((q.total + kWorkers - 1) / kWorkers), kThreads * kWorkers, kSmem, s>>>(q);
+    cached = n;
+    return cached;
+}
+
+int launch_stages(Int8Cache* c, ClArgs& a, cudaStream_t s) {
+    const uint32_t mc = (uint32_t)max_clusters();
+    const uint32_t clusters = a.units < mc ? a.units : mc;
+    a.consts = c->d_blob;
+    a.const_stride = c->per_limb;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute attr[1];
+    launch_config(cfg, attr, clusters, s);
+    ProfScope prof(a.n_stages == 2 ? "int8_cluster_n16_x2" : "int8_cluster_n16_x4", s);
+    if (cudaLaunchKernelEx(&cfg, int8_cluster_n16, a) != cudaSuccess) return 2;
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
@@ -666,21 +747,15 @@ int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32
     if ((uint64_t)n_polys * p.n_limbs > (1u << 24)) return 1;
     Int8Cache* c = get_cache(p);
     if (!c) return 2;
-    const uint32_t* in = static_cast<const uint32_t*>(src);
-    uint32_t* out = static_cast<uint32_t*>(dst);
-    uint32_t* mid = out;
-    if (src == dst) {  // stage A cannot run in place: stage it in the plan's workspace
-        mid = static_cast<uint32_t*>(plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * 4));
-        if (!mid) return 2;
-    }
-    const TcLimb* limbs = inverse ? c->d_inv : c->d_fwd;
-    QueueArgs q{};
-    q.st[0] = {in, mid, limbs, 0, 0};
-    q.st[1] = {mid, out, limbs, 1, 0};
-    q.n_stages = 2;
-    q.n_limbs = p.n_limbs;
-    q.units = n_polys * p.n_limbs;
-    return launch_queue(c, q, s);
+    ClArgs a{};
+    a.st[0] = stage(c, inverse, 0);
+    a.st[1] = stage(c, inverse, 1);
+    a.n_stages = 2;
+    a.src = static_cast<const uint32_t*>(src);
+    a.dst = static_cast<uint32_t*>(dst);
+    a.n_limbs = p.n_limbs;
+    a.units = n_polys * p.n_limbs;
+    return launch_stages(c, a, s);
 }
 
 int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStream_t s) {
@@ -688,17 +763,17 @@ int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStre
     if ((uint64_t)n_polys * p.n_limbs > (1u << 24)) return 1;
     Int8Cache* c = get_cache(p);
     if (!c) return 2;
-    uint32_t* ws = static_cast<uint32_t*>(plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * 4));
-    if (!ws) return 2;
-    QueueArgs q{};
-    q.st[0] = {data, ws, c->d_fwd, 0, 0};
-    q.st[1] = {ws, data, c->d_fwd, 1, 0};
-    q.st[2] = {data, ws, c->d_inv, 0, 0};
-    q.st[3] = {ws, data, c->d_inv, 1, 0};
-    q.n_stages = 4;
-    q.n_limbs = p.n_limbs;
-    q.units = n_polys * p.n_limbs;
-    return launch_queue(c, q, s);
+    ClArgs a{};
+    a.st[0] = stage(c, false, 0);
+    a.st[1] = stage(c, false, 1);
+    a.st[2] = stage(c, true, 0);
+    a.st[3] = stage(c, true, 1);
+    a.n_stages = 4;
+    a.src = data;
+    a.dst = data;
+    a.n_limbs = p.n_limbs;
+    a.units = n_polys * p.n_limbs;
+    return launch_stages(c, a, s);
 }
 
 void int8_release(Plan32* p) {
@@ -706,7 +781,6 @@ void int8_release(Plan32* p) {
     if (!c) return;
     if (c->d_fwd) cudaFree(c->d_fwd);
     if (c->d_blob) cudaFree(c->d_blob);
-    if (c->d_ctr) cudaFree(c->d_ctr);
     delete c;
     p->engine_data[1] = nullptr;
 }

@@ -91,6 +91,24 @@ def test_forward_inverse_one_call(torch_cuda, engine, n_polys):
     assert (y.astype(np.uint64) == ref).all()
 
 
+@pytest.mark.parametrize("engine", ["int8", "dmma"])
+def test_many_units_per_launch(torch_cuda, engine):
+    """3 polynomials x 24 limbs = 72 (poly, limb) units: more units than the
+    INT8 engine runs at once, so its persistent clusters each take several
+    units in turn.  Every limb of every polynomial is checked."""
+    lg, n_polys = 16, 3
+    x = rand_batch(n_polys, PRIMES17, 1 << lg, 72)
+    plan = nb.RnsPlan(lg, PRIMES17, negacyclic=True)
+    y = run(torch_cuda, plan, x, False, engine, out_of_place=True)
+    ref = O.rns(x.astype(np.uint64), PRIMES17, negacyclic=True)
+    assert (y.astype(np.uint64) == ref).all(), int((y.astype(np.uint64) != ref).sum())
+    d = to_dev(torch_cuda, x.reshape(-1))
+    plan.forward_inverse(d, n_polys, engine=engine)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint32).reshape(x.shape) == x).all()
+    assert nb.device_errors() == 0
+
+
 @pytest.mark.parametrize("engine", ["scalar", "auto"])
 def test_large_n_roundtrip_and_spotcheck(torch_cuda, engine):
     lg = 20
