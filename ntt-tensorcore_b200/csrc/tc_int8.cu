@@ -20,7 +20,10 @@
 // The four-step twiddles are geometric in the output index and are generated
 // in the epilogue: each thread walks two interleaved chains (even and odd
 // outputs, ratio^2 steps) over its 32 outputs.  Negacyclic twists and n^-1
-// are folded into the B matrices and the twiddle tables.
+// are folded into the B matrices and the twiddle tables.  The DFT-64 images
+// (rows ordered (k / 32, a, k % 32) so that each half of the outputs is one
+// N = 128 MMA) are precomputed per modulus and bulk-copied into shared
+// memory while the previous stage's epilogue runs.
 //
 // Execution: a cluster of 4 CTAs (one per SM, 512 threads = two 128-vector
 // tiles each) owns one polynomial of one limb -- 256 KB, held in the
@@ -75,18 +78,18 @@ constexpr uint32_t kMatBytes16 = 4 * 1024;   // DFT-16 byte-plane image (64 rows
 constexpr uint32_t kTileBytes = 32 * 1024;   // one 128-vector operand tile (SW128, 256 B rows)
 constexpr uint32_t kClCtas = 4;              // CTAs per cluster
 constexpr uint32_t kClThreads = 512;         // two tiles of 256 threads per CTA
-constexpr uint32_t kGenWords = 512;          // one generator table slot (4 * E words, E <= 128)
 // shared memory map (offsets from a 1024-aligned base)
 constexpr uint32_t kOffBuf0 = 0;                        // operand buffer 0: 2 tiles
 constexpr uint32_t kOffBuf1 = 2 * kTileBytes;           // operand buffer 1: 2 tiles
 constexpr uint32_t kOffImg = 4 * kTileBytes;            // DFT-64 image
-constexpr uint32_t kOffTab = kOffImg + kMatBytes64;     // 4 generator tables (8 KB)
-constexpr uint32_t kOffImg16 = kOffTab + 4 * kGenWords * 4;  // DFT-16 images: forward, inverse
-constexpr uint32_t kLimbConst = 4 * kGenWords * 4 + 2 * kMatBytes16;  // 16 KB per limb, one bulk copy
+constexpr uint32_t kOffImg16 = kOffImg + kMatBytes64;   // DFT-16 images: forward, inverse
+constexpr uint32_t kOffBar = kOffImg16 + 2 * kMatBytes16;
+constexpr size_t kClSmem = kOffBar + 256 + 1024;
 constexpr uint32_t kPiece = 1024;            // DSMEM exchange granule
 constexpr uint32_t kBufBytes = 2 * kTileBytes;
-constexpr uint32_t kOffBar = kOffTab + kLimbConst;
-constexpr size_t kClSmem = kOffBar + 128 + 1024;
+// per-limb device blob: DFT-16 images (8 KB), 3 DFT-64 images, twiddle tables
+constexpr uint32_t kImgSlots = 3;            // 0: stage A forward, 1: inverse (A and B), 2: stage B forward
+constexpr uint32_t kBlobImg = 2 * kMatBytes16;
 
 // Device constants of one modulus for one direction.
 struct TcLimb {
@@ -113,16 +116,16 @@ struct Int8Cache {
 struct ClStage {
     const TcLimb* limbs;  // twiddles of the stage's direction, per limb
     uint32_t kind;        // 0: stage A (columns), 1: stage B (rows)
-    uint32_t gen;         // generator table slot of the stage's DFT-64 image
-    uint32_t e;           // its length: 64, or 128 (negacyclic forward stage A)
+    uint32_t img;         // DFT-64 image slot of the stage
     uint32_t img16;       // stage B: DFT-16 image 0 (forward) or 1 (inverse)
+    uint32_t pad_;
 };
 
 struct ClArgs {
     ClStage st[4];
     const uint32_t* src;    // [units][2^16]
     uint32_t* dst;          // [units][2^16], may equal src
-    const uint8_t* consts;  // per limb: 4 generator tables, 2 DFT-16 images (kLimbConst bytes)
+    const uint8_t* consts;  // per limb: 2 DFT-16 images, 3 DFT-64 images
     uint64_t const_stride;
     uint32_t n_stages, n_limbs, units, pad_;
 };
@@ -179,52 +182,45 @@ __device__ __forceinline__ uint32_t beta(uint32_t m) {
     return ((m >> 3) & 3u) * 16u + ((m >> 5) & 1u) * 8u + (m & 7u) + (m >> 6) * 64u;
 }
 
-// The four 16-column planes (a = 0..3 at columns col + 64a) of this thread's TMEM lane.
-__device__ __forceinline__ void ld_planes64(uint32_t col, uint32_t (&c0)[16], uint32_t (&c1)[16],
-                                            uint32_t (&c2)[16], uint32_t (&c3)[16]) {
-    tc::ld_32x32b_x16(col + 0, c0);
-    tc::ld_32x32b_x16(col + 64, c1);
-    tc::ld_32x32b_x16(col + 128, c2);
-    tc::ld_32x32b_x16(col + 192, c3);
+// Eight outputs' four planes (a = 0..3 at columns col + 32a) of this thread's
+// TMEM lane (one N = 128 output half: columns a * 32 + k % 32).
+__device__ __forceinline__ void ld_planes8(uint32_t col, uint32_t (&c0)[8], uint32_t (&c1)[8], uint32_t (&c2)[8],
+                                           uint32_t (&c3)[8]) {
+    tc::ld_32x32b_x8(col + 0, c0);
+    tc::ld_32x32b_x8(col + 32, c1);
+    tc::ld_32x32b_x8(col + 64, c2);
+    tc::ld_32x32b_x8(col + 96, c3);
     tc::ld_wait();
-}
-
-// Writes the 256-row x 256-byte SW128 DFT-64 image from a byte-transposed
-// generator table (tab[a * E + e] packs byte a of 256^p * 2^32 * T[e] mod q,
-// p = 0..3, with W[k][j] = T[(j * m_k) mod E], m_k = k (E = 64) or 2k + 1
-// (E = 128)).  512 threads: row t = (a, k) = tid % 256, chunk half tid / 256.
-__device__ __forceinline__ void gen_image64(uint8_t* img, const uint32_t* tab, uint32_t E, uint32_t tid) {
-    const uint32_t t = tid & 255u, a = t >> 6, k = t & 63u, half = tid >> 8;
-    const uint32_t m = (E == 128u) ? 2u * k + 1u : k, mask = E - 1u;
-    const uint32_t* ta = tab + a * E;
-#pragma unroll
-    for (uint32_t i = 0; i < 8; i++) {
-        const uint32_t cc = 8u * half + i, j = 4u * cc;
-        uint4 w;
-        w.x = ta[(j * m) & mask];
-        w.y = ta[((j + 1u) * m) & mask];
-        w.z = ta[((j + 2u) * m) & mask];
-        w.w = ta[((j + 3u) * m) & mask];
-        *reinterpret_cast<uint4*>(img + tc::sw128_offset(t, 16u * cc, 256)) = w;
-    }
 }
 
 // Shared state of one CTA.
 struct Cl {
     uint8_t* base;
     uint32_t rank, tid, w, wt;  // CTA rank in the cluster, thread, tile, thread within tile
+    uint32_t quarter, h, lane;  // TMEM sub-partition, output half, lane of this thread's warp
     uint32_t taddr;             // TMEM base (512 columns: tile w at + 256 w)
-    uint64_t* bar;              // [0] MMA, [1] MMA level 2, [2] constants copy,
-                                // [3], [4] inbox of buffer 0 / 1, [5] unit done
-    uint32_t ph_mma, ph_mma2, ph_ld, ph_in0, ph_in1, ph_unit;
+    uint64_t* bar;
 };
+// Barriers (shared memory, after the images):
+//   [0, 1]  MMA of tile 0 / 1 (N = 256), issued in that order
+//   [4, 5]  level-2 MMA of tile 0 / 1
+//   [6]     per-unit constants (DFT-16 images + first DFT-64 image)
+//   [7]     DFT-64 image of the next stage
+//   [8, 9]  buffer 0 / 1 inbox: one arrival (the owner arming the 64 KB its
+//           four senders complete)
+//   [10]    unit done: one arrival per CTA of the cluster
+constexpr uint32_t kBarMma = 0, kBarMma2 = 4, kBarConst = 6, kBarImg = 7, kBarIn0 = 8, kBarIn1 = 9, kBarUnit = 10;
 
 __device__ __forceinline__ uint32_t buf_addr(const Cl& c, uint32_t which) {
     return tc::smem_u32(c.base + (which ? kOffBuf1 : kOffBuf0));
 }
 
-__device__ __forceinline__ void wait_local(uint64_t* bar, uint32_t& ph) {
+// Bounded waits; the phase bit is advanced by the caller.
+__device__ __forceinline__ void wait_parity(uint64_t* bar, uint32_t ph) {
     if (!tc::mbar_wait_bounded(bar, ph)) flag_error(1u);
+}
+__device__ __forceinline__ void wait_local(uint64_t* bar, uint32_t& ph) {
+    wait_parity(bar, ph);
     ph ^= 1u;
 }
 __device__ __forceinline__ void wait_cluster(uint64_t* bar, uint32_t& ph) {
@@ -236,6 +232,12 @@ __device__ __forceinline__ void arrive_all(const Cl& c, uint32_t idx) {
     const uint32_t a = tc::smem_u32(c.bar + idx);
 #pragma unroll
     for (uint32_t r = 0; r < kClCtas; r++) tc::arrive_cluster(tc::mapa(a, r));
+}
+// DFT-64 image `slot` of the unit's limb -> shared memory (thread 0), 4 x 16 KB.
+__device__ __forceinline__ void copy_image(const Cl& c, const uint8_t* limb_blob, uint32_t slot, uint64_t* bar) {
+    const uint8_t* src = limb_blob + kBlobImg + (size_t)slot * kMatBytes64;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++) tc::bulk_g2s(c.base + kOffImg + k * 16384u, src + k * 16384u, 16384u, bar);
 }
 
 // Stage A operand of tile w from HBM: row m = column b = 128(2c+w) + beta(m),
@@ -253,125 +255,153 @@ __device__ __forceinline__ void load_columns(const Cl& c, const uint32_t* x) {
             make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
 }
 
-// Stage A epilogue: y_d * t_A(b, d) (in [0, 2q)) for this thread's 32 outputs
-// d, staged in buffer 0 for the A->B exchange.  Output d goes to CTA P = d / 16,
+// TMEM columns of this thread's lane for its tile and output half.
+__device__ __forceinline__ uint32_t lane_cols(const Cl& c) {
+    return c.taddr + c.w * 256u + c.h * 128u + ((c.quarter * 32u) << 16);
+}
+
+// The epilogues run in two parts of 16 outputs.  `gate` runs between the
+// first part's arithmetic and its stores: it waits until the shared memory
+// the stores overwrite is no longer read by the tensor core.
+
+// Stage A epilogue: y_d * t_A(b, d) in [0, 2q) for outputs d = 32h + i,
+// staged in buffer 0 for the A->B exchange.  Output d goes to CTA P = d / 16,
 // tile w' = (d / 8) % 2, level-1 row m' = (b % 16) + 16 (d % 8), K word b / 16
 // (K block = this CTA's rank): piece j = d % 8 of the receiver's K block
 // (rows 16 j..), staged at piece slot (j / 4, 4 (j % 4) + P) of tile w'.
-__device__ __forceinline__ void epilogue_a(const Cl& c, const TcLimb& L) {
-    const uint32_t lane = c.tid & 31u, v = c.wt >> 5, quarter = v & 3u, h = v >> 2;
-    const uint32_t m = quarter * 32u + lane, b = 128u * (2u * c.rank + c.w) + beta(m);
+template <class Gate, class PartDone>
+__device__ __forceinline__ void epilogue_a(const Cl& c, const TcLimb& L, Gate gate, PartDone part_done) {
+    const uint32_t m = c.quarter * 32u + c.lane, b = 128u * (2u * c.rank + c.w) + beta(m);
     const uint32_t q = L.q, qinv = L.qinv;
     const uint32_t ratio = L.a_ratio[b];
     const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
-    uint32_t tw_e = L.a_st2[2 * b + h];                         // d = 32h
+    uint32_t tw_e = L.a_st2[2 * b + c.h];                       // d = 32h
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
+    const uint32_t col = lane_cols(c);
     const uint32_t bl = b & 15u, a2 = (b >> 4) & 15u;
     // SW64 offset of (row bl, K word a2) inside a 16-row piece
     const uint32_t inpiece = (bl >> 3) * 512u + (bl & 7u) * 64u + (((a2 >> 2) ^ ((bl >> 1) & 3u)) << 4) + 4u * (a2 & 3u);
-    uint8_t* stage = c.base + kOffBuf0 + inpiece;
-    const uint32_t lane_base = c.taddr + c.w * 256u + ((quarter * 32u) << 16);
-#pragma unroll 1
-    for (uint32_t sub = 0; sub < 2; sub++) {
-        uint32_t c0[16], c1[16], c2[16], c3[16];
-        ld_planes64(lane_base + 32u * h + 16u * sub, c0, c1, c2, c3);
-        uint8_t* o = stage + (2u * h + sub) * kPiece;  // P = 2h + sub
 #pragma unroll
-        for (uint32_t i = 0; i < 16; i += 2) {
-            const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
-            const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
-            // output i: w' = i / 8, j = i % 8 -> w' * 32 KB + (j / 4) * 16 KB + 4 (j % 4) KB
-            *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u + 4u * (i & 3u) * kPiece) =
-                mont_lazy(te, tw_e, q, qinv);
-            *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u +
-                                         4u * ((i + 1) & 3u) * kPiece) = mont_lazy(to, tw_o, q, qinv);
-            tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
-            tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+    for (uint32_t part = 0; part < 2; part++) {
+        uint32_t y[16];
+#pragma unroll
+        for (uint32_t sub = 0; sub < 2; sub++) {
+            uint32_t c0[8], c1[8], c2[8], c3[8];
+            ld_planes8(col + 16u * part + 8u * sub, c0, c1, c2, c3);
+#pragma unroll
+            for (uint32_t i = 0; i < 8; i += 2) {
+                y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
+                y[8 * sub + i + 1] =
+                    mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
+                tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
+                tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+            }
         }
+        if (part == 0) gate();
+        // d = 32h + 16 part + i: P = 2h + part, w' = i / 8, j = i % 8
+        uint8_t* o = c.base + kOffBuf0 + inpiece + (2u * c.h + part) * kPiece;
+#pragma unroll
+        for (uint32_t i = 0; i < 16; i++)
+            *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u + 4u * (i & 3u) * kPiece) =
+                y[i];
+        part_done(part);
     }
 }
 
-// Stage B level-1 epilogue: row m' = b2 + 16 r, outputs d2; z * t_B1(b2, d2)
-// (in [0, 2q)) -> level-2 operand of the same tile (overwriting level 1):
-// SW64, row r + 8 (d2 / 16) + 32 (d2 % 16), K word b2.
-__device__ __forceinline__ void epilogue_b1(const Cl& c, const TcLimb& L, uint8_t* a2buf) {
-    const uint32_t lane = c.tid & 31u, v = c.wt >> 5, quarter = v & 3u, h = v >> 2;
-    const uint32_t mv = quarter * 32u + lane, b2 = mv & 15u, r = mv >> 4;
+// Stage B level-1 epilogue: row m' = b2 + 16 r, outputs d2 = 32h + i;
+// z * t_B1(b2, d2) in [0, 2q) -> level-2 operand of the same tile (over
+// level 1), SW64, row r + 8 (d2 / 16) + 32 (d2 % 16), K word b2.
+template <class Gate>
+__device__ __forceinline__ void epilogue_b1(const Cl& c, const TcLimb& L, Gate gate) {
+    const uint32_t mv = c.quarter * 32u + c.lane, b2 = mv & 15u, r = mv >> 4;
     const uint32_t q = L.q, qinv = L.qinv;
     const uint32_t ratio = L.b_ratio[b2];
     const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
-    uint32_t tw_e = L.b_st2[2 * b2 + h];
+    uint32_t tw_e = L.b_st2[2 * b2 + c.h];
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
-    // sw64_offset(r + 8 (2h + sub) + 32 i, 4 b2) = off + 512 (2h + sub) + 2048 i
+    const uint32_t col = lane_cols(c);
+    // sw64_offset(r + 8 (2h + part) + 32 i, 4 b2) = off + 512 (2h + part) + 2048 i
     const uint32_t off = r * 64u + (((b2 >> 2) ^ ((r >> 1) & 3u)) << 4) + 4u * (b2 & 3u);
-    const uint32_t lane_base = c.taddr + c.w * 256u + ((quarter * 32u) << 16);
-#pragma unroll 1
-    for (uint32_t sub = 0; sub < 2; sub++) {
-        uint32_t c0[16], c1[16], c2[16], c3[16];
-        ld_planes64(lane_base + 32u * h + 16u * sub, c0, c1, c2, c3);
-        uint8_t* o = a2buf + off + 512u * (2u * h + sub);
 #pragma unroll
-        for (uint32_t i = 0; i < 16; i += 2) {
-            const uint32_t te = combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
-            const uint32_t to = combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv);
-            *reinterpret_cast<uint32_t*>(o + 2048u * i) = mont_lazy(te, tw_e, q, qinv);
-            *reinterpret_cast<uint32_t*>(o + 2048u * (i + 1)) = mont_lazy(to, tw_o, q, qinv);
-            tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
-            tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+    for (uint32_t part = 0; part < 2; part++) {
+        uint32_t y[16];
+#pragma unroll
+        for (uint32_t sub = 0; sub < 2; sub++) {
+            uint32_t c0[8], c1[8], c2[8], c3[8];
+            ld_planes8(col + 16u * part + 8u * sub, c0, c1, c2, c3);
+#pragma unroll
+            for (uint32_t i = 0; i < 8; i += 2) {
+                y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
+                y[8 * sub + i + 1] =
+                    mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
+                tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
+                tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+            }
         }
+        if (part == 0) gate();
+        uint8_t* o = c.base + kOffBuf1 + c.w * kTileBytes + off + 512u * (2u * c.h + part);
+#pragma unroll
+        for (uint32_t i = 0; i < 16; i++) *reinterpret_cast<uint32_t*>(o + 2048u * i) = y[i];
     }
 }
 
-// Stage B level-2 epilogue.  Lane row2 = 128 t2 + 32 quarter + lane holds
-// d2 = 16 (lane / 8) + 4 t2 + quarter, r = lane % 8, outputs c2:
-// X[d + 64 d2 + 4096 c2] with d = 8(2c + w) + r.  The last stage writes HBM
-// (canonical); otherwise X (in [0, 2q)) is staged in buffer 1 for the B->A
+// Stage B level-2 epilogue.  Lane row2 = 128 t2 + 32 quarter + lane
+// (t2 = 2h + part) holds d2 = 16 (lane / 8) + 4 t2 + quarter, r = lane % 8,
+// outputs c2: X[d + 64 d2 + 4096 c2], d = 8(2c + w) + r, in [0, 2q).  The last
+// stage writes HBM (canonical); otherwise X is staged in buffer 1 for the B->A
 // exchange: element (a, b) goes to CTA P = t2, tile w' = quarter / 2, row
 // 32 g + 8 c + r with g = 2 (quarter % 2) + w, K word a = lane / 8 + 4 c2 --
 // one word of the SW128 atom (g, K block c2 / 8), staged at piece slot
 // w' * 32 + P * 8 + 2 g + c2 / 8 (in KB).
-__device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qinv, uint32_t* gout) {
-    const uint32_t lane = c.tid & 31u, v = c.wt >> 5, quarter = v & 3u, h = v >> 2;
-    const uint32_t lane_base = c.taddr + c.w * 256u + ((quarter * 32u) << 16);
-    const uint32_t r = lane & 7u, d = 8u * (2u * c.rank + c.w) + r;
-#pragma unroll 1
-    for (uint32_t tt = 0; tt < 2; tt++) {
-        const uint32_t t2 = 2u * h + tt;
-        uint32_t c0[16], c1[16], c2[16], c3[16];
-        const uint32_t col = lane_base + t2 * 64u;
-        tc::ld_32x32b_x16(col + 0, c0);
-        tc::ld_32x32b_x16(col + 16, c1);
-        tc::ld_32x32b_x16(col + 32, c2);
-        tc::ld_32x32b_x16(col + 48, c3);
-        tc::ld_wait();
-        const uint32_t d2 = 16u * (lane >> 3) + 4u * t2 + quarter;
+template <class Gate, class PartDone>
+__device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qinv, uint32_t* gout, Gate gate,
+                                            PartDone part_done) {
+    const uint32_t base = c.taddr + c.w * 256u + ((c.quarter * 32u) << 16);
+    const uint32_t r = c.lane & 7u, d = 8u * (2u * c.rank + c.w) + r;
+#pragma unroll
+    for (uint32_t part = 0; part < 2; part++) {
+        const uint32_t t2 = 2u * c.h + part;
+        uint32_t y[16];
+#pragma unroll
+        for (uint32_t sub = 0; sub < 2; sub++) {
+            const uint32_t col = base + t2 * 64u + 8u * sub;
+            uint32_t c0[8], c1[8], c2[8], c3[8];
+            tc::ld_32x32b_x8(col + 0, c0);
+            tc::ld_32x32b_x8(col + 16, c1);
+            tc::ld_32x32b_x8(col + 32, c2);
+            tc::ld_32x32b_x8(col + 48, c3);
+            tc::ld_wait();
+#pragma unroll
+            for (uint32_t k = 0; k < 8; k++) y[8 * sub + k] = combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv);
+        }
         if (gout) {
+            const uint32_t d2 = 16u * (c.lane >> 3) + 4u * t2 + c.quarter;
             uint32_t* o = gout + d + 64u * d2;
 #pragma unroll
-            for (int k = 0; k < 16; k++)
-                __stcs(o + 4096u * k, canon(combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv), q));
+            for (uint32_t k = 0; k < 16; k++) __stcs(o + 4096u * k, canon(y[k], q));
         } else {
-            const uint32_t g = 2u * (quarter & 1u) + c.w;
-            uint8_t* o = c.base + kOffBuf1 + (quarter >> 1) * kTileBytes + t2 * 8u * kPiece + 2u * g * kPiece +
-                         r * 128u + 4u * (lane >> 3);
+            if (part == 0) gate();
+            const uint32_t g = 2u * (c.quarter & 1u) + c.w;
+            uint8_t* o = c.base + kOffBuf1 + (c.quarter >> 1) * kTileBytes + t2 * 8u * kPiece + 2u * g * kPiece +
+                         r * 128u + 4u * (c.lane >> 3);
 #pragma unroll
             for (uint32_t k = 0; k < 16; k++)
-                *reinterpret_cast<uint32_t*>(o + (k >> 3) * kPiece + (((k & 7u) ^ r) << 4)) =
-                    combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv);
+                *reinterpret_cast<uint32_t*>(o + (k >> 3) * kPiece + (((k & 7u) ^ r) << 4)) = y[k];
+            part_done(part);
         }
     }
 }
 
-// The 64 piece copies of one exchange (threads 0..63, one each), completing
-// on barrier `bar_idx` of the receiver.
-//   A->B (kind 0): piece (P, w', j) from buffer 0 slot (w', j / 4, 4 (j % 4) + P)
+// The 16 piece copies of one exchange bound for CTA P (lanes 0..15 of the
+// calling warp, one each), completing on barrier `bar_idx` of P.
+//   A->B (kind 0): piece (w', j) from buffer 0 slot (w', j / 4, 4 (j % 4) + P)
 //     to P's buffer 1, tile w', K block c, rows 16 j.. (offset 8 KB c + 1 KB j).
-//   B->A (kind 1): piece (P, w', g, kb) from buffer 1 slot w' * 32 + P * 8 + 2 g + kb
+//   B->A (kind 1): piece (w', g, kb) from buffer 1 slot w' * 32 + P * 8 + 2 g + kb
 //     to P's buffer 0, tile w', K block kb, atom 4 g + c.
-__device__ __forceinline__ void send_pieces(const Cl& c, uint32_t kind, uint32_t bar_idx) {
-    const uint32_t t = c.tid;
-    if (t >= 64) return;
-    const uint32_t P = t >> 4, wp = (t >> 3) & 1u;
+__device__ __forceinline__ void send_pieces(const Cl& c, uint32_t kind, uint32_t P, uint32_t bar_idx) {
+    const uint32_t t = c.lane;
+    if (t >= 16) return;
+    const uint32_t wp = t >> 3;
     uint32_t src, dst;
     if (kind == 0) {
         const uint32_t j = t & 7u;
@@ -387,9 +417,6 @@ __device__ __forceinline__ void send_pieces(const Cl& c, uint32_t kind, uint32_t
 }
 
 // ---- the cluster kernel ----------------------------------------------------------------
-// Barriers: [0] MMA, [1] level-2 MMA, [2] per-limb constants copy,
-// [3] buffer 0 inbox, [4] buffer 1 inbox (one arrival: the owner arming the
-// 64 KB the four senders will complete), [5] unit done (one arrival per CTA).
 __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_constant__ ClArgs args) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     Cl c;
@@ -398,137 +425,161 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
     c.tid = threadIdx.x;
     c.w = threadIdx.x >> 8;
     c.wt = threadIdx.x & 255u;
+    c.lane = threadIdx.x & 31u;
+    c.quarter = (c.wt >> 5) & 3u;
+    c.h = c.wt >> 7;
     c.bar = reinterpret_cast<uint64_t*>(c.base + kOffBar);
-    uint32_t* slot = reinterpret_cast<uint32_t*>(c.bar + 8);
-    uint8_t* img = c.base + kOffImg;
-    const uint32_t* tab = reinterpret_cast<const uint32_t*>(c.base + kOffTab);
-    const uint32_t img_a = tc::smem_u32(img);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(c.bar + 12);
+    const uint32_t img_a = tc::smem_u32(c.base + kOffImg);
     const bool four = args.n_stages == 4;
+    // the per-unit constants and operand: for the first unit, fetched before
+    // the cluster start-up barrier
+    auto fetch_unit = [&](uint32_t unit) {
+        const uint8_t* limb_blob = args.consts + (unit % args.n_limbs) * args.const_stride;
+        if (c.tid == 0) {
+            tc::mbar_expect_tx(c.bar + kBarConst, kBlobImg + kMatBytes64);
+            tc::bulk_g2s(c.base + kOffImg16, limb_blob, kBlobImg, c.bar + kBarConst);
+            copy_image(c, limb_blob, args.st[0].img, c.bar + kBarConst);
+        }
+        load_columns(c, args.src + ((uint64_t)unit << 16));
+    };
     if (c.tid < 32) tc::tmem_alloc(slot, 512);
     if (c.tid == 0) {
-        tc::mbar_init(c.bar + 0, 1);
-        tc::mbar_init(c.bar + 1, 1);
-        tc::mbar_init(c.bar + 2, 1);
-        tc::mbar_init(c.bar + 3, 1);
-        tc::mbar_init(c.bar + 4, 1);
-        tc::mbar_init(c.bar + 5, kClCtas);
+        for (uint32_t i = 0; i <= kBarUnit; i++) tc::mbar_init(c.bar + i, i == kBarUnit ? kClCtas : 1);
         // arm the inboxes of the first unit before any peer can send
-        tc::mbar_expect_tx(c.bar + 4, kBufBytes);
-        if (four) tc::mbar_expect_tx(c.bar + 3, kBufBytes);
+        tc::mbar_expect_tx(c.bar + kBarIn1, kBufBytes);
+        if (four) tc::mbar_expect_tx(c.bar + kBarIn0, kBufBytes);
     }
+    if (tc::cluster_id() < args.units) fetch_unit(tc::cluster_id());
     tc::fence_before_sync();
     __syncthreads();
     tc::cluster_sync();  // every CTA's barriers exist and are armed before any remote traffic
     tc::fence_after_sync();
     c.taddr = *slot;
-    c.ph_mma = c.ph_mma2 = c.ph_ld = c.ph_in0 = c.ph_in1 = c.ph_unit = 0;
+    uint32_t ph_mma = 0, ph_mma2 = 0, ph_ld = 0, ph_img = 0, ph_in0 = 0, ph_in1 = 0, ph_unit = 0;
     uint32_t iter = 0;
     for (uint32_t unit = tc::cluster_id(); unit < args.units; unit += tc::cluster_count(), iter++) {
         const uint32_t limb = unit % args.n_limbs;
         const uint64_t off = (uint64_t)unit << 16;
-        // the previous unit is finished everywhere: peers no longer read their
-        // buffers and every copy out of this CTA's buffers has landed
-        if (iter > 0) wait_cluster(c.bar + 5, c.ph_unit);
-        if (c.tid == 0) {
-            tc::mbar_expect_tx(c.bar + 2, kLimbConst);
-            tc::bulk_g2s(c.base + kOffTab, args.consts + limb * args.const_stride, kLimbConst, c.bar + 2);
+        const uint8_t* limb_blob = args.consts + limb * args.const_stride;
+        if (iter > 0) {
+            // the previous unit is finished everywhere: peers no longer read their
+            // buffers and every copy out of this CTA's buffers has landed
+            wait_cluster(c.bar + kBarUnit, ph_unit);
+            fetch_unit(unit);
         }
-        load_columns(c, args.src + off);
-        wait_local(c.bar + 2, c.ph_ld);
-        gen_image64(img, tab + args.st[0].gen * kGenWords, args.st[0].e, c.tid);
+        wait_local(c.bar + kBarConst, ph_ld);
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();
+        bool img_pending = false;  // thread 0: a next-stage image copy is in flight
         for (uint32_t s = 0; s < args.n_stages; s++) {
             const ClStage& S = args.st[s];
             const bool last = s + 1 == args.n_stages;
+            const bool next_img = !last && args.st[s + 1].img != S.img;
             const uint32_t in = buf_addr(c, s & 1u);
             if (s > 0) {  // this stage's 64 KB operand arrived from the four CTAs
-                if (s & 1u) wait_cluster(c.bar + 4, c.ph_in1);
-                else wait_cluster(c.bar + 3, c.ph_in0);
-                if (s == 1 && four && c.tid == 0) tc::mbar_expect_tx(c.bar + 4, kBufBytes);  // for stage 3
+                if (s & 1u) wait_cluster(c.bar + kBarIn1, ph_in1);
+                else wait_cluster(c.bar + kBarIn0, ph_in0);
+                if (s == 1 && four && c.tid == 0) tc::mbar_expect_tx(c.bar + kBarIn1, kBufBytes);  // stage 3
             }
-            tc::fence_after_sync();
             if (c.tid == 0) {
-                if (S.kind == 0) {
-                    issue_k256(c.taddr, in, 128, img_a, 256, 256);
-                    issue_k256(c.taddr + 256u, in + kTileBytes, 128, img_a, 256, 256);
-                } else {
-                    issue_k256_a64(c.taddr, in, 128, img_a, 256, 256);
-                    issue_k256_a64(c.taddr + 256u, in + kTileBytes, 128, img_a, 256, 256);
+                if (img_pending) wait_local(c.bar + kBarImg, ph_img);
+                img_pending = false;
+                tc::fence_after_sync();
+#pragma unroll
+                for (uint32_t w = 0; w < 2; w++) {
+                    if (S.kind == 0) issue_k256(c.taddr + w * 256u, in + w * kTileBytes, 128, img_a, 256, 256);
+                    else issue_k256_a64(c.taddr + w * 256u, in + w * kTileBytes, 128, img_a, 256, 256);
+                    tc::commit(c.bar + kBarMma + w);
                 }
-                tc::commit(c.bar + 0);
             }
             __syncwarp();
-            wait_local(c.bar + 0, c.ph_mma);
+            wait_parity(c.bar + kBarMma + c.w, ph_mma);
             tc::fence_after_sync();
-            if (!last && args.st[s + 1].gen != S.gen) {  // the image is free: build the next stage's
-                gen_image64(img, tab + args.st[s + 1].gen * kGenWords, args.st[s + 1].e, c.tid);
-                tc::fence_proxy_async_smem();
-            }
             const TcLimb& L = S.limbs[limb];
+            // before the first stores: the MMAs reading the overwritten operand
+            // are done; thread 0 then fetches the next stage's image
+            auto mma_gate = [&]() {
+                if (S.kind == 0 || (c.tid == 0 && next_img)) wait_parity(c.bar + kBarMma + 1, ph_mma);
+                if (c.tid == 0 && next_img) {
+                    tc::mbar_expect_tx(c.bar + kBarImg, kMatBytes64);
+                    copy_image(c, limb_blob, args.st[s + 1].img, c.bar + kBarImg);
+                    img_pending = true;
+                }
+            };
+            // after each part's stores: the 256 threads of output half h have
+            // staged every piece for CTA 2h + part, and one warp sends them
+            auto part_done = [&](uint32_t part) {
+                if (last) return;
+                tc::fence_proxy_async_smem();
+                asm volatile("bar.sync %0, %1;" ::"r"(3u + c.h), "r"(256u) : "memory");
+                if (c.w == 0 && c.quarter == 0)
+                    send_pieces(c, S.kind, 2u * c.h + part, S.kind == 0 ? kBarIn1 : kBarIn0);
+            };
             if (S.kind == 0) {
-                epilogue_a(c, L);
+                epilogue_a(c, L, mma_gate, part_done);
+                ph_mma ^= 1u;
             } else {
-                uint8_t* tile = c.base + kOffBuf1 + c.w * kTileBytes;
-                epilogue_b1(c, L, tile);
+                epilogue_b1(c, L, mma_gate);
+                ph_mma ^= 1u;
                 tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
-                __syncthreads();
-                if (c.tid == 0) {
+                asm volatile("bar.sync %0, %1;" ::"r"(1u + c.w), "r"(256u) : "memory");
+                if (c.wt == 0) {
                     tc::fence_after_sync();
                     const uint32_t idesc = tc::idesc_u8(128, 64);
                     const uint32_t bb = tc::smem_u32(c.base + kOffImg16 + S.img16 * kMatBytes16);
 #pragma unroll
-                    for (uint32_t w = 0; w < 2; w++)
+                    for (uint32_t t = 0; t < 4; t++)
 #pragma unroll
-                        for (uint32_t t = 0; t < 4; t++)
-#pragma unroll
-                            for (uint32_t ks = 0; ks < 2; ks++)
-                                tc::mma_i8(c.taddr + w * 256u + t * 64u,
-                                           tc::desc_k_sw64(in + w * kTileBytes + t * 8192u + ks * 32u),
-                                           tc::desc_k_sw64(bb + ks * 32u), idesc, ks > 0);
-                    tc::commit(c.bar + 1);
+                        for (uint32_t ks = 0; ks < 2; ks++)
+                            tc::mma_i8(c.taddr + c.w * 256u + t * 64u,
+                                       tc::desc_k_sw64(in + c.w * kTileBytes + t * 8192u + ks * 32u),
+                                       tc::desc_k_sw64(bb + ks * 32u), idesc, ks > 0);
+                    tc::commit(c.bar + kBarMma2 + c.w);
                 }
                 __syncwarp();
-                wait_local(c.bar + 1, c.ph_mma2);
+                wait_parity(c.bar + kBarMma2 + c.w, ph_mma2);
                 tc::fence_after_sync();
-                if (last && c.tid == 0) {
-                    // this CTA reads its buffers no more in this unit: re-arm the
-                    // inboxes for the next one, then report done to every CTA
-                    tc::mbar_expect_tx(c.bar + 4, kBufBytes);
-                    if (four) tc::mbar_expect_tx(c.bar + 3, kBufBytes);
-                    arrive_all(c, 5);
-                }
-                epilogue_b2(c, L.q, L.qinv, last ? args.dst + off : nullptr);
+                // staging overwrites both tiles' level-2 operands
+                epilogue_b2(c, L.q, L.qinv, last ? args.dst + off : nullptr,
+                            [&]() { wait_parity(c.bar + kBarMma2 + (c.w ^ 1u), ph_mma2); }, part_done);
+                ph_mma2 ^= 1u;
             }
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
-            if (!last) send_pieces(c, S.kind, S.kind == 0 ? 4 : 3);
+            if (last && c.tid == 0) {
+                // this CTA reads its buffers no more in this unit: re-arm the
+                // inboxes for the next one, then report done to every CTA
+                tc::mbar_expect_tx(c.bar + kBarIn1, kBufBytes);
+                if (four) tc::mbar_expect_tx(c.bar + kBarIn0, kBufBytes);
+                arrive_all(c, kBarUnit);
+            }
         }
     }
     // the last arrivals aimed at this CTA have landed before it exits
-    if (iter > 0) wait_cluster(c.bar + 5, c.ph_unit);
+    if (iter > 0) wait_cluster(c.bar + kBarUnit, ph_unit);
     tc::fence_before_sync();
     __syncthreads();
     if (c.tid < 32) tc::tmem_dealloc(c.taddr, 512);
 }
 
 // ---- host: tables and byte-plane images ------------------------------------------------
-// Byte-transposed generator table for DFT-64 images built on the device:
-// g[a*E + e] packs, for p = 0..3 (byte p), byte a of (256^p * 2^32 * root^e mod q).
-void build_gen(uint32_t* g, uint64_t root, uint32_t E, uint64_t q) {
-    uint64_t t = 1;
-    for (uint32_t e = 0; e < E; e++) {
-        uint32_t packed[4] = {0, 0, 0, 0};
-        for (uint32_t p = 0; p < 4; p++) {
-            const uint64_t v = h_mulmod(h_to_mont32(t, q), (1ull << (8 * p)) % q, q);
-            for (uint32_t a = 0; a < 4; a++) packed[a] |= (uint32_t)((v >> (8 * a)) & 255u) << (8 * p);
-        }
-        for (uint32_t a = 0; a < 4; a++) g[a * E + e] = packed[a];
-        t = h_mulmod(t, root, q);
-    }
+// Byte-plane image of a 64-point matrix: B[(a, k)][(j, p)] = byte a of
+// (256^p * 2^32 * W[k][j] mod q), K-major SW128, 256 rows ordered
+// (k / 32, a, k % 32) so that rows 128 h.. are the four planes of outputs
+// 32 h.. (one N = 128 MMA per output half).
+void build_image64(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) {
+    std::memset(img, 0, kMatBytes64);
+    for (uint32_t k = 0; k < 64; k++)
+        for (uint32_t j = 0; j < 64; j++)
+            for (uint32_t p = 0; p < 4; p++) {
+                const uint64_t v = h_mulmod(h_to_mont32(W[k * 64 + j], q), (1ull << (8 * p)) % q, q);
+                for (uint32_t a = 0; a < 4; a++)
+                    img[tc::sw128_offset((k >> 5) * 128 + a * 32 + (k & 31), 4 * j + p, 256)] = (uint8_t)(v >> (8 * a));
+            }
 }
 
 // Byte-plane image of a 16-point matrix: 64 rows (a, c) x 64 bytes, K-major SW64.
@@ -573,13 +624,14 @@ void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_
     }
 }
 
-// Generator table slots: 0 stage A forward, 1 stage A inverse, 2 stage B
-// level 1 forward, 3 its inverse (same table as slot 1).
+// DFT-64 image slots: 0 stage A forward, 1 inverse (stage A and stage B
+// level 1 share it), 2 stage B level 1 forward.
 int build_cache(Plan32& p, Int8Cache* c) {
     const uint32_t n = p.n, nl = p.n_limbs;
-    // blob layout per limb: kLimbConst bytes of device-side constants (4
-    // generator tables + DFT-16 forward / inverse images) then 2 twiddle tables
-    const size_t per_limb = kLimbConst + 2 * kTabWords * 4;
+    // blob layout per limb: DFT-16 forward / inverse images, the DFT-64
+    // images, then the forward and inverse twiddle tables
+    const size_t tab_off = kBlobImg + (size_t)kImgSlots * kMatBytes64;
+    const size_t per_limb = tab_off + 2 * kTabWords * 4;
     std::vector<uint8_t> blob(per_limb * nl);
     uint8_t* d_blob = nullptr;
     if (cudaMalloc(&d_blob, blob.size()) != cudaSuccess) return 4;
@@ -594,20 +646,19 @@ int build_cache(Plan32& p, Int8Cache* c) {
         const uint64_t w64 = h_powmod(w, n / 64, q), w64i = h_powmod(wi, n / 64, q);
         const uint64_t w16 = h_powmod(w, n / 16, q), w16i = h_powmod(wi, n / 16, q);
         // stage A forward: the negacyclic twist psi^(a * n/64) on the input index
-        // makes W[k][j] = psi_128^(j (2k + 1)) (table of 128 powers)
-        uint32_t* gen = reinterpret_cast<uint32_t*>(h);
-        build_gen(gen + 0 * kGenWords, p.negacyclic ? h_powmod(H.psi, n / 64, q) : w64, p.negacyclic ? 128 : 64, q);
-        build_gen(gen + 1 * kGenWords, w64i, 64, q);
-        build_gen(gen + 2 * kGenWords, w64, 64, q);
-        build_gen(gen + 3 * kGenWords, w64i, 64, q);
+        // makes W[k][j] = psi_128^(j (2k + 1)), psi_128 = psi^(n/64)
+        const uint64_t p128 = h_powmod(H.psi, n / 64, q);
+        build_image64(h + kBlobImg, p.negacyclic ? dft_matrix(64, h_mulmod(p128, p128, q), q, 1, p128) : dft_matrix(64, w64, q), q);
+        build_image64(h + kBlobImg + kMatBytes64, dft_matrix(64, w64i, q), q);
+        build_image64(h + kBlobImg + 2 * kMatBytes64, dft_matrix(64, w64, q), q);
         // stage B level 2 inverse: n^-1 (and psi^-(4096 c2)) folded on the output index
         std::vector<uint64_t> B2f = dft_matrix(16, w16, q);
         std::vector<uint64_t> B2i = p.negacyclic ? dft_matrix(16, w16i, q, h_powmod(H.psi_inv, 4096, q), 1, H.n_inv)
                                                  : dft_matrix(16, w16i, q, 1, 1, H.n_inv);
-        build_image16(h + 4 * kGenWords * 4, B2f, q);
-        build_image16(h + 4 * kGenWords * 4 + kMatBytes16, B2i, q);
-        uint32_t* tab = reinterpret_cast<uint32_t*>(h + kLimbConst);
-        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + kLimbConst);
+        build_image16(h, B2f, q);
+        build_image16(h + kMatBytes16, B2i, q);
+        uint32_t* tab = reinterpret_cast<uint32_t*>(h + tab_off);
+        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + tab_off);
         // forward: t_A(b, d) = psi^b (negacyclic) * omega^(b d); t_B1(b2, d2) = omega^(64 b2 d2)
         for (uint32_t b = 0; b < 1024; b++) {
             st[b] = p.negacyclic ? h_powmod(H.psi, b, q) : 1;
@@ -678,13 +729,10 @@ ClStage stage(const Int8Cache* c, bool inverse, uint32_t kind) {
     s.limbs = inverse ? c->d_inv : c->d_fwd;
     s.kind = kind;
     if (kind == 0) {
-        s.gen = inverse ? 1 : 0;
-        s.e = (!inverse && c->negacyclic) ? 128 : 64;
+        s.img = inverse ? 1 : 0;
     } else {
-        // the inverse stage B level-1 table is the inverse stage A table;
-        // cyclic: the forward ones coincide too (slot 0)
-        s.gen = inverse ? 1 : (c->negacyclic ? 2 : 0);
-        s.e = 64;
+        // cyclic: the forward stage A and B level-1 matrices coincide (slot 0)
+        s.img = inverse ? 1 : (c->negacyclic ? 2 : 0);
     }
     s.img16 = inverse ? 1 : 0;
     return s;
