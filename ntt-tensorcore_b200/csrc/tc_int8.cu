@@ -90,23 +90,18 @@ constexpr uint32_t kBufBytes = 2 * kTileBytes;
 // per-limb device blob: DFT-16 images (8 KB), 3 DFT-64 images, twiddle tables
 constexpr uint32_t kImgSlots = 3;            // 0: stage A forward, 1: inverse (A and B), 2: stage B forward
 constexpr uint32_t kBlobImg = 2 * kMatBytes16;
-
-// Device constants of one modulus for one direction.
-struct TcLimb {
-    uint32_t q, qinv;        // modulus, -q^-1 mod 2^32
-    uint32_t one_m, pad_;    // 2^32 mod q
-    // stage A twiddle t_A(b, d) = a_st2[2b + h] * a_ratio[b]^(d - 32h), d in [32h, 32h + 32)
-    const uint32_t* a_st2;   // 2048 entries (Montgomery form)
-    const uint32_t* a_ratio; // 1024 entries
-    // stage B level-1 twiddle t_B1(b2, d2) = b_st2[2 b2 + h] * b_ratio[b2]^(d2 - 32h)
-    const uint32_t* b_st2;   // 32 entries
-    const uint32_t* b_ratio; // 16 entries
-};
+// twiddle table of one direction (words): a_st2[2048] a_ratio[1024] b_st2[32]
+// b_ratio[16] q qinv (pad to 16 bytes); the forward table, then the inverse
+//   stage A:  t_A(b, d)   = a_st2[2b + h] * a_ratio[b]^(d - 32h),   d in [32h, 32h + 32)
+//   stage B1: t_B1(b2, d2) = b_st2[2 b2 + h] * b_ratio[b2]^(d2 - 32h)  (Montgomery form)
+constexpr uint32_t kTabAst = 0, kTabArat = 2048, kTabBst = 3072, kTabBrat = 3104, kTabQ = 3120;
+constexpr uint32_t kTabWords = 3124;
+constexpr uint32_t kBlobTab = kBlobImg + kImgSlots * kMatBytes64;
+constexpr uint32_t kBlobBytes = kBlobTab + 2 * kTabWords * 4;
+static_assert(kBlobBytes % 16 == 0, "per-limb blobs must stay 16-byte aligned");
 
 struct Int8Cache {
     uint32_t log_n = 0;
-    TcLimb* d_fwd = nullptr;
-    TcLimb* d_inv = nullptr;
     uint8_t* d_blob = nullptr;
     size_t per_limb = 0;
     bool negacyclic = false;
@@ -114,7 +109,7 @@ struct Int8Cache {
 
 // One stage of the on-chip stage list.
 struct ClStage {
-    const TcLimb* limbs;  // twiddles of the stage's direction, per limb
+    uint32_t dir;         // 0: forward, 1: inverse (twiddle table of the stage)
     uint32_t kind;        // 0: stage A (columns), 1: stage B (rows)
     uint32_t img;         // DFT-64 image slot of the stage
     uint32_t img16;       // stage B: DFT-16 image 0 (forward) or 1 (inverse)
@@ -270,18 +265,17 @@ __device__ __forceinline__ uint32_t lane_cols(const Cl& c) {
 // (K block = this CTA's rank): piece j = d % 8 of the receiver's K block
 // (rows 16 j..), staged at piece slot (j / 4, 4 (j % 4) + P) of tile w'.
 template <class Gate, class PartDone>
-__device__ __forceinline__ void epilogue_a(const Cl& c, const TcLimb& L, Gate gate, PartDone part_done) {
+__device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qinv, uint32_t ratio, uint32_t start,
+                                           Gate gate, PartDone part_done) {
     const uint32_t m = c.quarter * 32u + c.lane, b = 128u * (2u * c.rank + c.w) + beta(m);
-    const uint32_t q = L.q, qinv = L.qinv;
-    const uint32_t ratio = L.a_ratio[b];
     const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
-    uint32_t tw_e = L.a_st2[2 * b + c.h];                       // d = 32h
+    uint32_t tw_e = start;                                      // d = 32h
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
     const uint32_t col = lane_cols(c);
     const uint32_t bl = b & 15u, a2 = (b >> 4) & 15u;
     // SW64 offset of (row bl, K word a2) inside a 16-row piece
     const uint32_t inpiece = (bl >> 3) * 512u + (bl & 7u) * 64u + (((a2 >> 2) ^ ((bl >> 1) & 3u)) << 4) + 4u * (a2 & 3u);
-#pragma unroll
+#pragma unroll 1
     for (uint32_t part = 0; part < 2; part++) {
         uint32_t y[16];
 #pragma unroll
@@ -312,17 +306,16 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, const TcLimb& L, Gate ga
 // z * t_B1(b2, d2) in [0, 2q) -> level-2 operand of the same tile (over
 // level 1), SW64, row r + 8 (d2 / 16) + 32 (d2 % 16), K word b2.
 template <class Gate>
-__device__ __forceinline__ void epilogue_b1(const Cl& c, const TcLimb& L, Gate gate) {
+__device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qinv, uint32_t ratio, uint32_t start,
+                                            Gate gate) {
     const uint32_t mv = c.quarter * 32u + c.lane, b2 = mv & 15u, r = mv >> 4;
-    const uint32_t q = L.q, qinv = L.qinv;
-    const uint32_t ratio = L.b_ratio[b2];
     const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
-    uint32_t tw_e = L.b_st2[2 * b2 + c.h];
+    uint32_t tw_e = start;
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
     const uint32_t col = lane_cols(c);
     // sw64_offset(r + 8 (2h + part) + 32 i, 4 b2) = off + 512 (2h + part) + 2048 i
     const uint32_t off = r * 64u + (((b2 >> 2) ^ ((r >> 1) & 3u)) << 4) + 4u * (b2 & 3u);
-#pragma unroll
+#pragma unroll 1
     for (uint32_t part = 0; part < 2; part++) {
         uint32_t y[16];
 #pragma unroll
@@ -358,7 +351,7 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
                                             PartDone part_done) {
     const uint32_t base = c.taddr + c.w * 256u + ((c.quarter * 32u) << 16);
     const uint32_t r = c.lane & 7u, d = 8u * (2u * c.rank + c.w) + r;
-#pragma unroll
+#pragma unroll 1
     for (uint32_t part = 0; part < 2; part++) {
         const uint32_t t2 = 2u * c.h + part;
         uint32_t y[16];
@@ -478,6 +471,23 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             const bool last = s + 1 == args.n_stages;
             const bool next_img = !last && args.st[s + 1].img != S.img;
             const uint32_t in = buf_addr(c, s & 1u);
+            // this thread's twiddle inputs, loaded now so the latency hides
+            // behind the operand wait and the MMA
+            uint32_t q, qinv, ratio, start;
+            {
+                const uint32_t* T = reinterpret_cast<const uint32_t*>(limb_blob + kBlobTab) + S.dir * kTabWords;
+                q = __ldg(T + kTabQ);
+                qinv = __ldg(T + kTabQ + 1);
+                if (S.kind == 0) {
+                    const uint32_t b = 128u * (2u * c.rank + c.w) + beta(c.quarter * 32u + c.lane);
+                    ratio = __ldg(T + kTabArat + b);
+                    start = __ldg(T + kTabAst + 2 * b + c.h);
+                } else {
+                    const uint32_t b2 = c.lane & 15u;  // row m' = 32 quarter + lane: b2 = m' % 16
+                    ratio = __ldg(T + kTabBrat + b2);
+                    start = __ldg(T + kTabBst + 2 * b2 + c.h);
+                }
+            }
             if (s > 0) {  // this stage's 64 KB operand arrived from the four CTAs
                 if (s & 1u) wait_cluster(c.bar + kBarIn1, ph_in1);
                 else wait_cluster(c.bar + kBarIn0, ph_in0);
@@ -497,7 +507,6 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             __syncwarp();
             wait_parity(c.bar + kBarMma + c.w, ph_mma);
             tc::fence_after_sync();
-            const TcLimb& L = S.limbs[limb];
             // before the first stores: the MMAs reading the overwritten operand
             // are done; thread 0 then fetches the next stage's image
             auto mma_gate = [&]() {
@@ -518,10 +527,10 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                     send_pieces(c, S.kind, 2u * c.h + part, S.kind == 0 ? kBarIn1 : kBarIn0);
             };
             if (S.kind == 0) {
-                epilogue_a(c, L, mma_gate, part_done);
+                epilogue_a(c, q, qinv, ratio, start, mma_gate, part_done);
                 ph_mma ^= 1u;
             } else {
-                epilogue_b1(c, L, mma_gate);
+                epilogue_b1(c, q, qinv, ratio, start, mma_gate);
                 ph_mma ^= 1u;
                 tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
@@ -543,7 +552,7 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                 wait_parity(c.bar + kBarMma2 + c.w, ph_mma2);
                 tc::fence_after_sync();
                 // staging overwrites both tiles' level-2 operands
-                epilogue_b2(c, L.q, L.qinv, last ? args.dst + off : nullptr,
+                epilogue_b2(c, q, qinv, last ? args.dst + off : nullptr,
                             [&]() { wait_parity(c.bar + kBarMma2 + (c.w ^ 1u), ph_mma2); }, part_done);
                 ph_mma2 ^= 1u;
             }
@@ -608,19 +617,19 @@ std::vector<uint64_t> dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t
     return W;
 }
 
-// Twiddle tables of one direction: a_st2 (2048), a_ratio (1024), b_st2 (32), b_ratio (16).
-constexpr size_t kTabWords = 2048 + 1024 + 32 + 16;
-
+// Twiddle table of one direction (layout at kTabAst..kTabQ).
 void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_t* ratio_a, const uint64_t* ratio_b) {
+    t[kTabQ] = (uint32_t)q;
+    t[kTabQ + 1] = h_neg_inv32((uint32_t)q);
     for (uint32_t b = 0; b < 1024; b++) {
-        t[2 * b] = h_to_mont32(start_a[b], q);
-        t[2 * b + 1] = h_to_mont32(h_mulmod(start_a[b], h_powmod(ratio_a[b], 32, q), q), q);
-        t[2048 + b] = h_to_mont32(ratio_a[b], q);
+        t[kTabAst + 2 * b] = h_to_mont32(start_a[b], q);
+        t[kTabAst + 2 * b + 1] = h_to_mont32(h_mulmod(start_a[b], h_powmod(ratio_a[b], 32, q), q), q);
+        t[kTabArat + b] = h_to_mont32(ratio_a[b], q);
     }
     for (uint32_t b2 = 0; b2 < 16; b2++) {
-        t[3072 + 2 * b2] = h_to_mont32(1, q);
-        t[3072 + 2 * b2 + 1] = h_to_mont32(h_powmod(ratio_b[b2], 32, q), q);
-        t[3104 + b2] = h_to_mont32(ratio_b[b2], q);
+        t[kTabBst + 2 * b2] = h_to_mont32(1, q);
+        t[kTabBst + 2 * b2 + 1] = h_to_mont32(h_powmod(ratio_b[b2], 32, q), q);
+        t[kTabBrat + b2] = h_to_mont32(ratio_b[b2], q);
     }
 }
 
@@ -630,18 +639,15 @@ int build_cache(Plan32& p, Int8Cache* c) {
     const uint32_t n = p.n, nl = p.n_limbs;
     // blob layout per limb: DFT-16 forward / inverse images, the DFT-64
     // images, then the forward and inverse twiddle tables
-    const size_t tab_off = kBlobImg + (size_t)kImgSlots * kMatBytes64;
-    const size_t per_limb = tab_off + 2 * kTabWords * 4;
+    const size_t per_limb = kBlobBytes;
     std::vector<uint8_t> blob(per_limb * nl);
     uint8_t* d_blob = nullptr;
     if (cudaMalloc(&d_blob, blob.size()) != cudaSuccess) return 4;
-    std::vector<TcLimb> fwd(nl), inv(nl);
     std::vector<uint64_t> st(1024), ra(1024), rb(16);
     for (uint32_t l = 0; l < nl; l++) {
         const LimbHost& H = p.limbs[l];
         const uint64_t q = H.q;
         uint8_t* h = blob.data() + per_limb * l;
-        uint8_t* d = d_blob + per_limb * l;
         const uint64_t w = H.omega, wi = H.omega_inv;
         const uint64_t w64 = h_powmod(w, n / 64, q), w64i = h_powmod(wi, n / 64, q);
         const uint64_t w16 = h_powmod(w, n / 16, q), w16i = h_powmod(wi, n / 16, q);
@@ -657,8 +663,7 @@ int build_cache(Plan32& p, Int8Cache* c) {
                                                  : dft_matrix(16, w16i, q, 1, 1, H.n_inv);
         build_image16(h, B2f, q);
         build_image16(h + kMatBytes16, B2i, q);
-        uint32_t* tab = reinterpret_cast<uint32_t*>(h + tab_off);
-        uint32_t* dtab = reinterpret_cast<uint32_t*>(d + tab_off);
+        uint32_t* tab = reinterpret_cast<uint32_t*>(h + kBlobTab);
         // forward: t_A(b, d) = psi^b (negacyclic) * omega^(b d); t_B1(b2, d2) = omega^(64 b2 d2)
         for (uint32_t b = 0; b < 1024; b++) {
             st[b] = p.negacyclic ? h_powmod(H.psi, b, q) : 1;
@@ -677,34 +682,11 @@ int build_cache(Plan32& p, Int8Cache* c) {
             if (p.negacyclic) rb[b2] = h_mulmod(rb[b2], h_powmod(H.psi_inv, 64, q), q);
         }
         fill_tables(tab + kTabWords, q, st.data(), ra.data(), rb.data());
-        TcLimb f{}, v{};
-        f.q = v.q = (uint32_t)q;
-        f.qinv = v.qinv = h_neg_inv32((uint32_t)q);
-        f.one_m = v.one_m = h_to_mont32(1, q);
-        f.a_st2 = dtab;
-        f.a_ratio = dtab + 2048;
-        f.b_st2 = dtab + 3072;
-        f.b_ratio = dtab + 3104;
-        v.a_st2 = dtab + kTabWords;
-        v.a_ratio = dtab + kTabWords + 2048;
-        v.b_st2 = dtab + kTabWords + 3072;
-        v.b_ratio = dtab + kTabWords + 3104;
-        fwd[l] = f;
-        inv[l] = v;
     }
     if (cudaMemcpy(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaFree(d_blob);
         return 3;
     }
-    TcLimb* d_l = nullptr;
-    if (cudaMalloc(&d_l, 2 * nl * sizeof(TcLimb)) != cudaSuccess) {
-        cudaFree(d_blob);
-        return 4;
-    }
-    cudaMemcpy(d_l, fwd.data(), nl * sizeof(TcLimb), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_l + nl, inv.data(), nl * sizeof(TcLimb), cudaMemcpyHostToDevice);
-    c->d_fwd = d_l;
-    c->d_inv = d_l + nl;
     c->d_blob = d_blob;
     c->per_limb = per_limb;
     c->negacyclic = p.negacyclic;
@@ -726,7 +708,7 @@ Int8Cache* get_cache(Plan32& p) {
 
 ClStage stage(const Int8Cache* c, bool inverse, uint32_t kind) {
     ClStage s{};
-    s.limbs = inverse ? c->d_inv : c->d_fwd;
+    s.dir = inverse ? 1 : 0;
     s.kind = kind;
     if (kind == 0) {
         s.img = inverse ? 1 : 0;
@@ -827,7 +809,6 @@ int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStre
 void int8_release(Plan32* p) {
     auto* c = reinterpret_cast<Int8Cache*>(p->engine_data[1]);
     if (!c) return;
-    if (c->d_fwd) cudaFree(c->d_fwd);
     if (c->d_blob) cudaFree(c->d_blob);
     delete c;
     p->engine_data[1] = nullptr;
