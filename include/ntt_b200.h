@@ -164,6 +164,22 @@ NTTB_API int nttb_wide_plan_destroy(nttb_wide_plan* plan);
 NTTB_API int nttb_wide_transform(const nttb_wide_plan* plan, uint64_t* d_dst, const uint64_t* d_src, uint32_t n_polys,
                         int inverse, void* stream);
 
+/* ------------------------------------ K-limb residues (24-bit limbs)
+ * The reference's header-only arbitrary-modulus path: elements are
+ * DScalar<K> = K little-endian uint32 words, each a 24-bit limb, in
+ * Montgomery form (R = 2^(24 K)), canonical in [0, p).  Forward transform in
+ * place, natural order in and out: bit reversal then the radix-2 DIT network
+ * of host_ntt_naive (include/ntt_arbitrary.cuh:2651-2676) with twiddle
+ * d_tw[k * n / 2^(s+1)] at stage s (d_tw: n Montgomery-form powers of omega,
+ * as setup_ntt builds them).  `prime` is a HOST array of K limbs, np =
+ * -prime^-1 mod 2^24.  Replaces run_forward_ct, run_forward_ct_tcu
+ * (include/ntt_arbitrary.cuh:2556-2646) and run_forward_radix64_scalar
+ * (include/ntt_arbitrary_radix64.cuh:345-389), which compute the same
+ * network.  K in {2, 3, 11} (the reference's FieldConfig set), n = 2^log_n,
+ * log_n <= 24. */
+NTTB_API int nttb_klimb_forward(uint32_t K, uint32_t* d_data, const uint32_t* d_tw, uint64_t n, uint32_t log_n,
+                                const uint32_t* prime, uint32_t np, void* stream);
+
 /* ------------------------------------------------------------ accounting
  * No reference counterpart (the reference times with ad-hoc cudaEvents,
  * tests/benchmark.cu:52-99).  nttb_launch_count counts every kernel launch

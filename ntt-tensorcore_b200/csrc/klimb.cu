@@ -1,0 +1,164 @@
+// klimb.cu -- the K-limb forward NTT (residues of K x 24-bit limbs in
+// Montgomery form, the reference's DScalar<K> layout) behind
+// nttb_klimb_forward.
+//
+// The transform is the radix-2 decimation-in-time network of the reference's
+// host_ntt_naive (include/ntt_arbitrary.cuh:2651-2676) applied in the
+// Montgomery domain: bit-reverse, then for stage s = 0..log_n-1 the butterfly
+// (a[i], a[i + 2^s]) <- (u + t, u - t), t = a[i + 2^s] * tw[k * n / 2^(s+1)],
+// k = i mod 2^s.  The network is reproduced stage for stage (not replaced by
+// another DFT factorisation) because the reference's K = 2 field is not a
+// field with the advertised root of unity, so only the network itself defines
+// the result there.
+//
+// Execution: one in-place bit reversal, then "stage group" passes.  A pass
+// runs r consecutive stages s0..s0+r-1 on tiles held in shared memory: a tile
+// is C columns x 2^r elements, column (G, low) = { G 2^(s0+r) + j 2^s0 + low },
+// C consecutive `low` values so that loads are coalesced.  The first pass
+// (s0 = 0, C = 1) covers contiguous blocks; N = 2^20 with K = 3 needs two
+// passes instead of the twenty radix-2 sweeps.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/ntt_b200.h"
+#include "../../include/ntt_limb_arith.cuh"
+#include "engines.hpp"
+#include "profiler.hpp"
+
+namespace nttb {
+namespace {
+
+template <int K>
+struct Limbs {
+    uint32_t l[K];
+};
+
+template <int K>
+__global__ void klimb_bitrev(uint32_t* data, uint32_t n, uint32_t log_n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || log_n == 0) return;
+    const uint32_t j = __brev(i) >> (32u - log_n);
+    if (i >= j) return;
+    uint32_t* a = data + (size_t)i * K;
+    uint32_t* b = data + (size_t)j * K;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const uint32_t t = a[k];
+        a[k] = b[k];
+        b[k] = t;
+    }
+}
+
+// Stages s0 .. s0 + r - 1 on tiles of 2^(r + logC) elements (shared memory,
+// limb-major: sm[k * E + e], e = j * C + c).
+template <int K>
+__global__ void __launch_bounds__(256) klimb_group(uint32_t* data, const uint32_t* tw, uint32_t log_n, uint32_t s0,
+                                                   uint32_t r, uint32_t logC, Limbs<K> p, uint32_t np) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t E = 1u << (r + logC), C = 1u << logC;
+    const uint32_t chunks = (1u << s0) >> logC;  // column chunks per group of 2^(s0 + r)
+    const uint32_t G = blockIdx.x / chunks, low0 = (blockIdx.x % chunks) << logC;
+    const size_t base = ((size_t)G << (s0 + r)) + low0;
+    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const size_t i = base + ((size_t)(e >> logC) << s0) + (e & (C - 1));
+        const uint32_t* src = data + i * K;
+#pragma unroll
+        for (int k = 0; k < K; k++) sm[k * E + e] = src[k];
+    }
+    __syncthreads();
+    for (uint32_t t = 0; t < r; t++) {
+        const uint32_t half = 1u << t, tshift = log_n - s0 - t - 1;
+        for (uint32_t bf = threadIdx.x; bf < E / 2; bf += blockDim.x) {
+            const uint32_t c = bf & (C - 1), pi = bf >> logC;
+            const uint32_t jlo = ((pi >> t) << (t + 1)) | (pi & (half - 1));
+            const uint32_t elo = (jlo << logC) + c, ehi = elo + (half << logC);
+            const uint32_t ktw = ((jlo & (half - 1)) << s0) + low0 + c;
+            const uint32_t* w = tw + ((size_t)ktw << tshift) * K;
+            uint32_t wv[K], u[K], v[K], x[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                wv[k] = __ldg(w + k);
+                u[k] = sm[k * E + elo];
+                v[k] = sm[k * E + ehi];
+            }
+            nttb_limb::mont_mul<K>(x, v, wv, p.l, np);
+            nttb_limb::add_mod<K>(v, u, x, p.l);
+            nttb_limb::sub_mod<K>(u, u, x, p.l);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                sm[k * E + elo] = v[k];
+                sm[k * E + ehi] = u[k];
+            }
+        }
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
+        const size_t i = base + ((size_t)(e >> logC) << s0) + (e & (C - 1));
+        uint32_t* dst = data + i * K;
+#pragma unroll
+        for (int k = 0; k < K; k++) dst[k] = sm[k * E + e];
+    }
+}
+
+template <int K>
+int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const uint32_t* prime, uint32_t np,
+                  cudaStream_t s) {
+    Limbs<K> p;
+    for (int k = 0; k < K; k++) p.l[k] = prime[k];
+    const uint32_t n = 1u << log_n;
+    // largest tile: 48 KB of shared memory
+    const uint32_t log_emax = K <= 3 ? 12u : 10u;
+    {
+        ProfScope prof("klimb_bitrev", s);
+        klimb_bitrev<K><<<(n + 255) / 256, 256, 0, s>>>(d_data, n, log_n);
+        if (cudaGetLastError() != cudaSuccess) return 2;
+    }
+    uint32_t s0 = 0;
+    while (s0 < log_n) {
+        uint32_t r = log_n - s0, logC = 0;
+        if (s0 == 0) {
+            if (r > log_emax) r = log_emax;
+        } else {
+            if (r > 8) r = 8;
+            logC = log_emax - r < s0 ? log_emax - r : s0;
+        }
+        const uint32_t E = 1u << (r + logC);
+        const uint32_t threads = E / 2 < 256 ? E / 2 : 256;
+        ProfScope prof("klimb_group", s);
+        klimb_group<K><<<n / E, threads, (size_t)E * K * 4, s>>>(d_data, d_tw, log_n, s0, r, logC, p, np);
+        if (cudaGetLastError() != cudaSuccess) return 2;
+        s0 += r;
+    }
+    return 0;
+}
+
+}  // namespace
+}  // namespace nttb
+
+extern "C" {
+
+NTTB_API int nttb_klimb_forward(uint32_t K, uint32_t* d_data, const uint32_t* d_tw, uint64_t n, uint32_t log_n,
+                                const uint32_t* prime, uint32_t np, void* stream) {
+    using nttb::fail;
+    if (!d_data || !d_tw || !prime) return fail(NTTB_ERR_INVALID_ARG, "nttb_klimb_forward: null pointer");
+    if (log_n > 24 || n != (1ull << log_n))
+        return fail(NTTB_ERR_INVALID_ARG, "nttb_klimb_forward: n must be 2^log_n with log_n <= 24");
+    if (K != 2 && K != 3 && K != 11)
+        return fail(NTTB_ERR_UNSUPPORTED, "nttb_klimb_forward: K = %u (this build serves K = 2, 3, 11)", K);
+    if ((prime[0] & 1u) == 0) return fail(NTTB_ERR_INVALID_ARG, "nttb_klimb_forward: even modulus");
+    for (uint32_t k = 0; k < K; k++)
+        if (prime[k] > nttb_limb::kMask) return fail(NTTB_ERR_INVALID_ARG, "nttb_klimb_forward: limb %u >= 2^24", k);
+    if (np != nttb_limb::neg_inv24(prime[0]))
+        return fail(NTTB_ERR_INVALID_ARG, "nttb_klimb_forward: np != -p^-1 mod 2^24");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = 0;
+    switch (K) {
+        case 2: rc = nttb::klimb_forward<2>(d_data, d_tw, log_n, prime, np, s); break;
+        case 3: rc = nttb::klimb_forward<3>(d_data, d_tw, log_n, prime, np, s); break;
+        default: rc = nttb::klimb_forward<11>(d_data, d_tw, log_n, prime, np, s); break;
+    }
+    return rc ? fail(NTTB_ERR_CUDA, "nttb_klimb_forward: kernel launch failed") : NTTB_OK;
+}
+
+}  // extern "C"

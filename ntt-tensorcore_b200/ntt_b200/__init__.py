@@ -86,6 +86,7 @@ def lib():
         "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
+        "nttb_klimb_forward": (_int, [_u32, _vp, _vp, _u64, _u32, _vp, _u32, _vp]),
         "nttb_device_errors": (_int, [ctypes.POINTER(_u32), _int]),
         "nttb_launch_count": (_int, [ctypes.POINTER(_u64)]),
         "nttb_profile_start": (_int, []),
@@ -129,6 +130,19 @@ def _engine(e):
 
 def version():
     return lib().nttb_version().decode()
+
+
+# ------------------------------------------------------------ K-limb path
+def klimb_forward(K, d_data, d_tw, log_n, prime_limbs, np_, stream=None):
+    """nttb_klimb_forward: in-place forward NTT of 2^log_n K-limb Montgomery
+    residues (K uint32 words of 24-bit limbs each) with twiddle table d_tw."""
+    p = (ctypes.c_uint32 * K)(*[int(v) for v in prime_limbs])
+    _check(lib().nttb_klimb_forward(K, _ptr(d_data), _ptr(d_tw), 1 << log_n, log_n, p, np_, _stream(stream)))
+
+
+def klimb_neg_inv24(p0):
+    """-p^-1 mod 2^24 from the lowest limb (the np argument)."""
+    return (-pow(int(p0), -1, 1 << 24)) % (1 << 24)
 
 
 # ------------------------------------------------------------- accounting

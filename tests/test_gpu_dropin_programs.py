@@ -45,3 +45,28 @@ def test_reference_debug_rowmaj():
     assert rc == 0, out[-2000:]
     assert "Optimized vs host: 4096 / 4096  PASS" in out
     assert "RowMaj    vs host: 4096 / 4096  PASS" in out
+
+
+def test_reference_ntt_mma_arbitrary_driver():
+    """src/ntt_mma_arbitrary.cu (the K-limb driver) against ntt_arbitrary.cuh:
+    Montgomery self tests for K = 2, 3, 11 and the forward NTT checked against
+    host_ntt_naive at every size of its default sweep."""
+    rc, out = run("ntt_mma_arbitrary", timeout=1200)
+    assert rc == 0, out[-3000:]
+    assert out.count("mont round-trip + mult OK") == 3, out[-3000:]
+    assert out.count("device mont_mul == host mont_mul OK") == 3, out[-3000:]
+    assert out.count("0 mismatches  OK") == 3, out[-3000:]
+    assert out.count("CORRECT (matches host reference") == 7, out[-3000:]
+    assert "MISMATCH" not in out and "FAIL" not in out, out[-3000:]
+
+
+def test_reference_timing_compare_runs():
+    """tests/timing_compare.cu builds against the drop-in (including its direct
+    launches of bitrev_kernel_d / ct_stage_kernel) and runs its K = 2 and
+    K = 11 sweeps to completion."""
+    path = os.path.join(BIN, "dropin_timing_compare")
+    if not os.path.exists(path):
+        pytest.skip("drop-in program timing_compare not built")
+    r = subprocess.run([path, "6", "8", "10", "12"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (r.stdout + r.stderr)[-3000:]
+    assert "LEGEND" in r.stdout
