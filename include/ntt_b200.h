@@ -50,9 +50,11 @@ enum {
 NTTB_API const char* nttb_version(void);
 NTTB_API const char* nttb_status_string(int status);
 NTTB_API const char* nttb_last_error(void);
-/* Device-side error bits raised by bounded waits in the tensor-core kernels
- * (bit 0: an mbarrier wait ran out of budget and the tile was skipped).
- * Reads after a device synchronize; clear != 0 resets them. */
+/* Device-side error bits raised by bounded waits in the persistent kernels
+ * (bit 0: an INT8-engine mbarrier wait ran out of budget, bit 1: a wait on
+ * another CTA of an INT8 cluster did, bit 2: an uneven-batch queue
+ * dependency wait did; the work item ran on regardless and its output is
+ * wrong).  Reads after a device synchronize; clear != 0 resets them. */
 NTTB_API int nttb_device_errors(uint32_t* flags, int clear);
 
 /* ------------------------------------------------ modular parameters (host)
@@ -163,6 +165,59 @@ NTTB_API int nttb_wide_plan_create(uint32_t log_n, const uint64_t* moduli, uint3
 NTTB_API int nttb_wide_plan_destroy(nttb_wide_plan* plan);
 NTTB_API int nttb_wide_transform(const nttb_wide_plan* plan, uint64_t* d_dst, const uint64_t* d_src, uint32_t n_polys,
                         int inverse, void* stream);
+
+/* ------------------------------------------------------- uneven batches
+ * No single reference counterpart (the reference transforms one size and one
+ * modulus per call, ntt_forward_batch, src/ntt_basic.cu:337-389).  A batch
+ * plan holds twiddle tables for up to 2^24 residues for a set of 31-bit
+ * moduli; a batch is a list of jobs -- polynomials of any size 2^1 ..
+ * 2^max_log_n, any number of consecutive moduli of the plan, forward or
+ * inverse, cyclic or negacyclic -- run by ONE persistent launch that draws
+ * (unit, pass, tile) work items from a device queue.  Results equal
+ * nttb_rns_transform on each job.  Data of a job: n_limbs rows of 2^log_n
+ * uint32 residues (row l reduced mod moduli[first_modulus + l]), in place. */
+typedef struct nttb_batch_plan nttb_batch_plan;
+typedef struct nttb_batch nttb_batch;
+#define NTTB_BATCH_INVERSE 2u /* job flag; NTTB_NEGACYCLIC (1) selects the negacyclic twist */
+typedef struct {
+    uint32_t* data;         /* device memory, n_limbs << log_n words, transformed in place */
+    uint32_t log_n;         /* 1 .. plan max_log_n */
+    uint32_t n_limbs;
+    uint32_t first_modulus; /* row l uses the plan's modulus first_modulus + l */
+    uint32_t flags;         /* NTTB_BATCH_INVERSE | NTTB_NEGACYCLIC */
+} nttb_batch_job;
+/* Tuning knobs (see nttb_batch_autotune). */
+typedef struct {
+    uint32_t tile_elems;  /* shared-memory tile: 4096, 8192 or 16384 residues */
+    uint32_t threads;     /* CTA width: 256 (tiles 4096, 8192) or 512 (tiles 8192, 16384) */
+    uint32_t split;       /* two-pass radix split: 0 first pass 2^ceil(L/2), 1 first pass 2^floor(L/2) */
+    uint32_t lag;         /* two-pass units between a unit's first and second pass in the queue (1..64) */
+    uint32_t ctas_per_sm; /* 0: as many as fit */
+} nttb_batch_config;
+
+/* flags: NTTB_NEGACYCLIC to allow negacyclic jobs (moduli then need 2^(max_log_n+1) | q-1). */
+NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, uint32_t max_log_n, uint32_t flags,
+                                    nttb_batch_plan** out);
+NTTB_API int nttb_batch_plan_destroy(nttb_batch_plan* plan);
+NTTB_API int nttb_batch_default_config(nttb_batch_config* out);
+/* Times every knob combination on a sample of the jobs' mix (scratch
+ * buffers; the jobs' data is not touched), keeps the fastest as the plan's
+ * default for later nttb_batch_create calls and returns it. */
+NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs, void* stream,
+                                 nttb_batch_config* out);
+/* Builds the work queue of a job list (host work + device upload; allocates
+ * the queue and a workspace ring for the two-pass units).  config NULL: the
+ * plan's tuned configuration, else the default. */
+NTTB_API int nttb_batch_create(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs,
+                               const nttb_batch_config* config, nttb_batch** out);
+NTTB_API int nttb_batch_destroy(nttb_batch* batch);
+/* Runs the batch: a counter reset and one persistent kernel on `stream`; no
+ * allocation, no host synchronisation. */
+NTTB_API int nttb_batch_launch(nttb_batch* batch, void* stream);
+/* Same work, replayed from a CUDA graph captured on the first call. */
+NTTB_API int nttb_batch_graph_launch(nttb_batch* batch, void* stream);
+NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t* tiles, uint64_t* ws_bytes,
+                             nttb_batch_config* config);
 
 /* ------------------------------------ K-limb residues (24-bit limbs)
  * The reference's header-only arbitrary-modulus path: elements are

@@ -1,0 +1,773 @@
+// batch.cu -- uneven batches: polynomials of different sizes (2^1 .. 2^max_log),
+// limb counts, moduli and directions transformed in ONE persistent launch.
+//
+// Work decomposition.  Every (polynomial, limb) transform of n = 2^L residues
+// is a "unit":
+//   * L <= log2(tile): one single-pass unit covers up to `rows` consecutive
+//     limbs of a polynomial (one shared-memory tile, one row per limb: the
+//     limb split), DIF stages, natural order in and out;
+//   * larger L: a two-pass four-step unit per limb, n = N1 * N2:
+//       pass A: columns b of x as [N1][N2]: U[d][b] = DFT_N1(x[.][b])[d] * w^(d b),
+//               stored transposed at b N1 + d in a workspace slot;
+//       pass B: columns d of the slot as [N2][N1]: X[d + N1 k] = DFT_N2, to x.
+//     Pass A has N2 / va tiles, pass B N1 / vb tiles (va, vb vectors per tile).
+// Negacyclic twists psi^i and the inverse's n^-1 (psi^-i) are fused into the
+// first load and the last store.  This is the scalar engine's two-pass
+// layout, so results are bit-identical to the per-size transforms.
+//
+// The device work queue.  The host lays the tiles out in one array, largest
+// units first; a unit's pass B tiles are placed `lag` two-pass units after its
+// pass A tiles, so CTAs rarely wait.  CTAs of the persistent grid claim tiles
+// with an atomic ticket.  A pass B tile first waits (bounded spin, acquire)
+// until every pass A tile of its unit has signalled; a pass A tile first waits
+// until the previous user of its workspace slot has finished pass B.  Every
+// awaited tile has a smaller ticket, so it belongs to a CTA that is already
+// running: no deadlock.  Workspace slots form a ring of S > lag slots, so the
+// workspace is S x (largest unit), not the size of the batch.
+//
+// Tuning knobs (nttb_batch_config): shared-memory tile size and CTA width
+// (4096/256, 8192/256, 8192/512, 16384/512), the radix split of two-pass
+// units (first pass 2^ceil(L/2) or 2^floor(L/2)), the queue lag and the CTAs
+// per SM; nttb_batch_autotune times the candidates on a sample of the job mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <deque>
+#include <string>
+#include <vector>
+
+#include "../../include/ntt_b200.h"
+#include "arith.cuh"
+#include "engines.hpp"
+#include "plan.hpp"
+#include "profiler.hpp"
+
+namespace nttb {
+
+// bit 0: a queue dependency wait ran out of budget
+__device__ uint32_t g_batch_error;
+
+namespace {
+
+constexpr uint32_t BF_INV = 1, BF_PRE_PSI = 2, BF_POST_TW = 4, BF_STORE_T = 8, BF_POST_SCALE = 16, BF_POST_PSI = 32;
+constexpr uint32_t UF_INV = 1, UF_NEGA = 2;
+constexpr uint32_t kMaxRows = 32;
+
+// Per-modulus device constants at the plan's largest size 2^max_log.
+struct BModulus {
+    M32 ar;
+    const uint32_t* tw;       // omega^e R, e < 2^max_log (omega of order 2^max_log)
+    const uint32_t* tw_inv;   // omega^-e R
+    const uint32_t* psi;      // psi^e R, psi of order 2^(max_log + 1) (negacyclic plans)
+    const uint32_t* psi_inv;  // psi^-e R
+    uint32_t ninv[25];        // 2^-L R mod q
+    uint32_t pad_;
+};
+
+struct BUnit {
+    uint32_t* data;    // row 0 of the unit; row r (limb) at data + r n
+    uint32_t* ws;      // workspace slot (two-pass units)
+    uint32_t mod0;     // modulus index of row 0; row r uses mod0 + r
+    uint32_t log_n;
+    uint32_t flags;    // UF_INV | UF_NEGA
+    uint32_t lg1;      // log2 of the pass A length; 0: single pass
+    uint32_t rows;     // single pass: rows in the tile
+    uint32_t va, vb;   // vectors per tile in pass A / pass B
+    uint32_t tiles_a, tiles_b;
+    int32_t prev;      // two-pass unit that held the same workspace slot before, or -1
+};
+
+struct BTile {
+    uint32_t unit;
+    uint32_t pass_tile;  // pass in bit 31, tile index below
+};
+
+struct BArgs {
+    const BModulus* mods;
+    const BUnit* units;
+    const BTile* tiles;
+    uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u
+    uint32_t n_tiles, max_log;
+};
+
+__device__ __forceinline__ bool wait_ge(const uint32_t* p, uint32_t target) {
+    for (uint32_t i = 0; i < (1u << 24); i++) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+// One tile: V vectors of length len, in shared memory.  COL mode (DIT after
+// a bit-reversed load): vectors are columns vec of a [len][C] matrix; ROW
+// mode (DIF, bit-reversed read at the store): vectors are rows of n words.
+template <uint32_t T>
+__device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile, uint32_t* sm,
+                                         M32* s_ar) {
+    const uint32_t L = u.log_n, n = 1u << L, shift = a.max_log - L;
+    const bool inv = u.flags & UF_INV, nega = u.flags & UF_NEGA;
+    bool row;
+    uint32_t lg, V, v0, C, flags;
+    const uint32_t* src;
+    uint32_t* dst;
+    if (u.lg1 == 0) {
+        row = true;
+        lg = L;
+        V = u.rows;
+        v0 = 0;
+        C = n;
+        src = u.data;
+        dst = u.data;
+        flags = (nega && !inv ? BF_PRE_PSI : 0u) | (inv ? (nega ? BF_POST_PSI : BF_POST_SCALE) : 0u);
+    } else if (pass == 0) {
+        row = false;
+        lg = u.lg1;
+        V = u.va;
+        v0 = tile * V;
+        C = n >> lg;
+        src = u.data;
+        dst = u.ws;
+        flags = (nega && !inv ? BF_PRE_PSI : 0u) | BF_POST_TW | BF_STORE_T;
+    } else {
+        row = false;
+        lg = L - u.lg1;
+        V = u.vb;
+        v0 = tile * V;
+        C = 1u << u.lg1;
+        src = u.ws;
+        dst = u.data;
+        flags = inv ? (nega ? BF_POST_PSI : BF_POST_SCALE) : 0u;
+    }
+    const uint32_t len = 1u << lg, half_len = len >> 1;
+    const uint32_t stride = len >= 32 ? len + 1 : len;
+    const uint32_t n_mods = row ? V : 1u;
+    uint32_t* t = sm;
+    uint32_t* tws = sm + V * stride;  // n_mods x len / 2 root powers
+    if (threadIdx.x < n_mods) s_ar[threadIdx.x] = a.mods[u.mod0 + threadIdx.x].ar;
+    for (uint32_t i = threadIdx.x; i < n_mods * half_len; i += T) {
+        const uint32_t r = i / half_len, k = i % half_len;
+        const BModulus& M = a.mods[u.mod0 + r];
+        tws[i] = __ldg((inv ? M.tw_inv : M.tw) + ((size_t)k << (a.max_log - lg)));
+    }
+    __syncthreads();
+    // ---- load ----
+    const uint32_t total = V * len;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += T) {
+        uint32_t v, j, elem;
+        size_t pos;
+        if (row) {
+            v = idx / len;
+            j = idx % len;
+            pos = (size_t)v * n + j;
+            elem = j;
+        } else {
+            v = idx % V;
+            j = idx / V;
+            pos = (size_t)j * C + v0 + v;
+            elem = (uint32_t)pos;
+        }
+        uint32_t x = __ldcg(src + pos);
+        if (flags & BF_PRE_PSI) {
+            const BModulus& M = a.mods[u.mod0 + (row ? v : 0u)];
+            x = s_ar[row ? v : 0u].mul(x, __ldg(M.psi + ((size_t)elem << shift)));
+        }
+        t[v * stride + (row ? j : bitrev(j, (int)lg))] = x;
+    }
+    __syncthreads();
+    // ---- radix-2 stages ----
+    const uint32_t half_total = total >> 1;
+    if (!row) {
+        const M32 ar = s_ar[0];
+        for (uint32_t s = 0; s < lg; s++) {
+            const uint32_t half = 1u << s;
+            for (uint32_t bf = threadIdx.x; bf < half_total; bf += T) {
+                const uint32_t v = bf / half_len, j = bf % half_len;
+                const uint32_t p = j & (half - 1), i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+                uint32_t* rw = t + v * stride;
+                const uint32_t u0 = rw[i0], y = ar.mul(rw[i1], tws[p << (lg - 1 - s)]);
+                rw[i0] = ar.add(u0, y);
+                rw[i1] = ar.sub(u0, y);
+            }
+            __syncthreads();
+        }
+    } else {
+        for (int s = (int)lg - 1; s >= 0; s--) {
+            const uint32_t half = 1u << s;
+            for (uint32_t bf = threadIdx.x; bf < half_total; bf += T) {
+                const uint32_t v = bf / half_len, j = bf % half_len;
+                const uint32_t p = j & (half - 1), i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+                const M32 ar = s_ar[v];
+                uint32_t* rw = t + v * stride;
+                const uint32_t u0 = rw[i0], y = rw[i1];
+                rw[i0] = ar.add(u0, y);
+                rw[i1] = ar.mul(ar.sub(u0, y), tws[v * half_len + (p << (lg - 1 - s))]);
+            }
+            __syncthreads();
+        }
+    }
+    // ---- store ----
+    for (uint32_t idx = threadIdx.x; idx < total; idx += T) {
+        uint32_t v, k, elem;
+        size_t pos;
+        uint32_t x;
+        if (row) {
+            v = idx / len;
+            k = idx % len;
+            x = t[v * stride + bitrev(k, (int)lg)];
+            pos = (size_t)v * n + k;
+            elem = k;
+        } else {
+            v = idx % V;
+            k = idx / V;
+            x = t[v * stride + k];
+            const uint32_t vec = v0 + v;
+            pos = (flags & BF_STORE_T) ? (size_t)vec * len + k : (size_t)k * C + vec;
+            elem = (uint32_t)pos;
+            if (flags & BF_POST_TW) {
+                const BModulus& M = a.mods[u.mod0];
+                const uint32_t e = (uint32_t)(((uint64_t)k * vec) & (n - 1));
+                x = s_ar[0].mul(x, __ldg((inv ? M.tw_inv : M.tw) + ((size_t)e << shift)));
+            }
+        }
+        if (flags & (BF_POST_SCALE | BF_POST_PSI)) {
+            const uint32_t r = row ? v : 0u;
+            const BModulus& M = a.mods[u.mod0 + r];
+            x = s_ar[r].mul(x, M.ninv[L]);
+            if (flags & BF_POST_PSI) x = s_ar[r].mul(x, __ldg(M.psi_inv + ((size_t)elem << shift)));
+        }
+        dst[pos] = x;
+    }
+}
+
+template <uint32_t E, uint32_t T>
+__global__ void __launch_bounds__(T) batch_queue(const __grid_constant__ BArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t s_ticket;
+    __shared__ M32 s_ar[kMaxRows];
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = atomicAdd(a.ctr, 1u);
+        __syncthreads();
+        const uint32_t ticket = s_ticket;
+        if (ticket >= a.n_tiles) break;
+        const BTile tl = a.tiles[ticket];
+        const BUnit u = a.units[tl.unit];
+        const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (pass == 1) ok = wait_ge(a.ctr + 1 + 2 * tl.unit, u.tiles_a);
+            else if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, a.units[u.prev].tiles_b);
+            if (!ok) atomicOr(&g_batch_error, 1u);
+            __threadfence();
+        }
+        __syncthreads();
+        run_tile<T>(a, u, pass, tile, sm, s_ar);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0)
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.ctr + 1 + 2 * tl.unit + pass) : "memory");
+    }
+}
+
+// ---- host ------------------------------------------------------------------------
+struct Variant {
+    uint32_t E, T;
+    void (*fn)(BArgs);
+};
+const Variant kVariants[] = {
+    {4096, 256, batch_queue<4096, 256>},
+    {8192, 256, batch_queue<8192, 256>},
+    {8192, 512, batch_queue<8192, 512>},
+    {16384, 512, batch_queue<16384, 512>},
+};
+
+const Variant* find_variant(uint32_t E, uint32_t T) {
+    for (const Variant& v : kVariants)
+        if (v.E == E && v.T == T) return &v;
+    return nullptr;
+}
+
+// tile elements + root powers + padding, in words
+size_t smem_bytes(uint32_t E) { return ((size_t)E + E / 32 + kMaxRows + E / 2) * 4 + 64; }
+
+uint32_t ilog2(uint64_t x) {
+    uint32_t l = 0;
+    while ((1ull << l) < x) l++;
+    return l;
+}
+
+}  // namespace
+
+struct BatchPlan {
+    uint32_t max_log = 0;
+    bool negacyclic = false;
+    std::vector<LimbHost> limbs;
+    BModulus* d_mods = nullptr;
+    std::vector<void*> allocations;
+    nttb_batch_config tuned{};
+    bool have_tuned = false;
+};
+
+struct Batch {
+    BatchPlan* plan = nullptr;
+    nttb_batch_config cfg{};
+    const Variant* var = nullptr;
+    BUnit* d_units = nullptr;
+    BTile* d_tiles = nullptr;
+    uint32_t* d_ctr = nullptr;
+    uint32_t* d_ws = nullptr;
+    uint32_t n_units = 0, n_tiles = 0;
+    size_t ws_bytes = 0;
+    int grid = 0;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaStream_t cap = nullptr;
+};
+
+namespace {
+
+nttb_batch_config default_config() {
+    nttb_batch_config c{};
+    c.tile_elems = 8192;
+    c.threads = 256;
+    c.split = 0;
+    c.lag = 2;
+    c.ctas_per_sm = 0;
+    return c;
+}
+
+int check_config(const nttb_batch_config& c) {
+    if (!find_variant(c.tile_elems, c.threads))
+        return fail(NTTB_ERR_INVALID_ARG, "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512");
+    if (c.split > 1) return fail(NTTB_ERR_INVALID_ARG, "batch config: split must be 0 or 1");
+    if (c.lag < 1 || c.lag > 64) return fail(NTTB_ERR_INVALID_ARG, "batch config: lag must be in [1, 64]");
+    return 0;
+}
+
+void free_batch(Batch* b) {
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    cudaFree(b->d_units);
+    cudaFree(b->d_tiles);
+    cudaFree(b->d_ctr);
+    cudaFree(b->d_ws);
+    delete b;
+}
+
+// Units, queue order and workspace ring of one batch (host work only).
+int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, const nttb_batch_config& cfg,
+               std::vector<BUnit>& units, std::vector<BTile>& tiles, uint32_t* ws_words_out, uint32_t* slots_out) {
+    const uint32_t E = cfg.tile_elems, lgE = ilog2(E);
+    struct Pending {
+        BUnit u;
+        uint64_t work;
+    };
+    std::vector<Pending> list;
+    for (uint32_t j = 0; j < n_jobs; j++) {
+        const nttb_batch_job& J = jobs[j];
+        if (!J.data) return fail(NTTB_ERR_INVALID_ARG, "batch job %u: null data", j);
+        if (J.log_n < 1 || J.log_n > P.max_log)
+            return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u outside [1, %u]", j, J.log_n, P.max_log);
+        if (J.n_limbs == 0 || (uint64_t)J.first_modulus + J.n_limbs > P.limbs.size())
+            return fail(NTTB_ERR_INVALID_ARG, "batch job %u: limbs [%u, %u) outside the plan's %zu moduli", j,
+                        J.first_modulus, J.first_modulus + J.n_limbs, P.limbs.size());
+        if ((J.flags & NTTB_NEGACYCLIC) && !P.negacyclic)
+            return fail(NTTB_ERR_INVALID_ARG, "batch job %u: negacyclic job on a cyclic plan", j);
+        const uint32_t L = J.log_n, n = 1u << L;
+        const uint32_t uf = ((J.flags & NTTB_BATCH_INVERSE) ? UF_INV : 0u) | ((J.flags & NTTB_NEGACYCLIC) ? UF_NEGA : 0u);
+        if (L <= lgE) {
+            const uint32_t per = std::min<uint32_t>(E >> L, kMaxRows);
+            for (uint32_t l0 = 0; l0 < J.n_limbs; l0 += per) {
+                BUnit u{};
+                u.data = J.data + (size_t)l0 * n;
+                u.mod0 = J.first_modulus + l0;
+                u.log_n = L;
+                u.flags = uf;
+                u.lg1 = 0;
+                u.rows = std::min(per, J.n_limbs - l0);
+                u.tiles_a = 1;
+                u.prev = -1;
+                list.push_back({u, (uint64_t)u.rows * n * L});
+            }
+        } else {
+            uint32_t lg1 = cfg.split ? L / 2 : (L + 1) / 2;
+            if (lg1 > lgE) lg1 = lgE;
+            if (L - lg1 > lgE) lg1 = L - lgE;
+            if (lg1 > lgE || lg1 == 0) return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u too large for tile %u", j, L, E);
+            const uint32_t N1 = 1u << lg1, N2 = n >> lg1;
+            for (uint32_t l = 0; l < J.n_limbs; l++) {
+                BUnit u{};
+                u.data = J.data + (size_t)l * n;
+                u.mod0 = J.first_modulus + l;
+                u.log_n = L;
+                u.flags = uf;
+                u.lg1 = lg1;
+                u.rows = 1;
+                u.va = std::min(E / N1, N2);
+                u.vb = std::min(E / N2, N1);
+                u.tiles_a = N2 / u.va;
+                u.tiles_b = N1 / u.vb;
+                u.prev = -1;
+                list.push_back({u, (uint64_t)n * L});
+            }
+        }
+    }
+    // largest units first
+    std::stable_sort(list.begin(), list.end(), [](const Pending& x, const Pending& y) { return x.work > y.work; });
+    uint32_t max_two = 0, n_two = 0;
+    for (const Pending& p : list)
+        if (p.u.lg1) {
+            max_two = std::max(max_two, 1u << p.u.log_n);
+            n_two++;
+        }
+    const uint32_t lag = cfg.lag;
+    const uint32_t S = n_two ? std::max(lag + 2, std::min<uint32_t>(n_two, std::max<uint32_t>(16, lag + 2))) : 0;
+    units.clear();
+    tiles.clear();
+    std::vector<int32_t> slot_owner(S, -1);
+    std::deque<uint32_t> pend_b;
+    uint32_t two_idx = 0;
+    auto emit_b = [&](uint32_t ui) {
+        for (uint32_t t = 0; t < units[ui].tiles_b; t++) tiles.push_back({ui, 0x80000000u | t});
+    };
+    for (const Pending& p : list) {
+        const uint32_t ui = (uint32_t)units.size();
+        BUnit u = p.u;
+        if (u.lg1) {
+            const uint32_t slot = two_idx++ % S;
+            u.ws = reinterpret_cast<uint32_t*>((uintptr_t)slot * max_two * 4u);  // offset, rebased later
+            u.prev = slot_owner[slot];
+            slot_owner[slot] = (int32_t)ui;
+        }
+        units.push_back(u);
+        for (uint32_t t = 0; t < u.tiles_a; t++) tiles.push_back({ui, t});
+        if (u.lg1) {
+            pend_b.push_back(ui);
+            while (pend_b.size() > lag) {
+                emit_b(pend_b.front());
+                pend_b.pop_front();
+            }
+        }
+    }
+    while (!pend_b.empty()) {
+        emit_b(pend_b.front());
+        pend_b.pop_front();
+    }
+    *ws_words_out = max_two;
+    *slots_out = S;
+    return 0;
+}
+
+int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, const nttb_batch_config& cfg, Batch** out) {
+    if (int rc = check_config(cfg)) return rc;
+    std::vector<BUnit> units;
+    std::vector<BTile> tiles;
+    uint32_t ws_words = 0, slots = 0;
+    if (int rc = plan_batch(*P, jobs, n_jobs, cfg, units, tiles, &ws_words, &slots)) return rc;
+    if (tiles.size() >= 0x7fffffffu || units.size() >= 0x7fffffffu)
+        return fail(NTTB_ERR_INVALID_ARG, "batch: too many tiles");
+    Batch* b = new Batch();
+    b->plan = P;
+    b->cfg = cfg;
+    b->var = find_variant(cfg.tile_elems, cfg.threads);
+    b->n_units = (uint32_t)units.size();
+    b->n_tiles = (uint32_t)tiles.size();
+    b->ws_bytes = (size_t)ws_words * slots * 4;
+    bool ok = true;
+    ok = ok && cudaMalloc(&b->d_units, std::max<size_t>(1, units.size()) * sizeof(BUnit)) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(BTile)) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_ctr, (1 + 2 * (size_t)units.size()) * 4) == cudaSuccess;
+    if (ok && b->ws_bytes) ok = cudaMalloc(&b->d_ws, b->ws_bytes) == cudaSuccess;
+    if (!ok) {
+        free_batch(b);
+        return fail(NTTB_ERR_NO_MEMORY, "batch: device allocation failed");
+    }
+    for (BUnit& u : units)
+        if (u.lg1) u.ws = b->d_ws + (reinterpret_cast<uintptr_t>(u.ws) / 4);
+    ok = cudaMemcpy(b->d_units, units.data(), units.size() * sizeof(BUnit), cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = ok && cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (!ok) {
+        free_batch(b);
+        return fail(NTTB_ERR_CUDA, "batch: upload failed");
+    }
+    const size_t smem = smem_bytes(cfg.tile_elems);
+    cudaFuncSetAttribute(b->var->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->var->fn, (int)cfg.threads, smem);
+    if (occ < 1) occ = 1;
+    if (cfg.ctas_per_sm && (int)cfg.ctas_per_sm < occ) occ = (int)cfg.ctas_per_sm;
+    b->grid = (int)std::min<uint64_t>((uint64_t)sms * occ, std::max<uint32_t>(1, b->n_tiles));
+    *out = b;
+    return 0;
+}
+
+// Counter reset + the persistent launch (no allocation, no host synchronisation).
+int launch_batch(Batch* b, cudaStream_t s, bool count) {
+    if (b->n_tiles == 0) return 0;
+    BArgs a{};
+    a.mods = b->plan->d_mods;
+    a.units = b->d_units;
+    a.tiles = b->d_tiles;
+    a.ctr = b->d_ctr;
+    a.n_tiles = b->n_tiles;
+    a.max_log = b->plan->max_log;
+    if (cudaMemsetAsync(b->d_ctr, 0, (1 + 2 * (size_t)b->n_units) * 4, s) != cudaSuccess)
+        return fail(NTTB_ERR_CUDA, "batch: counter reset failed");
+    if (count) {
+        ProfScope prof("batch_queue", s);
+        b->var->fn<<<b->grid, b->var->T, smem_bytes(b->var->E), s>>>(a);
+    } else {
+        b->var->fn<<<b->grid, b->var->T, smem_bytes(b->var->E), s>>>(a);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(NTTB_ERR_CUDA, "batch: launch failed");
+}
+
+}  // namespace
+
+uint32_t batch_device_errors(bool clear) {
+    uint32_t v = 0;
+    cudaMemcpyFromSymbol(&v, g_batch_error, sizeof v);
+    if (clear) {
+        uint32_t z = 0;
+        cudaMemcpyToSymbol(g_batch_error, &z, sizeof z);
+    }
+    return v;
+}
+
+}  // namespace nttb
+
+using nttb::Batch;
+using nttb::BatchPlan;
+using nttb::fail;
+
+struct nttb_batch_plan {
+    BatchPlan p;
+};
+struct nttb_batch {
+    Batch* b;
+};
+
+extern "C" {
+
+NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, uint32_t max_log_n, uint32_t flags,
+                                    nttb_batch_plan** out) {
+    if (!moduli || !out || n_moduli == 0) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: no moduli");
+    if (max_log_n < 1 || max_log_n > 24) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: max_log_n in [1, 24]");
+    const bool nega = flags & NTTB_NEGACYCLIC;
+    auto* h = new nttb_batch_plan();
+    BatchPlan& P = h->p;
+    P.max_log = max_log_n;
+    P.negacyclic = nega;
+    const uint64_t N = 1ull << max_log_n;
+    P.limbs.resize(n_moduli);
+    for (uint32_t l = 0; l < n_moduli; l++) {
+        std::string why;
+        if (moduli[l] >= (1ull << 31)) {
+            delete h;
+            return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: modulus %u must be < 2^31", l);
+        }
+        if (!nttb::make_limb_host(moduli[l], N, nega, &P.limbs[l], &why)) {
+            delete h;
+            return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: %s", why.c_str());
+        }
+    }
+    const size_t tables = nega ? 4 : 2;
+    std::vector<uint32_t> host(tables * N);
+    std::vector<nttb::BModulus> mods(n_moduli);
+    for (uint32_t l = 0; l < n_moduli; l++) {
+        const nttb::LimbHost& H = P.limbs[l];
+        const uint64_t q = H.q;
+        auto powers = [&](uint32_t* dst, uint64_t base) {
+            uint64_t x = 1;
+            for (uint64_t e = 0; e < N; e++) {
+                dst[e] = nttb::h_to_mont32(x, q);
+                x = nttb::h_mulmod(x, base, q);
+            }
+        };
+        powers(host.data(), H.omega);
+        powers(host.data() + N, H.omega_inv);
+        if (nega) {
+            powers(host.data() + 2 * N, H.psi);
+            powers(host.data() + 3 * N, H.psi_inv);
+        }
+        uint32_t* d = nullptr;
+        if (cudaMalloc(&d, host.size() * 4) != cudaSuccess ||
+            cudaMemcpy(d, host.data(), host.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+            if (d) cudaFree(d);
+            for (void* a : P.allocations) cudaFree(a);
+            delete h;
+            return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_plan_create: twiddle tables");
+        }
+        P.allocations.push_back(d);
+        nttb::BModulus& M = mods[l];
+        M.ar.q = (uint32_t)q;
+        M.ar.qinv = nttb::h_neg_inv32((uint32_t)q);
+        M.tw = d;
+        M.tw_inv = d + N;
+        M.psi = nega ? d + 2 * N : nullptr;
+        M.psi_inv = nega ? d + 3 * N : nullptr;
+        for (uint32_t L = 0; L < 25; L++) M.ninv[L] = nttb::h_to_mont32(nttb::h_invmod((1ull << L) % q, q), q);
+    }
+    if (cudaMalloc(&P.d_mods, mods.size() * sizeof(nttb::BModulus)) != cudaSuccess ||
+        cudaMemcpy(P.d_mods, mods.data(), mods.size() * sizeof(nttb::BModulus), cudaMemcpyHostToDevice) != cudaSuccess) {
+        for (void* a : P.allocations) cudaFree(a);
+        delete h;
+        return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_plan_create: modulus table");
+    }
+    P.allocations.push_back(P.d_mods);
+    *out = h;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_plan_destroy(nttb_batch_plan* plan) {
+    if (!plan) return NTTB_OK;
+    for (void* a : plan->p.allocations) cudaFree(a);
+    delete plan;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_default_config(nttb_batch_config* out) {
+    if (!out) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_default_config: null");
+    *out = nttb::default_config();
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_create(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs,
+                               const nttb_batch_config* config, nttb_batch** out) {
+    if (!plan || !out || (!jobs && n_jobs)) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_create: null argument");
+    const nttb_batch_config cfg = config ? *config : plan->p.have_tuned ? plan->p.tuned : nttb::default_config();
+    Batch* b = nullptr;
+    if (int rc = nttb::create_batch(&plan->p, jobs, n_jobs, cfg, &b)) return rc;
+    *out = new nttb_batch{b};
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_destroy(nttb_batch* batch) {
+    if (!batch) return NTTB_OK;
+    nttb::free_batch(batch->b);
+    delete batch;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_launch(nttb_batch* batch, void* stream) {
+    if (!batch) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_launch: null batch");
+    return nttb::launch_batch(batch->b, static_cast<cudaStream_t>(stream), true);
+}
+
+NTTB_API int nttb_batch_graph_launch(nttb_batch* batch, void* stream) {
+    if (!batch) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_graph_launch: null batch");
+    Batch* b = batch->b;
+    if (b->n_tiles == 0) return NTTB_OK;
+    if (!b->gexec) {
+        if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(NTTB_ERR_CUDA, "nttb_batch_graph_launch: stream");
+        if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return fail(NTTB_ERR_CUDA, "nttb_batch_graph_launch: begin capture");
+        const int rc = nttb::launch_batch(b, b->cap, false);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+        if (rc || e != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            return fail(NTTB_ERR_CUDA, "nttb_batch_graph_launch: capture failed");
+        }
+        b->graph = g;
+        if (cudaGraphInstantiate(&b->gexec, g, 0) != cudaSuccess) {
+            b->gexec = nullptr;
+            return fail(NTTB_ERR_CUDA, "nttb_batch_graph_launch: instantiate failed");
+        }
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    nttb::ProfScope prof("batch_queue_graph", s);
+    return cudaGraphLaunch(b->gexec, s) == cudaSuccess ? NTTB_OK
+                                                        : fail(NTTB_ERR_CUDA, "nttb_batch_graph_launch: launch failed");
+}
+
+NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t* tiles, uint64_t* ws_bytes,
+                             nttb_batch_config* config) {
+    if (!batch) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_info: null batch");
+    if (units) *units = batch->b->n_units;
+    if (tiles) *tiles = batch->b->n_tiles;
+    if (ws_bytes) *ws_bytes = batch->b->ws_bytes;
+    if (config) *config = batch->b->cfg;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs, void* stream,
+                                 nttb_batch_config* out) {
+    if (!plan || !jobs || n_jobs == 0) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: no jobs");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // Sample of the mix: up to two jobs per (log_n, direction, twist), at
+    // most 4 limbs each, on scratch buffers (the caller's data is untouched).
+    std::vector<nttb_batch_job> sample;
+    std::vector<uint32_t> seen(64 * 4, 0);
+    size_t words = 0;
+    for (uint32_t j = 0; j < n_jobs; j++) {
+        const nttb_batch_job& J = jobs[j];
+        if (J.log_n < 1 || J.log_n > plan->p.max_log) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: job %u log_n", j);
+        const uint32_t key = J.log_n * 4 + ((J.flags & NTTB_BATCH_INVERSE) ? 1 : 0) + ((J.flags & NTTB_NEGACYCLIC) ? 2 : 0);
+        if (seen[key] >= 2) continue;
+        seen[key]++;
+        nttb_batch_job c = J;
+        c.n_limbs = std::min<uint32_t>(J.n_limbs, 4);
+        sample.push_back(c);
+        words += (size_t)c.n_limbs << c.log_n;
+    }
+    uint32_t* scratch = nullptr;
+    if (cudaMalloc(&scratch, words * 4) != cudaSuccess) return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_autotune: scratch");
+    cudaMemsetAsync(scratch, 0, words * 4, s);
+    size_t off = 0;
+    for (nttb_batch_job& c : sample) {
+        c.data = scratch + off;
+        off += (size_t)c.n_limbs << c.log_n;
+    }
+    const uint32_t shapes[4][2] = {{4096, 256}, {8192, 256}, {8192, 512}, {16384, 512}};
+    const uint32_t lags[2] = {1, 4};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    nttb_batch_config best_cfg = nttb::default_config();
+    int rc = 0;
+    for (const auto& sh : shapes)
+        for (uint32_t split = 0; split < 2; split++)
+            for (uint32_t lag : lags) {
+                nttb_batch_config c = nttb::default_config();
+                c.tile_elems = sh[0];
+                c.threads = sh[1];
+                c.split = split;
+                c.lag = lag;
+                Batch* b = nullptr;
+                if (nttb::create_batch(&plan->p, sample.data(), (uint32_t)sample.size(), c, &b)) continue;
+                float t_min = 1e30f;
+                for (int it = 0; it < 4 && rc == 0; it++) {
+                    cudaEventRecord(e0, s);
+                    rc = nttb::launch_batch(b, s, false);
+                    cudaEventRecord(e1, s);
+                    cudaEventSynchronize(e1);
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (it > 0) t_min = std::min(t_min, ms);  // the first run warms up
+                }
+                nttb::free_batch(b);
+                if (rc) break;
+                if (t_min < best) {
+                    best = t_min;
+                    best_cfg = c;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(scratch);
+    if (rc) return rc;
+    plan->p.tuned = best_cfg;
+    plan->p.have_tuned = true;
+    if (out) *out = best_cfg;
+    return NTTB_OK;
+}
+
+}  // extern "C"

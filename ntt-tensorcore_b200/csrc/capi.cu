@@ -154,7 +154,7 @@ const char* nttb_last_error(void) { return g_last_error.c_str(); }
 
 int nttb_device_errors(uint32_t* flags, int clear) {
     if (!flags) return fail(NTTB_ERR_INVALID_ARG, "device_errors: null argument");
-    *flags = int8_device_errors(clear != 0);
+    *flags = int8_device_errors(clear != 0) | (batch_device_errors(clear != 0) << 2);
     return cuda_status("device_errors");
 }
 

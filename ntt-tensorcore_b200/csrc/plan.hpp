@@ -116,6 +116,9 @@ uint32_t int8_device_errors(bool clear);
 // Forward then inverse, in place, in one persistent launch.
 int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStream_t s);
 
+// Uneven-batch queue kernel (batch.cu): its bounded-wait error bits.
+uint32_t batch_device_errors(bool clear);
+
 // FP64 DMMA tensor-core engine (tc_dmma.cu).
 bool dmma_serves(const Plan32& p, bool src_u64);
 int dmma_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,

@@ -41,6 +41,21 @@ class _PlanInfo(ctypes.Structure):
                 ("d_twiddles", _vp), ("d_twiddles_inv", _vp), ("params", _Params)]
 
 
+class BatchJob(ctypes.Structure):
+    """nttb_batch_job."""
+    _fields_ = [("data", _vp), ("log_n", _u32), ("n_limbs", _u32), ("first_modulus", _u32), ("flags", _u32)]
+
+
+class BatchConfig(ctypes.Structure):
+    """nttb_batch_config: tile_elems, threads, split, lag, ctas_per_sm."""
+    _fields_ = [("tile_elems", _u32), ("threads", _u32), ("split", _u32), ("lag", _u32), ("ctas_per_sm", _u32)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+BATCH_INVERSE = 2
+
 _lib = None
 
 
@@ -87,6 +102,16 @@ def lib():
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
         "nttb_klimb_forward": (_int, [_u32, _vp, _vp, _u64, _u32, _vp, _u32, _vp]),
+        "nttb_batch_plan_create": (_int, [_vp, _u32, _u32, _u32, ctypes.POINTER(_vp)]),
+        "nttb_batch_plan_destroy": (_int, [_vp]),
+        "nttb_batch_default_config": (_int, [ctypes.POINTER(BatchConfig)]),
+        "nttb_batch_autotune": (_int, [_vp, _vp, _u32, _vp, ctypes.POINTER(BatchConfig)]),
+        "nttb_batch_create": (_int, [_vp, _vp, _u32, ctypes.POINTER(BatchConfig), ctypes.POINTER(_vp)]),
+        "nttb_batch_destroy": (_int, [_vp]),
+        "nttb_batch_launch": (_int, [_vp, _vp]),
+        "nttb_batch_graph_launch": (_int, [_vp, _vp]),
+        "nttb_batch_info": (_int, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64),
+                                   ctypes.POINTER(BatchConfig)]),
         "nttb_device_errors": (_int, [ctypes.POINTER(_u32), _int]),
         "nttb_launch_count": (_int, [ctypes.POINTER(_u64)]),
         "nttb_profile_start": (_int, []),
@@ -130,6 +155,86 @@ def _engine(e):
 
 def version():
     return lib().nttb_version().decode()
+
+
+# ------------------------------------------------------------ uneven batches
+def _jobs(jobs):
+    """(data, log_n, n_limbs, first_modulus, inverse, negacyclic) tuples -> nttb_batch_job[]."""
+    arr = (BatchJob * len(jobs))()
+    for i, (data, log_n, n_limbs, first, inverse, nega) in enumerate(jobs):
+        arr[i] = BatchJob(_ptr(data), log_n, n_limbs, first,
+                          (BATCH_INVERSE if inverse else 0) | (NEGACYCLIC if nega else 0))
+    return arr
+
+
+class BatchPlan:
+    """Twiddle tables for a set of 31-bit moduli up to 2^max_log_n residues;
+    uneven job lists run on it in one persistent launch (nttb_batch_*)."""
+
+    def __init__(self, moduli, max_log_n, negacyclic=False):
+        import numpy as np
+        m = np.ascontiguousarray(moduli, dtype=np.uint64)
+        h = _vp()
+        _check(lib().nttb_batch_plan_create(m.ctypes.data, m.size, max_log_n, NEGACYCLIC if negacyclic else 0,
+                                            ctypes.byref(h)))
+        self._h, self.moduli, self.max_log_n = h, [int(x) for x in m], max_log_n
+
+    def autotune(self, jobs, stream=None):
+        cfg = BatchConfig()
+        arr = _jobs(jobs)
+        _check(lib().nttb_batch_autotune(self._h, arr, len(jobs), _stream(stream), ctypes.byref(cfg)))
+        return cfg.as_dict()
+
+    def batch(self, jobs, config=None):
+        """jobs: (data, log_n, n_limbs, first_modulus, inverse, negacyclic) tuples."""
+        arr = _jobs(jobs)
+        cfg = None
+        if config is not None:
+            cfg = BatchConfig()
+            _check(lib().nttb_batch_default_config(ctypes.byref(cfg)))
+            for k, v in config.items():
+                setattr(cfg, k, int(v))
+        h = _vp()
+        _check(lib().nttb_batch_create(self._h, arr, len(jobs), ctypes.byref(cfg) if cfg else None, ctypes.byref(h)))
+        return Batch(h, self)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nttb_batch_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    def __init__(self, h, plan):
+        self._h, self._plan = h, plan
+
+    def launch(self, stream=None):
+        _check(lib().nttb_batch_launch(self._h, _stream(stream)))
+
+    def graph_launch(self, stream=None):
+        _check(lib().nttb_batch_graph_launch(self._h, _stream(stream)))
+
+    def info(self):
+        u, t, w, cfg = _u64(), _u64(), _u64(), BatchConfig()
+        _check(lib().nttb_batch_info(self._h, ctypes.byref(u), ctypes.byref(t), ctypes.byref(w), ctypes.byref(cfg)))
+        return {"units": int(u.value), "tiles": int(t.value), "ws_bytes": int(w.value), "config": cfg.as_dict()}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nttb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------ K-limb path

@@ -1,0 +1,144 @@
+"""GPU parity of uneven batches (nttb_batch_*: one persistent launch over a
+device work queue) against the oracle, job by job: every job's output equals
+the oracle's RNS transform of that job (same moduli, direction and twist).
+Zero mismatches allowed."""
+import numpy as np
+import pytest
+
+from conftest import to_dev, to_host
+from oracle import oracle as O
+import ntt_b200 as nb
+
+pytestmark = pytest.mark.gpu
+
+PRIMES = nb.generate_primes(31, 21, 12)  # q == 1 mod 2^21: negacyclic up to 2^20
+
+CONFIGS = [
+    None,  # the default
+    {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 1},
+    {"tile_elems": 8192, "threads": 512, "split": 0, "lag": 3},
+    {"tile_elems": 16384, "threads": 512, "split": 1, "lag": 4, "ctas_per_sm": 1},
+]
+
+
+def make_jobs(torch, rng, n_jobs, log_range, limb_range, n_moduli, nega_ok=True):
+    """Random job list: (host array, device tensor, log_n, limbs, first, inverse, nega)."""
+    jobs = []
+    for _ in range(n_jobs):
+        lg = int(rng.integers(log_range[0], log_range[1] + 1))
+        limbs = int(rng.integers(limb_range[0], limb_range[1] + 1))
+        first = int(rng.integers(0, n_moduli - limbs + 1))
+        inv = bool(rng.integers(0, 2))
+        nega = nega_ok and bool(rng.integers(0, 2))
+        x = np.empty((limbs, 1 << lg), dtype=np.uint32)
+        for l in range(limbs):
+            x[l] = rng.integers(0, PRIMES[first + l], 1 << lg, dtype=np.uint64).astype(np.uint32)
+        jobs.append([x, to_dev(torch, x.reshape(-1)), lg, limbs, first, inv, nega])
+    return jobs
+
+
+def spec(jobs):
+    return [(j[1], j[2], j[3], j[4], j[5], j[6]) for j in jobs]
+
+
+def expect(job):
+    x, _, lg, limbs, first, inv, nega = job
+    return O.rns(x[None].astype(np.uint64), PRIMES[first:first + limbs], negacyclic=nega, inverse=inv)[0]
+
+
+def check(torch, jobs):
+    torch.cuda.synchronize()
+    for j in jobs:
+        got = to_host(j[1], np.uint32).reshape(j[0].shape).astype(np.uint64)
+        want = expect(j)
+        assert (got == want).all(), (j[2:], int((got != want).sum()))
+    assert nb.device_errors() == 0
+
+
+@pytest.mark.parametrize("config", CONFIGS)
+def test_batch_mixed_small_sizes(torch_cuda, config):
+    """2^1 .. 2^15 (single-pass tiles with several limbs per tile, and
+    two-pass units for the sizes above the tile), both directions and twists."""
+    rng = np.random.default_rng(7)
+    plan = nb.BatchPlan(PRIMES, 15, negacyclic=True)
+    jobs = make_jobs(torch_cuda, rng, 40, (1, 15), (1, 4), len(PRIMES))
+    b = plan.batch(spec(jobs), config)
+    b.launch()
+    check(torch_cuda, jobs)
+
+
+def test_batch_large_sizes(torch_cuda):
+    """2^16 .. 2^20 two-pass units sharing the workspace ring."""
+    rng = np.random.default_rng(20)
+    plan = nb.BatchPlan(PRIMES, 20, negacyclic=True)
+    jobs = make_jobs(torch_cuda, rng, 10, (16, 20), (1, 2), len(PRIMES))
+    b = plan.batch(spec(jobs), {"tile_elems": 4096, "threads": 256, "split": 0, "lag": 1})
+    info = b.info()
+    assert info["units"] == sum(j[3] for j in jobs)
+    b.launch()
+    check(torch_cuda, jobs)
+
+
+def test_batch_cyclic_plan(torch_cuda):
+    rng = np.random.default_rng(3)
+    plan = nb.BatchPlan(PRIMES[:6], 17, negacyclic=False)
+    jobs = make_jobs(torch_cuda, rng, 16, (2, 17), (1, 3), 6, nega_ok=False)
+    plan.batch(spec(jobs)).launch()
+    check(torch_cuda, jobs)
+
+
+def test_batch_graph_replay(torch_cuda):
+    """The CUDA-graph replay gives the launch's results, on two replays."""
+    rng = np.random.default_rng(11)
+    plan = nb.BatchPlan(PRIMES, 18, negacyclic=True)
+    jobs = make_jobs(torch_cuda, rng, 12, (6, 18), (1, 3), len(PRIMES))
+    b = plan.batch(spec(jobs))
+    for rep in range(2):
+        for j in jobs:  # fresh input in the same buffers
+            j[1].copy_(to_dev(torch_cuda, j[0].reshape(-1)))
+        b.graph_launch()
+        check(torch_cuda, jobs)
+
+
+def test_batch_round_trip_uneven(torch_cuda):
+    """A reduced config-4 mix (log2 N in 12..20, 1..3 limbs): a forward batch
+    then an inverse batch over the same buffers returns the input."""
+    rng = np.random.default_rng(4)
+    plan = nb.BatchPlan(PRIMES, 20, negacyclic=True)
+    jobs = make_jobs(torch_cuda, rng, 24, (12, 20), (1, 3), len(PRIMES))
+    fwd = [(j[1], j[2], j[3], j[4], False, j[6]) for j in jobs]
+    inv = [(j[1], j[2], j[3], j[4], True, j[6]) for j in jobs]
+    plan.batch(fwd).launch()
+    plan.batch(inv).launch()
+    torch_cuda.cuda.synchronize()
+    for j in jobs:
+        assert (to_host(j[1], np.uint32).reshape(j[0].shape) == j[0]).all()
+    assert nb.device_errors() == 0
+
+
+def test_batch_autotune(torch_cuda):
+    rng = np.random.default_rng(5)
+    plan = nb.BatchPlan(PRIMES, 16, negacyclic=True)
+    jobs = make_jobs(torch_cuda, rng, 20, (8, 16), (1, 3), len(PRIMES))
+    before = [to_host(j[1], np.uint32).copy() for j in jobs]
+    cfg = plan.autotune(spec(jobs))
+    assert cfg["tile_elems"] in (4096, 8192, 16384) and cfg["split"] in (0, 1) and cfg["lag"] >= 1
+    for j, b0 in zip(jobs, before):  # autotuning leaves the jobs' data alone
+        assert (to_host(j[1], np.uint32) == b0).all()
+    b = plan.batch(spec(jobs))
+    assert b.info()["config"] == cfg
+    b.launch()
+    check(torch_cuda, jobs)
+
+
+def test_batch_rejects_bad_jobs(torch_cuda):
+    plan = nb.BatchPlan(PRIMES[:4], 12, negacyclic=False)
+    d = torch_cuda.zeros(1 << 14, dtype=torch_cuda.int32, device="cuda")
+    with pytest.raises(nb.NTTError):
+        plan.batch([(d, 13, 1, 0, False, False)])  # log_n above the plan
+    with pytest.raises(nb.NTTError):
+        plan.batch([(d, 10, 3, 2, False, False)])  # moduli 2..4 of 4
+    with pytest.raises(nb.NTTError):
+        plan.batch([(d, 10, 1, 0, False, True)])  # negacyclic job, cyclic plan
+    with pytest.raises(nb.NTTError):
+        plan.batch([(d, 10, 1, 0, False, False)], {"tile_elems": 2048})
