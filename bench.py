@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "int8", "dmma", "scalar"])
+    ap.add_argument("--workload", default="rns", choices=["rns", "uneven"],
+                    help="rns: the 24-limb 2^16 negacyclic batch (headline); uneven: 512 polynomials of "
+                         "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
                     help="warm-up + timed steps only (no clock soak, e2e, comparisons or CPU leg): "
@@ -367,9 +370,120 @@ def run_ours(args, world, rank, local):
     return result, qs
 
 
+# ------------------------------------------------------- uneven workload
+UNEVEN_JOBS = 512
+UNEVEN_WORKLOAD = "uneven_512polys_logN12-20_limbs1-32_mixed_dir"
+
+
+def uneven_jobs(seed=4):
+    """Job shapes: log2 N ~ U{12..20}, limbs ~ U{1..32}, 50% forward / 50% inverse."""
+    rng = np.random.default_rng(seed)
+    lg = rng.integers(12, 21, UNEVEN_JOBS)
+    limbs = rng.integers(1, 33, UNEVEN_JOBS)
+    inv = rng.integers(0, 2, UNEVEN_JOBS)
+    return [(int(a), int(b), bool(c)) for a, b, c in zip(lg, limbs, inv)]
+
+
+def run_uneven(args, world, rank, local):
+    import torch
+    import ntt_b200 as nb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    qs = nb.generate_primes(31, 21, 32)
+    shapes = uneven_jobs()
+    words = sum(b << a for a, b, _ in shapes)
+    buf = torch.empty(words, dtype=torch.int32, device=dev)
+    qt = torch.tensor([int(q) for q in qs], dtype=torch.int64, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(4 + rank)
+    jobs, off = [], 0
+    for lg, limbs, inv in shapes:
+        n = 1 << lg
+        view = buf[off:off + limbs * n].view(limbs, n)
+        r = torch.randint(0, 1 << 31, (limbs, n), generator=gen, device=dev, dtype=torch.int64)
+        view.copy_((r % qt[:limbs, None]).to(torch.int32))
+        jobs.append((view, lg, limbs, 0, inv, False))
+        off += limbs * n
+    torch.cuda.synchronize()
+    coeffs = words  # one transform per residue per launch
+    plan = nb.BatchPlan(qs, 20)
+    tuned = plan.autotune(jobs, stream=stream)
+    batch = plan.batch(jobs)
+    info = batch.info()
+    for _ in range(max(3, args.warmup)):
+        batch.launch(stream)
+    torch.cuda.synchronize()
+    assert nb.device_errors() == 0
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = nb.launch_count()
+        e0.record(stream)
+        for _ in range(steps):
+            fn(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), nb.launch_count() - c0
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_end = time.time() + 1.0
+    while time.time() < t_end:
+        batch.launch(stream)
+        torch.cuda.synchronize()
+    ms, launches = timed(batch.launch, args.steps)
+    clk = clocks.stop()
+    batch.graph_launch(stream)
+    g_ms, _ = timed(batch.graph_launch, args.steps)
+    value = world * coeffs * args.steps / (ms / 1e3)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    avg_s = ms / args.steps / 1e3
+    alg_bytes = 8 * coeffs
+    # units of two passes move each residue twice (through the workspace ring)
+    two_pass = sum(b << a for a, b, _ in shapes if a > {4096: 12, 8192: 13, 16384: 14}[info["config"]["tile_elems"]])
+    model_bytes = 8 * (coeffs - two_pass) + 16 * two_pass
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded uniform residues (generated on the device)",
+        "config": {"workload": UNEVEN_WORKLOAD, "polys": UNEVEN_JOBS, "limbs_total": sum(b for _, b, _ in shapes),
+                   "residues": coeffs, "bytes": 4 * coeffs, "moduli": "32 x 31-bit, q == 1 mod 2^21",
+                   "negacyclic": False, "units": info["units"], "tiles": info["tiles"],
+                   "workspace_bytes": info["ws_bytes"], "tuned": tuned, "l2": "inputs 7.9 GB >> L2",
+                   "parallelism": "replicas x%d" % world},
+        "graph_replay": {"value": world * coeffs * args.steps / (g_ms / 1e3), "ms_per_step": g_ms / args.steps},
+        "roofline": {"bound": "hbm", "kernel": "batch_queue", "achieved": alg_bytes / avg_s / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg_bytes / avg_s / 1e9 / peak, "traffic": None,
+                     "model_bytes_per_launch": model_bytes, "model_frac": model_bytes / avg_s / 1e9 / peak,
+                     "alg_bytes_per_launch": alg_bytes,
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"},
+        "gpu_launches": launches, "clocks": clk, "e2e": None,
+    }
+    batch.close()
+    plan.close()
+    return result
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.workload == "uneven" and args.impl == "ours":
+        r = run_uneven(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(r))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         if rank != 0:
             return

@@ -179,12 +179,19 @@ NTTB_API int nttb_wide_transform(const nttb_wide_plan* plan, uint64_t* d_dst, co
 typedef struct nttb_batch_plan nttb_batch_plan;
 typedef struct nttb_batch nttb_batch;
 #define NTTB_BATCH_INVERSE 2u /* job flag; NTTB_NEGACYCLIC (1) selects the negacyclic twist */
+/* Job flag: product of two polynomials.  data <- a * b (negacyclic with
+ * NTTB_NEGACYCLIC, else cyclic), a = data, b = pointwise (same layout, left
+ * in the NTT domain).  Forward(a), forward(b), the pointwise product and the
+ * inverse run in the same launch; replaces poly_multiply_ntt
+ * (src/ntt_basic.cu:391-409) between ntt_forward and ntt_inverse calls. */
+#define NTTB_BATCH_POLYMUL 4u
 typedef struct {
     uint32_t* data;         /* device memory, n_limbs << log_n words, transformed in place */
     uint32_t log_n;         /* 1 .. plan max_log_n */
     uint32_t n_limbs;
     uint32_t first_modulus; /* row l uses the plan's modulus first_modulus + l */
-    uint32_t flags;         /* NTTB_BATCH_INVERSE | NTTB_NEGACYCLIC */
+    uint32_t flags;         /* NTTB_BATCH_INVERSE | NTTB_NEGACYCLIC | NTTB_BATCH_POLYMUL */
+    uint32_t* pointwise;    /* NTTB_BATCH_POLYMUL: the second operand (overwritten by its transform) */
 } nttb_batch_job;
 /* Tuning knobs (see nttb_batch_autotune). */
 typedef struct {

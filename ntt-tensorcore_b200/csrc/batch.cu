@@ -15,6 +15,12 @@
 // first load and the last store.  This is the scalar engine's two-pass
 // layout, so results are bit-identical to the per-size transforms.
 //
+// Polynomial products (job flag NTTB_BATCH_POLYMUL): each row group becomes
+// three units -- forward(a), forward(b), and inverse(a . b), whose first load
+// multiplies the two spectra (the reference's poly_multiply_ntt,
+// src/ntt_basic.cu:391-409, fused between the passes).  The inverse unit
+// depends on both forward units; all three run in the same launch.
+//
 // The device work queue.  The host lays the tiles out in one array, largest
 // units first; a unit's pass B tiles are placed `lag` two-pass units after its
 // pass A tiles, so CTAs rarely wait.  CTAs of the persistent grid claim tiles
@@ -50,7 +56,8 @@ __device__ uint32_t g_batch_error;
 
 namespace {
 
-constexpr uint32_t BF_INV = 1, BF_PRE_PSI = 2, BF_POST_TW = 4, BF_STORE_T = 8, BF_POST_SCALE = 16, BF_POST_PSI = 32;
+constexpr uint32_t BF_INV = 1, BF_PRE_PSI = 2, BF_POST_TW = 4, BF_STORE_T = 8, BF_POST_SCALE = 16, BF_POST_PSI = 32,
+                   BF_PRE_MUL = 64;
 constexpr uint32_t UF_INV = 1, UF_NEGA = 2;
 constexpr uint32_t kMaxRows = 32;
 
@@ -62,12 +69,13 @@ struct BModulus {
     const uint32_t* psi;      // psi^e R, psi of order 2^(max_log + 1) (negacyclic plans)
     const uint32_t* psi_inv;  // psi^-e R
     uint32_t ninv[25];        // 2^-L R mod q
-    uint32_t pad_;
+    uint32_t r2;              // R^2 mod q (plain product a b = mul(mul(a, b), R^2))
 };
 
 struct BUnit {
     uint32_t* data;    // row 0 of the unit; row r (limb) at data + r n
     uint32_t* ws;      // workspace slot (two-pass units)
+    const uint32_t* pre_mul;  // inverse of a product: the input is data . pre_mul (same layout), else null
     uint32_t mod0;     // modulus index of row 0; row r uses mod0 + r
     uint32_t log_n;
     uint32_t flags;    // UF_INV | UF_NEGA
@@ -76,6 +84,7 @@ struct BUnit {
     uint32_t va, vb;   // vectors per tile in pass A / pass B
     uint32_t tiles_a, tiles_b;
     int32_t prev;      // two-pass unit that held the same workspace slot before, or -1
+    int32_t after[2];  // units that must be complete before this one starts, or -1
 };
 
 struct BTile {
@@ -121,7 +130,8 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
         C = n;
         src = u.data;
         dst = u.data;
-        flags = (nega && !inv ? BF_PRE_PSI : 0u) | (inv ? (nega ? BF_POST_PSI : BF_POST_SCALE) : 0u);
+        flags = (nega && !inv ? BF_PRE_PSI : 0u) | (inv ? (nega ? BF_POST_PSI : BF_POST_SCALE) : 0u) |
+                (u.pre_mul ? BF_PRE_MUL : 0u);
     } else if (pass == 0) {
         row = false;
         lg = u.lg1;
@@ -130,7 +140,7 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
         C = n >> lg;
         src = u.data;
         dst = u.ws;
-        flags = (nega && !inv ? BF_PRE_PSI : 0u) | BF_POST_TW | BF_STORE_T;
+        flags = (nega && !inv ? BF_PRE_PSI : 0u) | BF_POST_TW | BF_STORE_T | (u.pre_mul ? BF_PRE_MUL : 0u);
     } else {
         row = false;
         lg = L - u.lg1;
@@ -170,6 +180,10 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
             elem = (uint32_t)pos;
         }
         uint32_t x = __ldcg(src + pos);
+        if (flags & BF_PRE_MUL) {
+            const M32& ar = s_ar[row ? v : 0u];
+            x = ar.mul(ar.mul(x, __ldcg(u.pre_mul + pos)), a.mods[u.mod0 + (row ? v : 0u)].r2);
+        }
         if (flags & BF_PRE_PSI) {
             const BModulus& M = a.mods[u.mod0 + (row ? v : 0u)];
             x = s_ar[row ? v : 0u].mul(x, __ldg(M.psi + ((size_t)elem << shift)));
@@ -257,8 +271,17 @@ __global__ void __launch_bounds__(T) batch_queue(const __grid_constant__ BArgs a
         const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
         if (threadIdx.x == 0) {
             bool ok = true;
-            if (pass == 1) ok = wait_ge(a.ctr + 1 + 2 * tl.unit, u.tiles_a);
-            else if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, a.units[u.prev].tiles_b);
+            if (pass == 1) {
+                ok = wait_ge(a.ctr + 1 + 2 * tl.unit, u.tiles_a);
+            } else {
+                if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, a.units[u.prev].tiles_b);
+                for (int d = 0; d < 2; d++) {
+                    const int32_t w = u.after[d];
+                    if (w < 0) continue;
+                    const BUnit& W = a.units[w];  // complete = its last pass has signalled every tile
+                    ok = wait_ge(a.ctr + (W.lg1 ? 2u : 1u) + 2 * (uint32_t)w, W.lg1 ? W.tiles_b : W.tiles_a) && ok;
+                }
+            }
             if (!ok) atomicOr(&g_batch_error, 1u);
             __threadfence();
         }
@@ -358,14 +381,67 @@ void free_batch(Batch* b) {
 }
 
 // Units, queue order and workspace ring of one batch (host work only).
+// Units of phase 0 (plain jobs, forward halves of products) come first,
+// largest first; phase 1 holds the inverse units of products, which depend
+// on phase-0 units.  Every pass B tile deferred by the lag is flushed at the
+// phase boundary, so each awaited tile precedes its waiter in the queue.
 int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, const nttb_batch_config& cfg,
                std::vector<BUnit>& units, std::vector<BTile>& tiles, uint32_t* ws_words_out, uint32_t* slots_out) {
     const uint32_t E = cfg.tile_elems, lgE = ilog2(E);
     struct Pending {
         BUnit u;
         uint64_t work;
+        uint32_t phase, id;
+        int32_t after_id[2];
     };
     std::vector<Pending> list;
+    // Units of one transform over rows [l0, l0 + rows) of `data`.
+    auto add_units = [&](uint32_t j, uint32_t* data, const uint32_t* pre_mul, uint32_t L, uint32_t first,
+                         uint32_t n_limbs, uint32_t uf, uint32_t phase, std::vector<uint32_t>* ids,
+                         const std::vector<uint32_t>* dep_a, const std::vector<uint32_t>* dep_b) -> int {
+        const uint32_t n = 1u << L;
+        uint32_t lg1 = 0, per = 1;
+        if (L <= lgE) {
+            per = std::min<uint32_t>(E >> L, kMaxRows);
+        } else {
+            lg1 = cfg.split ? L / 2 : (L + 1) / 2;
+            if (lg1 > lgE) lg1 = lgE;
+            if (L - lg1 > lgE) lg1 = L - lgE;
+            if (lg1 > lgE || lg1 == 0)
+                return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u too large for tile %u", j, L, E);
+        }
+        uint32_t k = 0;
+        for (uint32_t l0 = 0; l0 < n_limbs; l0 += per, k++) {
+            Pending p{};
+            BUnit& u = p.u;
+            u.data = data + (size_t)l0 * n;
+            u.pre_mul = pre_mul ? pre_mul + (size_t)l0 * n : nullptr;
+            u.mod0 = first + l0;
+            u.log_n = L;
+            u.flags = uf;
+            u.lg1 = lg1;
+            u.rows = lg1 ? 1u : std::min(per, n_limbs - l0);
+            if (lg1) {
+                const uint32_t N1 = 1u << lg1, N2 = n >> lg1;
+                u.va = std::min(E / N1, N2);
+                u.vb = std::min(E / N2, N1);
+                u.tiles_a = N2 / u.va;
+                u.tiles_b = N1 / u.vb;
+            } else {
+                u.tiles_a = 1;
+            }
+            u.prev = -1;
+            u.after[0] = u.after[1] = -1;
+            p.work = (uint64_t)u.rows * n * L;
+            p.phase = phase;
+            p.id = (uint32_t)list.size();
+            p.after_id[0] = dep_a ? (int32_t)(*dep_a)[k] : -1;
+            p.after_id[1] = dep_b ? (int32_t)(*dep_b)[k] : -1;
+            if (ids) ids->push_back(p.id);
+            list.push_back(p);
+        }
+        return 0;
+    };
     for (uint32_t j = 0; j < n_jobs; j++) {
         const nttb_batch_job& J = jobs[j];
         if (!J.data) return fail(NTTB_ERR_INVALID_ARG, "batch job %u: null data", j);
@@ -376,47 +452,30 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
                         J.first_modulus, J.first_modulus + J.n_limbs, P.limbs.size());
         if ((J.flags & NTTB_NEGACYCLIC) && !P.negacyclic)
             return fail(NTTB_ERR_INVALID_ARG, "batch job %u: negacyclic job on a cyclic plan", j);
-        const uint32_t L = J.log_n, n = 1u << L;
-        const uint32_t uf = ((J.flags & NTTB_BATCH_INVERSE) ? UF_INV : 0u) | ((J.flags & NTTB_NEGACYCLIC) ? UF_NEGA : 0u);
-        if (L <= lgE) {
-            const uint32_t per = std::min<uint32_t>(E >> L, kMaxRows);
-            for (uint32_t l0 = 0; l0 < J.n_limbs; l0 += per) {
-                BUnit u{};
-                u.data = J.data + (size_t)l0 * n;
-                u.mod0 = J.first_modulus + l0;
-                u.log_n = L;
-                u.flags = uf;
-                u.lg1 = 0;
-                u.rows = std::min(per, J.n_limbs - l0);
-                u.tiles_a = 1;
-                u.prev = -1;
-                list.push_back({u, (uint64_t)u.rows * n * L});
-            }
+        const uint32_t nega = (J.flags & NTTB_NEGACYCLIC) ? UF_NEGA : 0u;
+        if (J.flags & NTTB_BATCH_POLYMUL) {
+            if (!J.pointwise || J.pointwise == J.data)
+                return fail(NTTB_ERR_INVALID_ARG, "batch job %u: a product needs a distinct second operand", j);
+            std::vector<uint32_t> fa, fb;
+            if (int rc = add_units(j, J.data, nullptr, J.log_n, J.first_modulus, J.n_limbs, nega, 0, &fa, nullptr, nullptr)) return rc;
+            if (int rc = add_units(j, const_cast<uint32_t*>(J.pointwise), nullptr, J.log_n, J.first_modulus, J.n_limbs,
+                                   nega, 0, &fb, nullptr, nullptr))
+                return rc;
+            if (int rc = add_units(j, J.data, J.pointwise, J.log_n, J.first_modulus, J.n_limbs, nega | UF_INV, 1,
+                                   nullptr, &fa, &fb))
+                return rc;
         } else {
-            uint32_t lg1 = cfg.split ? L / 2 : (L + 1) / 2;
-            if (lg1 > lgE) lg1 = lgE;
-            if (L - lg1 > lgE) lg1 = L - lgE;
-            if (lg1 > lgE || lg1 == 0) return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u too large for tile %u", j, L, E);
-            const uint32_t N1 = 1u << lg1, N2 = n >> lg1;
-            for (uint32_t l = 0; l < J.n_limbs; l++) {
-                BUnit u{};
-                u.data = J.data + (size_t)l * n;
-                u.mod0 = J.first_modulus + l;
-                u.log_n = L;
-                u.flags = uf;
-                u.lg1 = lg1;
-                u.rows = 1;
-                u.va = std::min(E / N1, N2);
-                u.vb = std::min(E / N2, N1);
-                u.tiles_a = N2 / u.va;
-                u.tiles_b = N1 / u.vb;
-                u.prev = -1;
-                list.push_back({u, (uint64_t)n * L});
-            }
+            const uint32_t uf = ((J.flags & NTTB_BATCH_INVERSE) ? UF_INV : 0u) | nega;
+            if (int rc = add_units(j, J.data, nullptr, J.log_n, J.first_modulus, J.n_limbs, uf, 0, nullptr, nullptr, nullptr))
+                return rc;
         }
     }
-    // largest units first
-    std::stable_sort(list.begin(), list.end(), [](const Pending& x, const Pending& y) { return x.work > y.work; });
+    // phase by phase, largest units first
+    std::stable_sort(list.begin(), list.end(), [](const Pending& x, const Pending& y) {
+        return x.phase != y.phase ? x.phase < y.phase : x.work > y.work;
+    });
+    std::vector<int32_t> index_of(list.size());
+    for (size_t i = 0; i < list.size(); i++) index_of[list[i].id] = (int32_t)i;
     uint32_t max_two = 0, n_two = 0;
     for (const Pending& p : list)
         if (p.u.lg1) {
@@ -429,13 +488,24 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
     tiles.clear();
     std::vector<int32_t> slot_owner(S, -1);
     std::deque<uint32_t> pend_b;
-    uint32_t two_idx = 0;
+    uint32_t two_idx = 0, phase = 0;
     auto emit_b = [&](uint32_t ui) {
         for (uint32_t t = 0; t < units[ui].tiles_b; t++) tiles.push_back({ui, 0x80000000u | t});
     };
+    auto flush = [&]() {
+        while (!pend_b.empty()) {
+            emit_b(pend_b.front());
+            pend_b.pop_front();
+        }
+    };
     for (const Pending& p : list) {
+        if (p.phase != phase) {
+            flush();
+            phase = p.phase;
+        }
         const uint32_t ui = (uint32_t)units.size();
         BUnit u = p.u;
+        for (int d = 0; d < 2; d++) u.after[d] = p.after_id[d] >= 0 ? index_of[p.after_id[d]] : -1;
         if (u.lg1) {
             const uint32_t slot = two_idx++ % S;
             u.ws = reinterpret_cast<uint32_t*>((uintptr_t)slot * max_two * 4u);  // offset, rebased later
@@ -452,10 +522,7 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
             }
         }
     }
-    while (!pend_b.empty()) {
-        emit_b(pend_b.front());
-        pend_b.pop_front();
-    }
+    flush();
     *ws_words_out = max_two;
     *slots_out = S;
     return 0;
@@ -612,6 +679,7 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
         M.psi = nega ? d + 2 * N : nullptr;
         M.psi_inv = nega ? d + 3 * N : nullptr;
         for (uint32_t L = 0; L < 25; L++) M.ninv[L] = nttb::h_to_mont32(nttb::h_invmod((1ull << L) % q, q), q);
+        M.r2 = nttb::h_to_mont32(nttb::h_to_mont32(1, q), q);
     }
     if (cudaMalloc(&P.d_mods, mods.size() * sizeof(nttb::BModulus)) != cudaSuccess ||
         cudaMemcpy(P.d_mods, mods.data(), mods.size() * sizeof(nttb::BModulus), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -704,18 +772,19 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
     // Sample of the mix: up to two jobs per (log_n, direction, twist), at
     // most 4 limbs each, on scratch buffers (the caller's data is untouched).
     std::vector<nttb_batch_job> sample;
-    std::vector<uint32_t> seen(64 * 4, 0);
+    std::vector<uint32_t> seen(64 * 8, 0);
     size_t words = 0;
     for (uint32_t j = 0; j < n_jobs; j++) {
         const nttb_batch_job& J = jobs[j];
         if (J.log_n < 1 || J.log_n > plan->p.max_log) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: job %u log_n", j);
-        const uint32_t key = J.log_n * 4 + ((J.flags & NTTB_BATCH_INVERSE) ? 1 : 0) + ((J.flags & NTTB_NEGACYCLIC) ? 2 : 0);
+        const uint32_t key = J.log_n * 8 + ((J.flags & NTTB_BATCH_INVERSE) ? 1 : 0) + ((J.flags & NTTB_NEGACYCLIC) ? 2 : 0) +
+                             ((J.flags & NTTB_BATCH_POLYMUL) ? 4 : 0);
         if (seen[key] >= 2) continue;
         seen[key]++;
         nttb_batch_job c = J;
         c.n_limbs = std::min<uint32_t>(J.n_limbs, 4);
         sample.push_back(c);
-        words += (size_t)c.n_limbs << c.log_n;
+        words += ((size_t)c.n_limbs << c.log_n) * ((c.flags & NTTB_BATCH_POLYMUL) ? 2 : 1);
     }
     uint32_t* scratch = nullptr;
     if (cudaMalloc(&scratch, words * 4) != cudaSuccess) return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_autotune: scratch");
@@ -724,6 +793,10 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
     for (nttb_batch_job& c : sample) {
         c.data = scratch + off;
         off += (size_t)c.n_limbs << c.log_n;
+        if (c.flags & NTTB_BATCH_POLYMUL) {
+            c.pointwise = scratch + off;
+            off += (size_t)c.n_limbs << c.log_n;
+        }
     }
     const uint32_t shapes[4][2] = {{4096, 256}, {8192, 256}, {8192, 512}, {16384, 512}};
     const uint32_t lags[2] = {1, 4};

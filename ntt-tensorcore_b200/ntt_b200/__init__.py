@@ -43,7 +43,8 @@ class _PlanInfo(ctypes.Structure):
 
 class BatchJob(ctypes.Structure):
     """nttb_batch_job."""
-    _fields_ = [("data", _vp), ("log_n", _u32), ("n_limbs", _u32), ("first_modulus", _u32), ("flags", _u32)]
+    _fields_ = [("data", _vp), ("log_n", _u32), ("n_limbs", _u32), ("first_modulus", _u32), ("flags", _u32),
+                ("pointwise", _vp)]
 
 
 class BatchConfig(ctypes.Structure):
@@ -55,6 +56,7 @@ class BatchConfig(ctypes.Structure):
 
 
 BATCH_INVERSE = 2
+BATCH_POLYMUL = 4
 
 _lib = None
 
@@ -159,11 +161,17 @@ def version():
 
 # ------------------------------------------------------------ uneven batches
 def _jobs(jobs):
-    """(data, log_n, n_limbs, first_modulus, inverse, negacyclic) tuples -> nttb_batch_job[]."""
+    """Job tuples -> nttb_batch_job[].  A transform is (data, log_n, n_limbs,
+    first_modulus, inverse, negacyclic); a product adds its second operand:
+    (a, log_n, n_limbs, first_modulus, "mul", negacyclic, b)."""
     arr = (BatchJob * len(jobs))()
-    for i, (data, log_n, n_limbs, first, inverse, nega) in enumerate(jobs):
-        arr[i] = BatchJob(_ptr(data), log_n, n_limbs, first,
-                          (BATCH_INVERSE if inverse else 0) | (NEGACYCLIC if nega else 0))
+    for i, job in enumerate(jobs):
+        data, log_n, n_limbs, first, kind, nega = job[:6]
+        if kind == "mul":
+            flags, other = BATCH_POLYMUL, _ptr(job[6])
+        else:
+            flags, other = (BATCH_INVERSE if kind else 0), None
+        arr[i] = BatchJob(_ptr(data), log_n, n_limbs, first, flags | (NEGACYCLIC if nega else 0), other)
     return arr
 
 

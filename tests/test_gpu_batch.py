@@ -142,3 +142,40 @@ def test_batch_rejects_bad_jobs(torch_cuda):
         plan.batch([(d, 10, 1, 0, False, True)])  # negacyclic job, cyclic plan
     with pytest.raises(nb.NTTError):
         plan.batch([(d, 10, 1, 0, False, False)], {"tile_elems": 2048})
+
+
+def expect_product(a, b, moduli, nega):
+    """inverse(forward(a) . forward(b)) per limb through the oracle."""
+    fa = O.rns(a[None].astype(np.uint64), moduli, negacyclic=nega)[0]
+    fb = O.rns(b[None].astype(np.uint64), moduli, negacyclic=nega)[0]
+    q = np.array(moduli, dtype=np.uint64)[:, None]
+    return O.rns(((fa * fb) % q)[None], moduli, negacyclic=nega, inverse=True)[0]
+
+
+@pytest.mark.parametrize("nega", [True, False])
+def test_batch_polymul_fused(torch_cuda, nega):
+    """Products (forward a, forward b, pointwise, inverse in one launch) of
+    sizes 2^3 .. 2^17 mixed with plain transforms in the same batch."""
+    rng = np.random.default_rng(17 + nega)
+    plan = nb.BatchPlan(PRIMES, 17, negacyclic=nega)
+    plain = make_jobs(torch_cuda, rng, 8, (3, 17), (1, 3), len(PRIMES), nega_ok=nega)
+    prods = []
+    for _ in range(14):
+        lg = int(rng.integers(3, 18))
+        limbs = int(rng.integers(1, 4))
+        first = int(rng.integers(0, len(PRIMES) - limbs + 1))
+        mods = PRIMES[first:first + limbs]
+        a = np.stack([rng.integers(0, q, 1 << lg, dtype=np.uint64) for q in mods]).astype(np.uint32)
+        b = np.stack([rng.integers(0, q, 1 << lg, dtype=np.uint64) for q in mods]).astype(np.uint32)
+        prods.append((a, b, to_dev(torch_cuda, a.reshape(-1)), to_dev(torch_cuda, b.reshape(-1)), lg, limbs, first))
+    jobs = spec(plain) + [(p[2], p[4], p[5], p[6], "mul", nega, p[3]) for p in prods]
+    plan.batch(jobs).launch()
+    check(torch_cuda, plain)
+    for a, b, da, db, lg, limbs, first in prods:
+        got = to_host(da, np.uint32).reshape(a.shape).astype(np.uint64)
+        want = expect_product(a, b, PRIMES[first:first + limbs], nega)
+        assert (got == want).all(), (lg, limbs, int((got != want).sum()))
+        if nega and lg <= 8:  # against the schoolbook product itself
+            for l in range(limbs):
+                ref = O.polymul_negacyclic(a[l].astype(np.uint64), b[l].astype(np.uint64), PRIMES[first + l])
+                assert (got[l] == ref).all()
