@@ -226,6 +226,50 @@ NTTB_API int nttb_batch_graph_launch(nttb_batch* batch, void* stream);
 NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t* tiles, uint64_t* ws_bytes,
                              nttb_batch_config* config);
 
+/* ------------------------------------------------------------- serving
+ * No reference counterpart (the reference has no request loop).  A server
+ * multiplies polynomials for callers in host memory: request = (a, b) with
+ * n_limbs rows of 2^log_n residues (row l mod moduli[first_modulus + l]),
+ * result out = a * b per limb (negacyclic unless config.negacyclic == 0).
+ * Requests are admitted in arrival order while their device operands
+ * (2 x n_limbs x 2^log_n words) fit in the HBM budget left after the resident
+ * twiddle tables and queues, and are batched continuously: up to `slots`
+ * batches are in flight on separate streams, each one persistent launch
+ * (forward a, forward b, product, inverse) between its copies.  a, b and out
+ * must stay valid until the request completes; pinned host memory lets the
+ * copies overlap.  Latency = submit -> completion, host steady clock. */
+typedef struct nttb_server nttb_server;
+typedef struct {
+    uint64_t hbm_budget_bytes;   /* device bytes for tables, queues and request operands */
+    uint32_t max_log_n;          /* largest request size */
+    uint32_t slots;              /* batches in flight (streams), 1..16 */
+    uint32_t max_batch_requests; /* requests per batch */
+    uint32_t negacyclic;         /* 1: negacyclic products (x^n = -1), 0: cyclic */
+    uint64_t max_batch_residues; /* transform residues per batch (3 per operand residue) */
+    nttb_batch_config batch;     /* tiles of the batch engine */
+} nttb_server_config;
+typedef struct {
+    uint64_t submitted, completed, queued, batches, batched_requests;
+    uint64_t bytes_in_use, peak_bytes_in_use, region_bytes, resident_bytes;
+} nttb_server_stats_t;
+
+/* Defaults: 60 GB budget, 2^17, 3 slots, 64 requests and 2^27 residues per batch, negacyclic. */
+NTTB_API int nttb_server_default_config(nttb_server_config* out);
+NTTB_API int nttb_server_create(const uint64_t* moduli, uint32_t n_moduli, const nttb_server_config* config,
+                                nttb_server** out);
+/* Queues a request; NTTB_ERR_BUDGET if its operands alone exceed the request region. */
+NTTB_API int nttb_server_submit(nttb_server* server, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                                uint32_t log_n, uint32_t n_limbs, uint32_t first_modulus, uint64_t* id);
+/* Waits for one request (NTTB_ERR_TIMEOUT after timeout_s); its latency in seconds. */
+NTTB_API int nttb_server_wait(nttb_server* server, uint64_t id, double timeout_s, double* latency_s);
+NTTB_API int nttb_server_drain(nttb_server* server, double timeout_s);
+NTTB_API int nttb_server_stats(nttb_server* server, nttb_server_stats_t* out);
+/* Latencies of completed requests in completion order (count = how many
+ * there are; up to cap copied); reset != 0 forgets them. */
+NTTB_API int nttb_server_latencies(nttb_server* server, double* out, uint64_t cap, uint64_t* count, int reset);
+/* Drains, then releases the server. */
+NTTB_API int nttb_server_destroy(nttb_server* server);
+
 /* ------------------------------------ K-limb residues (24-bit limbs)
  * The reference's header-only arbitrary-modulus path: elements are
  * DScalar<K> = K little-endian uint32 words, each a 24-bit limb, in

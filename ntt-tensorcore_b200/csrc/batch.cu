@@ -45,6 +45,7 @@
 
 #include "../../include/ntt_b200.h"
 #include "arith.cuh"
+#include "batch.hpp"
 #include "engines.hpp"
 #include "plan.hpp"
 #include "profiler.hpp"
@@ -323,14 +324,8 @@ uint32_t ilog2(uint64_t x) {
 
 }  // namespace
 
-struct BatchPlan {
-    uint32_t max_log = 0;
-    bool negacyclic = false;
-    std::vector<LimbHost> limbs;
-    BModulus* d_mods = nullptr;
-    std::vector<void*> allocations;
-    nttb_batch_config tuned{};
-    bool have_tuned = false;
+struct BatchPlan::Mods {
+    BModulus* d = nullptr;
 };
 
 struct Batch {
@@ -577,7 +572,7 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
 int launch_batch(Batch* b, cudaStream_t s, bool count) {
     if (b->n_tiles == 0) return 0;
     BArgs a{};
-    a.mods = b->plan->d_mods;
+    a.mods = b->plan->mods->d;
     a.units = b->d_units;
     a.tiles = b->d_tiles;
     a.ctr = b->d_ctr;
@@ -596,6 +591,132 @@ int launch_batch(Batch* b, cudaStream_t s, bool count) {
 
 }  // namespace
 
+// ---- runner: repeated batches without per-batch allocation -----------------------
+struct BatchRunner {
+    BatchPlan* plan = nullptr;
+    nttb_batch_config cfg{};
+    const Variant* var = nullptr;
+    BUnit* d_units = nullptr;
+    BTile* d_tiles = nullptr;
+    uint32_t* d_ctr = nullptr;
+    uint32_t* d_ws = nullptr;
+    BUnit* h_units = nullptr;  // pinned staging
+    BTile* h_tiles = nullptr;
+    size_t cap_units = 0, cap_tiles = 0, ws_bytes = 0;
+    int grid = 0;
+    std::vector<BUnit> units;
+    std::vector<BTile> tiles;
+};
+
+namespace {
+void runner_free_queue(BatchRunner* r) {
+    cudaFree(r->d_units);
+    cudaFree(r->d_tiles);
+    cudaFree(r->d_ctr);
+    cudaFreeHost(r->h_units);
+    cudaFreeHost(r->h_tiles);
+    r->d_units = nullptr;
+    r->d_tiles = nullptr;
+    r->d_ctr = nullptr;
+    r->h_units = nullptr;
+    r->h_tiles = nullptr;
+    r->cap_units = r->cap_tiles = 0;
+}
+int runner_reserve(BatchRunner* r, size_t units, size_t tiles) {
+    if (units <= r->cap_units && tiles <= r->cap_tiles) return 0;
+    const size_t cu = std::max(units, r->cap_units * 2), ct = std::max(tiles, r->cap_tiles * 2);
+    runner_free_queue(r);
+    bool ok = cudaMalloc(&r->d_units, cu * sizeof(BUnit)) == cudaSuccess;
+    ok = ok && cudaMalloc(&r->d_tiles, ct * sizeof(BTile)) == cudaSuccess;
+    ok = ok && cudaMalloc(&r->d_ctr, (1 + 2 * cu) * 4) == cudaSuccess;
+    ok = ok && cudaMallocHost(&r->h_units, cu * sizeof(BUnit)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&r->h_tiles, ct * sizeof(BTile)) == cudaSuccess;
+    if (!ok) {
+        runner_free_queue(r);
+        return fail(NTTB_ERR_NO_MEMORY, "batch runner: queue allocation failed");
+    }
+    r->cap_units = cu;
+    r->cap_tiles = ct;
+    return 0;
+}
+}  // namespace
+
+int runner_create(BatchPlan* P, const nttb_batch_config& cfg, BatchRunner** out) {
+    if (int rc = check_config(cfg)) return rc;
+    auto* r = new BatchRunner();
+    r->plan = P;
+    r->cfg = cfg;
+    r->var = find_variant(cfg.tile_elems, cfg.threads);
+    const size_t slots = std::max<size_t>(16, cfg.lag + 2);
+    r->ws_bytes = slots * ((size_t)4 << P->max_log);
+    if (cudaMalloc(&r->d_ws, r->ws_bytes) != cudaSuccess || runner_reserve(r, 256, 4096)) {
+        runner_destroy(r);
+        return fail(NTTB_ERR_NO_MEMORY, "batch runner: allocation failed");
+    }
+    const size_t smem = smem_bytes(cfg.tile_elems);
+    cudaFuncSetAttribute(r->var->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, r->var->fn, (int)cfg.threads, smem);
+    if (occ < 1) occ = 1;
+    if (cfg.ctas_per_sm && (int)cfg.ctas_per_sm < occ) occ = (int)cfg.ctas_per_sm;
+    r->grid = sms * occ;
+    *out = r;
+    return 0;
+}
+
+void runner_destroy(BatchRunner* r) {
+    if (!r) return;
+    runner_free_queue(r);
+    cudaFree(r->d_ws);
+    delete r;
+}
+
+size_t runner_device_bytes(const BatchRunner* r) {
+    return r->ws_bytes + r->cap_units * (sizeof(BUnit) + 8) + r->cap_tiles * sizeof(BTile);
+}
+
+// Plans the jobs, uploads the queue from pinned staging and launches, all on
+// `s`.  One run per runner may be in flight: the staging is reused.
+int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cudaStream_t s) {
+    uint32_t ws_words = 0, slots = 0;
+    if (int rc = plan_batch(*r->plan, jobs, n_jobs, r->cfg, r->units, r->tiles, &ws_words, &slots)) return rc;
+    if ((size_t)ws_words * slots * 4 > r->ws_bytes) return fail(NTTB_ERR_INVALID_ARG, "batch runner: workspace too small");
+    if (r->tiles.empty()) return 0;
+    if (r->units.size() > r->cap_units || r->tiles.size() > r->cap_tiles) {
+        cudaStreamSynchronize(s);  // the previous run may still read the queue
+        if (int rc = runner_reserve(r, r->units.size(), r->tiles.size())) return rc;
+    }
+    for (size_t i = 0; i < r->units.size(); i++) {
+        BUnit u = r->units[i];
+        if (u.lg1) u.ws = r->d_ws + (reinterpret_cast<uintptr_t>(u.ws) / 4);
+        r->h_units[i] = u;
+    }
+    std::memcpy(r->h_tiles, r->tiles.data(), r->tiles.size() * sizeof(BTile));
+    BArgs a{};
+    a.mods = r->plan->mods->d;
+    a.units = r->d_units;
+    a.tiles = r->d_tiles;
+    a.ctr = r->d_ctr;
+    a.n_tiles = (uint32_t)r->tiles.size();
+    a.max_log = r->plan->max_log;
+    bool ok = cudaMemcpyAsync(r->d_units, r->h_units, r->units.size() * sizeof(BUnit), cudaMemcpyHostToDevice, s) ==
+              cudaSuccess;
+    ok = ok && cudaMemcpyAsync(r->d_tiles, r->h_tiles, r->tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice, s) ==
+                   cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->d_ctr, 0, (1 + 2 * r->units.size()) * 4, s) == cudaSuccess;
+    if (!ok) return fail(NTTB_ERR_CUDA, "batch runner: queue upload failed");
+    const int grid = (int)std::min<size_t>((size_t)r->grid, r->tiles.size());
+    ProfScope prof("batch_queue", s);
+    r->var->fn<<<grid, r->var->T, smem_bytes(r->var->E), s>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail(NTTB_ERR_CUDA, "batch runner: launch failed");
+}
+
+size_t batch_plan_device_bytes(const BatchPlan* P) {
+    return (size_t)P->limbs.size() * (P->negacyclic ? 4 : 2) * ((size_t)4 << P->max_log);
+}
+
 uint32_t batch_device_errors(bool clear) {
     uint32_t v = 0;
     cudaMemcpyFromSymbol(&v, g_batch_error, sizeof v);
@@ -612,9 +733,6 @@ using nttb::Batch;
 using nttb::BatchPlan;
 using nttb::fail;
 
-struct nttb_batch_plan {
-    BatchPlan p;
-};
 struct nttb_batch {
     Batch* b;
 };
@@ -628,6 +746,7 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
     const bool nega = flags & NTTB_NEGACYCLIC;
     auto* h = new nttb_batch_plan();
     BatchPlan& P = h->p;
+    P.mods = new BatchPlan::Mods();
     P.max_log = max_log_n;
     P.negacyclic = nega;
     const uint64_t N = 1ull << max_log_n;
@@ -635,10 +754,12 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
     for (uint32_t l = 0; l < n_moduli; l++) {
         std::string why;
         if (moduli[l] >= (1ull << 31)) {
+            delete P.mods;
             delete h;
             return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: modulus %u must be < 2^31", l);
         }
         if (!nttb::make_limb_host(moduli[l], N, nega, &P.limbs[l], &why)) {
+            delete P.mods;
             delete h;
             return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: %s", why.c_str());
         }
@@ -667,6 +788,7 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
             cudaMemcpy(d, host.data(), host.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
             if (d) cudaFree(d);
             for (void* a : P.allocations) cudaFree(a);
+            delete P.mods;
             delete h;
             return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_plan_create: twiddle tables");
         }
@@ -681,13 +803,14 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
         for (uint32_t L = 0; L < 25; L++) M.ninv[L] = nttb::h_to_mont32(nttb::h_invmod((1ull << L) % q, q), q);
         M.r2 = nttb::h_to_mont32(nttb::h_to_mont32(1, q), q);
     }
-    if (cudaMalloc(&P.d_mods, mods.size() * sizeof(nttb::BModulus)) != cudaSuccess ||
-        cudaMemcpy(P.d_mods, mods.data(), mods.size() * sizeof(nttb::BModulus), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (cudaMalloc(&P.mods->d, mods.size() * sizeof(nttb::BModulus)) != cudaSuccess ||
+        cudaMemcpy(P.mods->d, mods.data(), mods.size() * sizeof(nttb::BModulus), cudaMemcpyHostToDevice) != cudaSuccess) {
         for (void* a : P.allocations) cudaFree(a);
+        delete P.mods;
         delete h;
         return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_plan_create: modulus table");
     }
-    P.allocations.push_back(P.d_mods);
+    P.allocations.push_back(P.mods->d);
     *out = h;
     return NTTB_OK;
 }
@@ -695,6 +818,7 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
 NTTB_API int nttb_batch_plan_destroy(nttb_batch_plan* plan) {
     if (!plan) return NTTB_OK;
     for (void* a : plan->p.allocations) cudaFree(a);
+    delete plan->p.mods;
     delete plan;
     return NTTB_OK;
 }

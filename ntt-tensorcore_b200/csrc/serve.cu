@@ -1,0 +1,412 @@
+// serve.cu -- the serving loop: polynomial products (negacyclic by default) of
+// mixed sizes and limb counts, admitted against an HBM budget and batched
+// continuously.
+//
+// A request is (a, b) in host memory: n_limbs rows of 2^log_n residues, row l
+// reduced mod moduli[first_modulus + l]; its result a * b (per limb) goes to
+// `out` in host memory.  Its device footprint is 2 x n_limbs x 2^log_n words
+// (a, with the result written over it, and b).
+//
+// One worker thread owns the device side.  Device memory for requests is one
+// region of (budget - resident tables and queues) bytes, carved first-fit in
+// 256-byte granules.  Whenever a stream slot is free and the queue is not
+// empty, the worker admits requests in arrival order while their operands fit
+// in the region (and the batch stays under max_batch_requests /
+// max_batch_residues), and issues the batch on the slot's stream: host ->
+// device copies of every operand, ONE persistent batch launch (forward a,
+// forward b, pointwise product, inverse, per limb), device -> host copies of
+// the results, and a host callback that stamps the completion time, returns
+// the memory to the region and frees the slot.  Several slots are in flight
+// at once, so a batch's copies and kernels overlap with its neighbours', and
+// requests that arrive while others run are admitted as soon as memory and a
+// slot come free: continuous batching, not a queue drained batch by batch.
+// Latency is submit -> completion callback, on the host's steady clock.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ntt_b200.h"
+#include "batch.hpp"
+#include "engines.hpp"
+
+namespace nttb {
+namespace {
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+constexpr size_t kGranule = 256;
+size_t round_up(size_t x) { return (x + kGranule - 1) / kGranule * kGranule; }
+
+// First-fit allocator over one device region, coalescing on release.
+class Arena {
+   public:
+    void init(size_t bytes) {
+        size_ = bytes / kGranule * kGranule;
+        free_.clear();
+        if (size_) free_[0] = size_;
+    }
+    bool alloc(size_t bytes, size_t* off) {
+        bytes = round_up(bytes);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            const size_t o = it->first, rest = it->second - bytes;
+            free_.erase(it);
+            if (rest) free_[o + bytes] = rest;
+            *off = o;
+            used_ += bytes;
+            peak_ = std::max(peak_, used_);
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        bytes = round_up(bytes);
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    size_t size() const { return size_; }
+    size_t used() const { return used_; }
+    size_t peak() const { return peak_; }
+
+   private:
+    std::map<size_t, size_t> free_;
+    size_t size_ = 0, used_ = 0, peak_ = 0;
+};
+
+struct Req {
+    const uint32_t* a = nullptr;
+    const uint32_t* b = nullptr;
+    uint32_t* out = nullptr;
+    uint32_t log_n = 0, limbs = 0, first = 0;
+    size_t words = 0;  // per operand
+    size_t off = 0;    // device offset of a; b follows
+    double t_submit = 0, t_done = 0;
+    int status = NTTB_OK;
+    bool done = false;
+};
+
+}  // namespace
+}  // namespace nttb
+
+struct nttb_server;
+
+namespace nttb {
+namespace {
+struct Slot {
+    nttb_server* srv = nullptr;
+    cudaStream_t stream = nullptr;
+    BatchRunner* runner = nullptr;
+    bool busy = false;
+    std::vector<uint64_t> ids;
+    std::vector<nttb_batch_job> jobs;
+};
+}  // namespace
+}  // namespace nttb
+
+struct nttb_server {
+    int device = 0;
+    nttb_server_config cfg{};
+    nttb_batch_plan* plan = nullptr;
+    uint8_t* region = nullptr;
+    size_t resident = 0;
+    nttb::Arena arena;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<uint64_t> queue;
+    std::unordered_map<uint64_t, nttb::Req> reqs;
+    uint64_t next_id = 1;
+    std::vector<nttb::Slot> slots;
+    std::thread worker;
+    bool stop = false;
+    uint64_t submitted = 0, completed = 0, batches = 0, batched_requests = 0;
+    std::vector<double> latencies;
+};
+
+namespace nttb {
+namespace {
+
+// Host callback at the end of a batch: no CUDA calls here.
+void CUDART_CB batch_done(void* p) {
+    Slot* sl = static_cast<Slot*>(p);
+    nttb_server* s = sl->srv;
+    std::lock_guard<std::mutex> lk(s->mu);
+    const double t = now_s();
+    for (uint64_t id : sl->ids) {
+        Req& r = s->reqs[id];
+        r.t_done = t;
+        r.done = true;
+        s->arena.release(r.off, 2 * r.words * 4);
+        s->latencies.push_back(t - r.t_submit);
+        s->completed++;
+    }
+    sl->ids.clear();
+    sl->busy = false;
+    s->cv.notify_all();
+}
+
+void worker_main(nttb_server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        auto free_slot = [&]() -> Slot* {
+            for (Slot& sl : s->slots)
+                if (!sl.busy) return &sl;
+            return nullptr;
+        };
+        s->cv.wait(lk, [&] { return s->stop || (!s->queue.empty() && free_slot()); });
+        if (s->stop) break;
+        Slot* sl = free_slot();
+        // admit in arrival order while memory and the batch limits allow
+        std::vector<uint64_t> ids;
+        size_t residues = 0;
+        while (!s->queue.empty() && ids.size() < s->cfg.max_batch_requests) {
+            Req& r = s->reqs[s->queue.front()];
+            if (!ids.empty() && residues + r.words * 3 > s->cfg.max_batch_residues) break;
+            size_t off = 0;
+            if (!s->arena.alloc(2 * r.words * 4, &off)) break;
+            r.off = off;
+            ids.push_back(s->queue.front());
+            residues += r.words * 3;
+            s->queue.pop_front();
+        }
+        if (ids.empty()) {  // memory is full: wait for a batch to finish
+            const uint64_t c0 = s->completed;
+            s->cv.wait(lk, [&] { return s->stop || s->completed != c0; });
+            continue;
+        }
+        sl->busy = true;
+        sl->ids = ids;
+        sl->jobs.clear();
+        std::vector<Req> work;
+        for (uint64_t id : ids) {
+            const Req& r = s->reqs[id];
+            work.push_back(r);
+            nttb_batch_job j{};
+            j.data = reinterpret_cast<uint32_t*>(s->region + r.off);
+            j.pointwise = j.data + r.words;
+            j.log_n = r.log_n;
+            j.n_limbs = r.limbs;
+            j.first_modulus = r.first;
+            j.flags = NTTB_BATCH_POLYMUL | (s->cfg.negacyclic ? NTTB_NEGACYCLIC : 0u);
+            sl->jobs.push_back(j);
+        }
+        s->batches++;
+        s->batched_requests += ids.size();
+        lk.unlock();
+        // issue the batch on the slot's stream (no lock held: CUDA calls)
+        bool ok = true;
+        for (size_t i = 0; i < work.size() && ok; i++) {
+            const size_t bytes = work[i].words * 4;
+            ok = cudaMemcpyAsync(sl->jobs[i].data, work[i].a, bytes, cudaMemcpyHostToDevice, sl->stream) == cudaSuccess &&
+                 cudaMemcpyAsync(sl->jobs[i].pointwise, work[i].b, bytes, cudaMemcpyHostToDevice, sl->stream) ==
+                     cudaSuccess;
+        }
+        ok = ok && runner_run(sl->runner, sl->jobs.data(), (uint32_t)sl->jobs.size(), sl->stream) == 0;
+        for (size_t i = 0; i < work.size() && ok; i++)
+            ok = cudaMemcpyAsync(work[i].out, sl->jobs[i].data, work[i].words * 4, cudaMemcpyDeviceToHost,
+                                 sl->stream) == cudaSuccess;
+        ok = ok && cudaLaunchHostFunc(sl->stream, batch_done, sl) == cudaSuccess;
+        lk.lock();
+        if (!ok) {  // nothing will call back: fail the batch's requests here
+            for (uint64_t id : ids) s->reqs[id].status = NTTB_ERR_CUDA;
+            lk.unlock();
+            cudaStreamSynchronize(sl->stream);
+            batch_done(sl);
+            lk.lock();
+        }
+    }
+}
+
+}  // namespace
+}  // namespace nttb
+
+using nttb::fail;
+
+extern "C" {
+
+NTTB_API int nttb_server_default_config(nttb_server_config* out) {
+    if (!out) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_default_config: null");
+    *out = nttb_server_config{};
+    out->hbm_budget_bytes = 60ull << 30;
+    out->max_log_n = 17;
+    out->slots = 3;
+    out->max_batch_requests = 64;
+    out->negacyclic = 1;
+    out->max_batch_residues = 1ull << 27;
+    nttb_batch_default_config(&out->batch);
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_server_create(const uint64_t* moduli, uint32_t n_moduli, const nttb_server_config* cfg,
+                                nttb_server** out) {
+    if (!cfg || !out) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_create: null argument");
+    if (cfg->slots < 1 || cfg->slots > 16) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_create: slots in [1, 16]");
+    if (cfg->max_batch_requests < 1 || cfg->max_batch_residues < 1)
+        return fail(NTTB_ERR_INVALID_ARG, "nttb_server_create: batch limits must be positive");
+    auto* s = new nttb_server();
+    s->cfg = *cfg;
+    cudaGetDevice(&s->device);
+    if (int rc = nttb_batch_plan_create(moduli, n_moduli, cfg->max_log_n, cfg->negacyclic ? NTTB_NEGACYCLIC : 0,
+                                        &s->plan)) {
+        delete s;
+        return rc;
+    }
+    s->resident = nttb::batch_plan_device_bytes(&s->plan->p);
+    s->slots.resize(cfg->slots);
+    for (nttb::Slot& sl : s->slots) {
+        sl.srv = s;
+        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            nttb::runner_create(&s->plan->p, cfg->batch, &sl.runner)) {
+            for (nttb::Slot& t : s->slots) {
+                if (t.runner) nttb::runner_destroy(t.runner);
+                if (t.stream) cudaStreamDestroy(t.stream);
+            }
+            nttb_batch_plan_destroy(s->plan);
+            delete s;
+            return fail(NTTB_ERR_NO_MEMORY, "nttb_server_create: stream slots");
+        }
+        s->resident += nttb::runner_device_bytes(sl.runner);
+    }
+    if (cfg->hbm_budget_bytes <= s->resident + (1u << 20)) {
+        for (nttb::Slot& t : s->slots) {
+            nttb::runner_destroy(t.runner);
+            cudaStreamDestroy(t.stream);
+        }
+        nttb_batch_plan_destroy(s->plan);
+        const size_t res = s->resident;
+        delete s;
+        return fail(NTTB_ERR_BUDGET, "nttb_server_create: budget below the resident tables and queues (%zu bytes)", res);
+    }
+    const size_t region = cfg->hbm_budget_bytes - s->resident;
+    if (cudaMalloc(&s->region, region) != cudaSuccess) {
+        for (nttb::Slot& t : s->slots) {
+            nttb::runner_destroy(t.runner);
+            cudaStreamDestroy(t.stream);
+        }
+        nttb_batch_plan_destroy(s->plan);
+        delete s;
+        return fail(NTTB_ERR_NO_MEMORY, "nttb_server_create: request region of %zu bytes", region);
+    }
+    s->arena.init(region);
+    s->worker = std::thread(nttb::worker_main, s);
+    *out = s;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_server_submit(nttb_server* s, const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t log_n,
+                                uint32_t n_limbs, uint32_t first_modulus, uint64_t* id) {
+    if (!s || !a || !b || !out || !id) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: null argument");
+    if (log_n < 1 || log_n > s->cfg.max_log_n)
+        return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: log_n %u outside [1, %u]", log_n, s->cfg.max_log_n);
+    if (n_limbs == 0 || (uint64_t)first_modulus + n_limbs > s->plan->p.limbs.size())
+        return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: limbs outside the server's moduli");
+    nttb::Req r;
+    r.a = a;
+    r.b = b;
+    r.out = out;
+    r.log_n = log_n;
+    r.limbs = n_limbs;
+    r.first = first_modulus;
+    r.words = (size_t)n_limbs << log_n;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (nttb::round_up(2 * r.words * 4) > s->arena.size())
+        return fail(NTTB_ERR_BUDGET, "nttb_server_submit: %zu bytes exceed the HBM budget's request region (%zu)",
+                    2 * r.words * 4, s->arena.size());
+    r.t_submit = nttb::now_s();
+    *id = s->next_id++;
+    s->reqs[*id] = r;
+    s->queue.push_back(*id);
+    s->submitted++;
+    s->cv.notify_all();
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_server_wait(nttb_server* s, uint64_t id, double timeout_s, double* latency_s) {
+    if (!s) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_wait: null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_wait: unknown request %llu", (unsigned long long)id);
+    const bool done = s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return s->reqs[id].done; });
+    if (!done) return fail(NTTB_ERR_TIMEOUT, "nttb_server_wait: request %llu not done", (unsigned long long)id);
+    const nttb::Req r = s->reqs[id];
+    s->reqs.erase(id);
+    if (latency_s) *latency_s = r.t_done - r.t_submit;
+    return r.status == NTTB_OK ? NTTB_OK : fail(r.status, "nttb_server_wait: request %llu failed", (unsigned long long)id);
+}
+
+NTTB_API int nttb_server_drain(nttb_server* s, double timeout_s) {
+    if (!s) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_drain: null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    const bool ok = s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                   [&] { return s->completed == s->submitted; });
+    return ok ? NTTB_OK : fail(NTTB_ERR_TIMEOUT, "nttb_server_drain: requests still pending");
+}
+
+NTTB_API int nttb_server_stats(nttb_server* s, nttb_server_stats_t* out) {
+    if (!s || !out) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_stats: null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->submitted = s->submitted;
+    out->completed = s->completed;
+    out->queued = s->queue.size();
+    out->batches = s->batches;
+    out->batched_requests = s->batched_requests;
+    out->bytes_in_use = s->arena.used();
+    out->peak_bytes_in_use = s->arena.peak();
+    out->region_bytes = s->arena.size();
+    out->resident_bytes = s->resident;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_server_latencies(nttb_server* s, double* out, uint64_t cap, uint64_t* count, int reset) {
+    if (!s || !count) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_latencies: null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    *count = s->latencies.size();
+    if (out)
+        for (uint64_t i = 0; i < cap && i < s->latencies.size(); i++) out[i] = s->latencies[i];
+    if (reset) s->latencies.clear();
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_server_destroy(nttb_server* s) {
+    if (!s) return NTTB_OK;
+    nttb_server_drain(s, 600.0);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    s->worker.join();
+    for (nttb::Slot& sl : s->slots) {
+        cudaStreamSynchronize(sl.stream);
+        nttb::runner_destroy(sl.runner);
+        cudaStreamDestroy(sl.stream);
+    }
+    cudaFree(s->region);
+    nttb_batch_plan_destroy(s->plan);
+    delete s;
+    return NTTB_OK;
+}
+
+}  // extern "C"

@@ -19,6 +19,7 @@ OK = 0
 ENGINE_AUTO, ENGINE_SCALAR, ENGINE_DMMA, ENGINE_INT8 = 0, 1, 2, 3
 ENGINES = {"auto": ENGINE_AUTO, "scalar": ENGINE_SCALAR, "dmma": ENGINE_DMMA, "int8": ENGINE_INT8}
 NEGACYCLIC = 1
+ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_NO_MEMORY, ERR_TIMEOUT, ERR_BUDGET = 1, 2, 3, 4, 5, 6
 
 _u64 = ctypes.c_uint64
 _u32 = ctypes.c_uint32
@@ -53,6 +54,18 @@ class BatchConfig(ctypes.Structure):
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+class ServerConfig(ctypes.Structure):
+    """nttb_server_config."""
+    _fields_ = [("hbm_budget_bytes", _u64), ("max_log_n", _u32), ("slots", _u32), ("max_batch_requests", _u32),
+                ("negacyclic", _u32), ("max_batch_residues", _u64), ("batch", BatchConfig)]
+
+
+class ServerStats(ctypes.Structure):
+    """nttb_server_stats_t."""
+    _fields_ = [(f, _u64) for f in ("submitted", "completed", "queued", "batches", "batched_requests",
+                                    "bytes_in_use", "peak_bytes_in_use", "region_bytes", "resident_bytes")]
 
 
 BATCH_INVERSE = 2
@@ -104,6 +117,14 @@ def lib():
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
         "nttb_klimb_forward": (_int, [_u32, _vp, _vp, _u64, _u32, _vp, _u32, _vp]),
+        "nttb_server_default_config": (_int, [ctypes.POINTER(ServerConfig)]),
+        "nttb_server_create": (_int, [_vp, _u32, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
+        "nttb_server_submit": (_int, [_vp, _vp, _vp, _vp, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
+        "nttb_server_wait": (_int, [_vp, _u64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+        "nttb_server_drain": (_int, [_vp, ctypes.c_double]),
+        "nttb_server_stats": (_int, [_vp, ctypes.POINTER(ServerStats)]),
+        "nttb_server_latencies": (_int, [_vp, _vp, _u64, ctypes.POINTER(_u64), _int]),
+        "nttb_server_destroy": (_int, [_vp]),
         "nttb_batch_plan_create": (_int, [_vp, _u32, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_batch_plan_destroy": (_int, [_vp]),
         "nttb_batch_default_config": (_int, [ctypes.POINTER(BatchConfig)]),
@@ -237,6 +258,76 @@ class Batch:
         if getattr(self, "_h", None):
             lib().nttb_batch_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- serving
+class Server:
+    """Polynomial-product server (nttb_server_*): requests are host arrays
+    (numpy, or pinned torch CPU tensors) of n_limbs x 2^log_n residues."""
+
+    def __init__(self, moduli, **config):
+        import numpy as np
+        cfg = ServerConfig()
+        _check(lib().nttb_server_default_config(ctypes.byref(cfg)))
+        for k, v in config.items():
+            if k == "batch":
+                for bk, bv in v.items():
+                    setattr(cfg.batch, bk, int(bv))
+            else:
+                setattr(cfg, k, int(v))
+        m = np.ascontiguousarray(moduli, dtype=np.uint64)
+        h = _vp()
+        _check(lib().nttb_server_create(m.ctypes.data, m.size, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h, self._keep, self.moduli = h, {}, [int(x) for x in m]
+
+    @staticmethod
+    def _addr(x):
+        if hasattr(x, "data_ptr"):
+            return x.data_ptr()
+        return x.ctypes.data
+
+    def submit(self, a, b, out, log_n, n_limbs, first_modulus=0):
+        i = _u64()
+        _check(lib().nttb_server_submit(self._h, self._addr(a), self._addr(b), self._addr(out), log_n, n_limbs,
+                                        first_modulus, ctypes.byref(i)))
+        self._keep[int(i.value)] = (a, b, out)
+        return int(i.value)
+
+    def wait(self, rid, timeout=60.0):
+        lat = ctypes.c_double()
+        try:
+            _check(lib().nttb_server_wait(self._h, rid, timeout, ctypes.byref(lat)))
+        finally:
+            self._keep.pop(rid, None)
+        return lat.value
+
+    def drain(self, timeout=600.0):
+        _check(lib().nttb_server_drain(self._h, timeout))
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().nttb_server_stats(self._h, ctypes.byref(st)))
+        return {f: int(getattr(st, f)) for f, _ in st._fields_}
+
+    def latencies(self, reset=False):
+        import numpy as np
+        n = _u64()
+        _check(lib().nttb_server_latencies(self._h, None, 0, ctypes.byref(n), 0))
+        out = np.zeros(max(1, n.value), dtype=np.float64)
+        _check(lib().nttb_server_latencies(self._h, out.ctypes.data, out.size, ctypes.byref(n), int(reset)))
+        return out[:n.value]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nttb_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
 
     def __del__(self):
         try:
