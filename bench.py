@@ -45,9 +45,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "int8", "dmma", "scalar"])
-    ap.add_argument("--workload", default="rns", choices=["rns", "uneven"],
+    ap.add_argument("--workload", default="rns", choices=["rns", "uneven", "serve"],
                     help="rns: the 24-limb 2^16 negacyclic batch (headline); uneven: 512 polynomials of "
-                         "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch")
+                         "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch; "
+                         "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
                     help="warm-up + timed steps only (no clock soak, e2e, comparisons or CPU leg): "
@@ -473,11 +475,130 @@ def run_uneven(args, world, rank, local):
     return result
 
 
+# --------------------------------------------------------- serving workload
+SERVE_WORKLOAD = "serve_negacyclic_polymul_logN12-17_limbs4-48_60GB"
+
+
+def run_serve(args, world, rank, local):
+    """Closed loop at saturation (at most `outstanding` requests in flight)
+    for the peak rate, then open-loop Poisson arrivals at 25/50/80/100% of
+    it; latency = submit -> completion per request."""
+    import threading
+    import torch
+    import ntt_b200 as nb
+
+    torch.cuda.set_device(local)
+    qs = nb.generate_primes(31, 18, 48)
+    rng = np.random.default_rng(5 + rank)
+    pool_n, outstanding = 96, 64
+    pool = []
+    for _ in range(pool_n):
+        lg = int(rng.integers(12, 18))
+        limbs = int(rng.integers(4, 49))
+        first = int(rng.integers(0, 48 - limbs + 1))
+        mods = np.array(qs[first:first + limbs], dtype=np.uint64)[:, None]
+        a = torch.from_numpy((rng.integers(0, 1 << 62, (limbs, 1 << lg), dtype=np.uint64) % mods)
+                             .astype(np.uint32).view(np.int32)).pin_memory()
+        b = torch.from_numpy((rng.integers(0, 1 << 62, (limbs, 1 << lg), dtype=np.uint64) % mods)
+                             .astype(np.uint32).view(np.int32)).pin_memory()
+        pool.append((a, b, lg, limbs, first))
+    # tile configuration tuned on this request mix
+    tplan = nb.BatchPlan(qs, 17, negacyclic=True)
+    sample = []
+    for a, b, lg, limbs, first in pool[:24]:
+        da, db = a.cuda(), b.cuda()
+        sample.append((da, lg, limbs, first, "mul", True, db))
+    tuned = tplan.autotune(sample)
+    del sample
+    tplan.close()
+    budget = 60 << 30
+    srv = nb.Server(qs, hbm_budget_bytes=budget, max_log_n=17, slots=3, max_batch_requests=64,
+                    max_batch_residues=1 << 27, batch=tuned)
+    coeffs = [3 * limbs << lg for _, _, lg, limbs, _ in pool]  # transforms per request
+
+    def phase(rate, seconds):
+        """rate None: closed loop; else Poisson arrivals at `rate` requests/s."""
+        srv.latencies(reset=True)
+        ids, done = [], [0]
+        lock = threading.Condition()
+        stop = [False]
+
+        def reaper():
+            k = 0
+            while True:
+                with lock:
+                    while k >= len(ids) and not stop[0]:
+                        lock.wait(0.05)
+                    if k >= len(ids) and stop[0]:
+                        return
+                    rid = ids[k]
+                srv.wait(rid, 120.0)
+                k += 1
+                with lock:
+                    done[0] = k
+                    lock.notify_all()
+
+        th = threading.Thread(target=reaper)
+        th.start()
+        t0 = time.perf_counter()
+        nxt, i, work = t0, 0, 0
+        arr = np.random.default_rng(99)
+        while time.perf_counter() - t0 < seconds:
+            if rate is None:
+                with lock:
+                    while len(ids) - done[0] >= outstanding:
+                        lock.wait(0.01)
+            else:
+                nxt += arr.exponential(1.0 / rate)
+                dt = nxt - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+            a, b, lg, limbs, first = pool[i % pool_n]
+            rid = srv.submit(a, b, a, lg, limbs, first)  # result over a (the pool keeps residues < q)
+            work += coeffs[i % pool_n]
+            with lock:
+                ids.append(rid)
+                lock.notify_all()
+            i += 1
+        t_sub = time.perf_counter() - t0
+        with lock:
+            stop[0] = True
+            lock.notify_all()
+        th.join()
+        t_all = time.perf_counter() - t0
+        lat = np.sort(srv.latencies(reset=True)) * 1e3
+        return {"offered_rps": None if rate is None else rate, "requests": i,
+                "achieved_rps": i / t_all, "coeffs_per_s": work / t_all, "submit_s": t_sub,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "mean_ms": float(lat.mean())}
+
+    phase(None, 1.0)  # warm-up
+    sat = phase(None, args.serve_seconds)
+    peak = sat["achieved_rps"]
+    levels = {}
+    for frac in (0.25, 0.5, 0.8, 1.0):
+        levels["%d%%" % int(frac * 100)] = phase(frac * peak, args.serve_seconds)
+    st = srv.stats()
+    srv.close()
+    return {
+        "metric": METRIC, "value": sat["coeffs_per_s"], "unit": UNIT, "n_gpus": world, "steps": sat["requests"],
+        "warmup": 1, "ms_per_step": 1e3 / sat["achieved_rps"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded uniform residues, pinned host buffers",
+        "config": {"workload": SERVE_WORKLOAD, "n": "2^12..2^17", "limbs": "4..48", "moduli": "48 x 31-bit",
+                   "budget_bytes": budget, "slots": 3, "max_batch_requests": 64, "tuned": tuned,
+                   "closed_loop_outstanding": outstanding, "parallelism": "replicas x%d" % world},
+        "serve": {"saturated": sat, "load_levels": levels, "batches": st["batches"],
+                  "mean_batch_requests": st["batched_requests"] / max(1, st["batches"]),
+                  "peak_region_bytes_in_use": st["peak_bytes_in_use"], "resident_bytes": st["resident_bytes"]},
+        "e2e": {"value": sat["coeffs_per_s"], "unit": UNIT, "note": "host buffers in, host buffers out"},
+    }
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
-    if args.workload == "uneven" and args.impl == "ours":
-        r = run_uneven(args, world, rank, local)
+    if args.workload in ("uneven", "serve") and args.impl == "ours":
+        r = run_uneven(args, world, rank, local) if args.workload == "uneven" else run_serve(args, world, rank, local)
         if rank == 0:
             print(json.dumps(r))
         if world > 1:
