@@ -50,6 +50,8 @@ def parse():
                          "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch; "
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
+    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch"], default=None,
+                    help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
                     help="warm-up + timed steps only (no clock soak, e2e, comparisons or CPU leg): "
@@ -594,8 +596,47 @@ def run_serve(args, world, rank, local):
     }
 
 
+# ----------------------------------------------------- small profiling cases
+def profile_case(name):
+    """Small, self-checking cases for ncu captures (a few launches, < 1 GB):
+    int8 / dmma: forward+inverse of the 24-limb 2^16 negacyclic batch, four
+    launches; batch: a ~600 MB uneven batch (log2 N 12..20, 1..8 limbs, mixed
+    directions) launched twice."""
+    import torch
+    import ntt_b200 as nb
+    if name in ("int8", "dmma"):
+        qs = nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
+        plan = nb.RnsPlan(LOG_N, qs, negacyclic=True)
+        x = make_batch(qs, 7)
+        d = torch.from_numpy(x.reshape(-1).view(np.int32)).cuda()
+        for _ in range(4):
+            plan.forward_inverse(d, 1, engine=name)
+        torch.cuda.synchronize()
+        assert (d.cpu().numpy().view(np.uint32).reshape(x.shape) == x).all()
+    else:
+        qs = nb.generate_primes(31, 21, 8)
+        rng = np.random.default_rng(1)
+        jobs, bufs, words = [], [], 0
+        while words < 150_000_000:
+            lg, limbs = int(rng.integers(12, 21)), int(rng.integers(1, 9))
+            t = torch.randint(0, 1 << 30, (limbs << lg,), dtype=torch.int32, device="cuda") % int(min(qs))
+            bufs.append(t)
+            words += limbs << lg
+            jobs.append((t, lg, limbs, 0, bool(rng.integers(0, 2)), False))
+        plan = nb.BatchPlan(qs, 20)
+        b = plan.batch(jobs, {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 4})
+        b.launch()
+        b.launch()
+        torch.cuda.synchronize()
+        assert nb.device_errors() == 0
+    print("profile case %s ok" % name)
+
+
 def main():
     args = parse()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     world, rank, local = dist_setup(args)
     if args.workload in ("uneven", "serve") and args.impl == "ours":
         r = run_uneven(args, world, rank, local) if args.workload == "uneven" else run_serve(args, world, rank, local)
