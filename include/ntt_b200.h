@@ -200,6 +200,7 @@ typedef struct {
     uint32_t split;       /* two-pass radix split: 0 first pass 2^ceil(L/2), 1 first pass 2^floor(L/2) */
     uint32_t lag;         /* two-pass units between a unit's first and second pass in the queue (1..64) */
     uint32_t ctas_per_sm; /* 0: as many as fit */
+    uint32_t group;       /* radix-2 stages per register group inside a tile: 1, 3 or 4 */
 } nttb_batch_config;
 
 /* flags: NTTB_NEGACYCLIC to allow negacyclic jobs (moduli then need 2^(max_log_n+1) | q-1). */

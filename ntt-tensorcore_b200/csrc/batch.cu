@@ -31,10 +31,17 @@
 // running: no deadlock.  Workspace slots form a ring of S > lag slots, so the
 // workspace is S x (largest unit), not the size of the batch.
 //
+// Inside a tile, radix-2 stages run in register groups of 1, 3 or 4: one
+// thread loads the 2, 8 or 16 elements that a group's stages combine,
+// applies the group's butterflies in registers and stores them once -- one
+// barrier and one shared-memory round trip per group.  Twiddles and twists
+// come from two-level power tables (8 KB per base and modulus, L2-resident).
+//
 // Tuning knobs (nttb_batch_config): shared-memory tile size and CTA width
-// (4096/256, 8192/256, 8192/512, 16384/512), the radix split of two-pass
-// units (first pass 2^ceil(L/2) or 2^floor(L/2)), the queue lag and the CTAs
-// per SM; nttb_batch_autotune times the candidates on a sample of the job mix.
+// (4096/256, 8192/256, 8192/512, 16384/512), stages per register group (3,
+// 4, or 1 = stage by stage), the radix split of two-pass units (first pass 2^ceil(L/2) or
+// 2^floor(L/2)), the queue lag and the CTAs per SM; nttb_batch_autotune
+// times the candidates on a sample of the job mix.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -62,16 +69,27 @@ constexpr uint32_t BF_INV = 1, BF_PRE_PSI = 2, BF_POST_TW = 4, BF_STORE_T = 8, B
 constexpr uint32_t UF_INV = 1, UF_NEGA = 2;
 constexpr uint32_t kMaxRows = 32;
 
+// Power tables: x^e R for e < 2^max_log as hi[e >> kLoBits] * lo[e & lo_mask]
+// (one exact Montgomery product), 2 x 4 KB-ish per base instead of 4 MB, so
+// the tables of every modulus stay resident in L2.  Bases: 0 omega (order
+// 2^max_log), 1 omega^-1, 2 psi (order 2^(max_log + 1), negacyclic plans),
+// 3 psi^-1.
+constexpr uint32_t kLoBits = 10;
+enum : uint32_t { PW_OMEGA = 0, PW_OMEGA_INV = 1, PW_PSI = 2, PW_PSI_INV = 3 };
+
 // Per-modulus device constants at the plan's largest size 2^max_log.
 struct BModulus {
     M32 ar;
-    const uint32_t* tw;       // omega^e R, e < 2^max_log (omega of order 2^max_log)
-    const uint32_t* tw_inv;   // omega^-e R
-    const uint32_t* psi;      // psi^e R, psi of order 2^(max_log + 1) (negacyclic plans)
-    const uint32_t* psi_inv;  // psi^-e R
+    const uint32_t* pw;       // 4 bases x [hi (2^(max_log - lo_bits)) | lo (2^lo_bits)]
+    uint32_t lo_bits, hi_len; // lo_bits = min(kLoBits, max_log)
     uint32_t ninv[25];        // 2^-L R mod q
     uint32_t r2;              // R^2 mod q (plain product a b = mul(mul(a, b), R^2))
 };
+
+__device__ __forceinline__ uint32_t pw(const BModulus& M, const M32& ar, uint32_t base, uint32_t e) {
+    const uint32_t* t = M.pw + base * (M.hi_len + (1u << M.lo_bits));
+    return ar.mul(__ldg(t + (e >> M.lo_bits)), __ldg(t + M.hi_len + (e & ((1u << M.lo_bits) - 1))));
+}
 
 struct BUnit {
     uint32_t* data;    // row 0 of the unit; row r (limb) at data + r n
@@ -114,7 +132,7 @@ __device__ __forceinline__ bool wait_ge(const uint32_t* p, uint32_t target) {
 // One tile: V vectors of length len, in shared memory.  COL mode (DIT after
 // a bit-reversed load): vectors are columns vec of a [len][C] matrix; ROW
 // mode (DIF, bit-reversed read at the store): vectors are rows of n words.
-template <uint32_t T>
+template <uint32_t T, uint32_t kGroup>
 __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile, uint32_t* sm,
                                          M32* s_ar) {
     const uint32_t L = u.log_n, n = 1u << L, shift = a.max_log - L;
@@ -153,15 +171,20 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
         flags = inv ? (nega ? BF_POST_PSI : BF_POST_SCALE) : 0u;
     }
     const uint32_t len = 1u << lg, half_len = len >> 1;
-    const uint32_t stride = len >= 32 ? len + 1 : len;
+    // V is a power of two for column tiles (a row tile's V is its row count);
+    // every index split below is a shift or a mask
+    const uint32_t lgV = row ? 0u : 31u - __clz(V);
+    // row stride and in-row padding (one word every 32) keep the register
+    // groups' loads and stores free of bank conflicts
+    const uint32_t stride = len >= 32 ? len + (len >> 5) + 1 : len;
     const uint32_t n_mods = row ? V : 1u;
     uint32_t* t = sm;
     uint32_t* tws = sm + V * stride;  // n_mods x len / 2 root powers
     if (threadIdx.x < n_mods) s_ar[threadIdx.x] = a.mods[u.mod0 + threadIdx.x].ar;
     for (uint32_t i = threadIdx.x; i < n_mods * half_len; i += T) {
-        const uint32_t r = i / half_len, k = i % half_len;
+        const uint32_t r = i >> (lg - 1), k = i & (half_len - 1);
         const BModulus& M = a.mods[u.mod0 + r];
-        tws[i] = __ldg((inv ? M.tw_inv : M.tw) + ((size_t)k << (a.max_log - lg)));
+        tws[i] = pw(M, M.ar, inv ? PW_OMEGA_INV : PW_OMEGA, k << (a.max_log - lg));
     }
     __syncthreads();
     // ---- load ----
@@ -170,13 +193,13 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
         uint32_t v, j, elem;
         size_t pos;
         if (row) {
-            v = idx / len;
-            j = idx % len;
+            v = idx >> lg;
+            j = idx & (len - 1);
             pos = (size_t)v * n + j;
             elem = j;
         } else {
-            v = idx % V;
-            j = idx / V;
+            v = idx & (V - 1);
+            j = idx >> lgV;
             pos = (size_t)j * C + v0 + v;
             elem = (uint32_t)pos;
         }
@@ -187,38 +210,96 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
         }
         if (flags & BF_PRE_PSI) {
             const BModulus& M = a.mods[u.mod0 + (row ? v : 0u)];
-            x = s_ar[row ? v : 0u].mul(x, __ldg(M.psi + ((size_t)elem << shift)));
+            const M32& ar = s_ar[row ? v : 0u];
+            x = ar.mul(x, pw(M, ar, PW_PSI, elem << shift));
         }
-        t[v * stride + (row ? j : bitrev(j, (int)lg))] = x;
+        const uint32_t jj = row ? j : bitrev(j, (int)lg);
+        t[v * stride + jj + (jj >> 5)] = x;
     }
     __syncthreads();
-    // ---- radix-2 stages ----
-    const uint32_t half_total = total >> 1;
+    // ---- radix-2 stages, up to kGroup at a time in registers ----
+    // A group of r stages s0 .. s0+r-1 touches, for each base index with
+    // zero bits [s0, s0 + r), exactly the 2^r elements base + k 2^s0; one
+    // thread loads them, runs the group's butterflies (the same butterflies,
+    // in the same order, as one stage at a time) and stores them back.
+    constexpr uint32_t kG = 1u << kGroup;
     if (!row) {
         const M32 ar = s_ar[0];
-        for (uint32_t s = 0; s < lg; s++) {
-            const uint32_t half = 1u << s;
-            for (uint32_t bf = threadIdx.x; bf < half_total; bf += T) {
-                const uint32_t v = bf / half_len, j = bf % half_len;
-                const uint32_t p = j & (half - 1), i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+        for (uint32_t s0 = 0; s0 < lg; s0 += kGroup) {
+            const uint32_t r = lg - s0 < kGroup ? lg - s0 : kGroup, nk = 1u << r;
+            const uint32_t groups = len >> r, items = V * groups;
+            for (uint32_t it = threadIdx.x; it < items; it += T) {
+                const uint32_t v = it & (V - 1), g = it >> lgV;
+                const uint32_t low = g & ((1u << s0) - 1), base = ((g >> s0) << (s0 + r)) | low;
                 uint32_t* rw = t + v * stride;
-                const uint32_t u0 = rw[i0], y = ar.mul(rw[i1], tws[p << (lg - 1 - s)]);
-                rw[i0] = ar.add(u0, y);
-                rw[i1] = ar.sub(u0, y);
+                uint32_t x[kG];
+#pragma unroll
+                for (uint32_t k = 0; k < kG; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s0);
+                        x[k] = rw[i + (i >> 5)];
+                    }
+#pragma unroll
+                for (uint32_t tt = 0; tt < kGroup; tt++) {
+                    if (tt >= r) break;
+                    const uint32_t s = s0 + tt, half = 1u << tt;
+#pragma unroll
+                    for (uint32_t k = 0; k < kG; k++) {
+                        if ((k & half) || k + half >= nk) continue;
+                        const uint32_t p = low + ((k & (half - 1)) << s0);
+                        const uint32_t y = ar.mul(x[k + half], tws[p << (lg - 1 - s)]);
+                        const uint32_t u0 = x[k];
+                        x[k] = ar.add(u0, y);
+                        x[k + half] = ar.sub(u0, y);
+                    }
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kG; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s0);
+                        rw[i + (i >> 5)] = x[k];
+                    }
             }
             __syncthreads();
         }
     } else {
-        for (int s = (int)lg - 1; s >= 0; s--) {
-            const uint32_t half = 1u << s;
-            for (uint32_t bf = threadIdx.x; bf < half_total; bf += T) {
-                const uint32_t v = bf / half_len, j = bf % half_len;
-                const uint32_t p = j & (half - 1), i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+        // DIF: stages from lg-1 down, groups [s_lo, s_lo + r)
+        for (int s_hi = (int)lg - 1; s_hi >= 0; s_hi -= (int)kGroup) {
+            const uint32_t r = (uint32_t)s_hi + 1 < kGroup ? (uint32_t)s_hi + 1 : kGroup, nk = 1u << r;
+            const uint32_t s_lo = (uint32_t)s_hi + 1 - r;
+            const uint32_t groups = len >> r, items = V * groups;
+            for (uint32_t it = threadIdx.x; it < items; it += T) {
+                const uint32_t v = it >> (lg - r), g = it & (groups - 1);
+                const uint32_t low = g & ((1u << s_lo) - 1), base = ((g >> s_lo) << (s_lo + r)) | low;
                 const M32 ar = s_ar[v];
+                const uint32_t* tw_row = tws + v * half_len;
                 uint32_t* rw = t + v * stride;
-                const uint32_t u0 = rw[i0], y = rw[i1];
-                rw[i0] = ar.add(u0, y);
-                rw[i1] = ar.mul(ar.sub(u0, y), tws[v * half_len + (p << (lg - 1 - s))]);
+                uint32_t x[kG];
+#pragma unroll
+                for (uint32_t k = 0; k < kG; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s_lo);
+                        x[k] = rw[i + (i >> 5)];
+                    }
+#pragma unroll
+                for (int tt = (int)kGroup - 1; tt >= 0; tt--) {
+                    if ((uint32_t)tt >= r) continue;
+                    const uint32_t s = s_lo + (uint32_t)tt, half = 1u << tt;
+#pragma unroll
+                    for (uint32_t k = 0; k < kG; k++) {
+                        if ((k & half) || k + half >= nk) continue;
+                        const uint32_t p = low + ((k & (half - 1)) << s_lo);
+                        const uint32_t u0 = x[k], y = x[k + half];
+                        x[k] = ar.add(u0, y);
+                        x[k + half] = ar.mul(ar.sub(u0, y), tw_row[p << (lg - 1 - s)]);
+                    }
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kG; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s_lo);
+                        rw[i + (i >> 5)] = x[k];
+                    }
             }
             __syncthreads();
         }
@@ -229,36 +310,38 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
         size_t pos;
         uint32_t x;
         if (row) {
-            v = idx / len;
-            k = idx % len;
-            x = t[v * stride + bitrev(k, (int)lg)];
+            v = idx >> lg;
+            k = idx & (len - 1);
+            const uint32_t kk = bitrev(k, (int)lg);
+            x = t[v * stride + kk + (kk >> 5)];
             pos = (size_t)v * n + k;
             elem = k;
         } else {
-            v = idx % V;
-            k = idx / V;
-            x = t[v * stride + k];
+            v = idx & (V - 1);
+            k = idx >> lgV;
+            x = t[v * stride + k + (k >> 5)];
             const uint32_t vec = v0 + v;
             pos = (flags & BF_STORE_T) ? (size_t)vec * len + k : (size_t)k * C + vec;
             elem = (uint32_t)pos;
             if (flags & BF_POST_TW) {
                 const BModulus& M = a.mods[u.mod0];
                 const uint32_t e = (uint32_t)(((uint64_t)k * vec) & (n - 1));
-                x = s_ar[0].mul(x, __ldg((inv ? M.tw_inv : M.tw) + ((size_t)e << shift)));
+                x = s_ar[0].mul(x, pw(M, s_ar[0], inv ? PW_OMEGA_INV : PW_OMEGA, e << shift));
             }
         }
         if (flags & (BF_POST_SCALE | BF_POST_PSI)) {
             const uint32_t r = row ? v : 0u;
             const BModulus& M = a.mods[u.mod0 + r];
             x = s_ar[r].mul(x, M.ninv[L]);
-            if (flags & BF_POST_PSI) x = s_ar[r].mul(x, __ldg(M.psi_inv + ((size_t)elem << shift)));
+            if (flags & BF_POST_PSI) x = s_ar[r].mul(x, pw(M, s_ar[r], PW_PSI_INV, elem << shift));
         }
         dst[pos] = x;
     }
 }
 
-template <uint32_t E, uint32_t T>
-__global__ void __launch_bounds__(T) batch_queue(const __grid_constant__ BArgs a) {
+template <uint32_t E, uint32_t T, uint32_t G>
+// more resident CTAs for the small register groups
+__global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T) batch_queue(const __grid_constant__ BArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_ticket;
     __shared__ M32 s_ar[kMaxRows];
@@ -287,7 +370,7 @@ __global__ void __launch_bounds__(T) batch_queue(const __grid_constant__ BArgs a
             __threadfence();
         }
         __syncthreads();
-        run_tile<T>(a, u, pass, tile, sm, s_ar);
+        run_tile<T, G>(a, u, pass, tile, sm, s_ar);
         __threadfence();
         __syncthreads();
         if (threadIdx.x == 0)
@@ -297,24 +380,27 @@ __global__ void __launch_bounds__(T) batch_queue(const __grid_constant__ BArgs a
 
 // ---- host ------------------------------------------------------------------------
 struct Variant {
-    uint32_t E, T;
+    uint32_t E, T, G;
     void (*fn)(BArgs);
 };
 const Variant kVariants[] = {
-    {4096, 256, batch_queue<4096, 256>},
-    {8192, 256, batch_queue<8192, 256>},
-    {8192, 512, batch_queue<8192, 512>},
-    {16384, 512, batch_queue<16384, 512>},
+    {4096, 256, 1, batch_queue<4096, 256, 1>},    {4096, 256, 3, batch_queue<4096, 256, 3>},
+    {4096, 256, 4, batch_queue<4096, 256, 4>},    {8192, 256, 1, batch_queue<8192, 256, 1>},
+    {8192, 256, 3, batch_queue<8192, 256, 3>},    {8192, 256, 4, batch_queue<8192, 256, 4>},
+    {8192, 512, 1, batch_queue<8192, 512, 1>},    {8192, 512, 3, batch_queue<8192, 512, 3>},
+    {8192, 512, 4, batch_queue<8192, 512, 4>},    {16384, 512, 1, batch_queue<16384, 512, 1>},
+    {16384, 512, 3, batch_queue<16384, 512, 3>},  {16384, 512, 4, batch_queue<16384, 512, 4>},
 };
 
-const Variant* find_variant(uint32_t E, uint32_t T) {
+const Variant* find_variant(uint32_t E, uint32_t T, uint32_t G) {
     for (const Variant& v : kVariants)
-        if (v.E == E && v.T == T) return &v;
+        if (v.E == E && v.T == T && v.G == G) return &v;
     return nullptr;
 }
 
 // tile elements + root powers + padding, in words
-size_t smem_bytes(uint32_t E) { return ((size_t)E + E / 32 + kMaxRows + E / 2) * 4 + 64; }
+// padded tile (E + E/32 + one word per vector) + root powers + slack, in bytes
+size_t smem_bytes(uint32_t E) { return ((size_t)E + E / 16 + kMaxRows + E / 2) * 4 + 64; }
 
 uint32_t ilog2(uint64_t x) {
     uint32_t l = 0;
@@ -353,12 +439,14 @@ nttb_batch_config default_config() {
     c.split = 0;
     c.lag = 2;
     c.ctas_per_sm = 0;
+    c.group = 3;
     return c;
 }
 
 int check_config(const nttb_batch_config& c) {
-    if (!find_variant(c.tile_elems, c.threads))
-        return fail(NTTB_ERR_INVALID_ARG, "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512");
+    if (!find_variant(c.tile_elems, c.threads, c.group))
+        return fail(NTTB_ERR_INVALID_ARG,
+                    "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512, group 1, 3 or 4");
     if (c.split > 1) return fail(NTTB_ERR_INVALID_ARG, "batch config: split must be 0 or 1");
     if (c.lag < 1 || c.lag > 64) return fail(NTTB_ERR_INVALID_ARG, "batch config: lag must be in [1, 64]");
     return 0;
@@ -534,7 +622,7 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
     Batch* b = new Batch();
     b->plan = P;
     b->cfg = cfg;
-    b->var = find_variant(cfg.tile_elems, cfg.threads);
+    b->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group);
     b->n_units = (uint32_t)units.size();
     b->n_tiles = (uint32_t)tiles.size();
     b->ws_bytes = (size_t)ws_words * slots * 4;
@@ -646,7 +734,7 @@ int runner_create(BatchPlan* P, const nttb_batch_config& cfg, BatchRunner** out)
     auto* r = new BatchRunner();
     r->plan = P;
     r->cfg = cfg;
-    r->var = find_variant(cfg.tile_elems, cfg.threads);
+    r->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group);
     const size_t slots = std::max<size_t>(16, cfg.lag + 2);
     r->ws_bytes = slots * ((size_t)4 << P->max_log);
     if (cudaMalloc(&r->d_ws, r->ws_bytes) != cudaSuccess || runner_reserve(r, 256, 4096)) {
@@ -714,7 +802,9 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
 }
 
 size_t batch_plan_device_bytes(const BatchPlan* P) {
-    return (size_t)P->limbs.size() * (P->negacyclic ? 4 : 2) * ((size_t)4 << P->max_log);
+    const uint32_t lo = std::min<uint32_t>(kLoBits, P->max_log);
+    return (size_t)P->limbs.size() * 4 * 4 * (((size_t)1 << (P->max_log - lo)) + ((size_t)1 << lo)) +
+           P->limbs.size() * sizeof(BModulus);
 }
 
 uint32_t batch_device_errors(bool clear) {
@@ -764,24 +854,33 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
             return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_plan_create: %s", why.c_str());
         }
     }
-    const size_t tables = nega ? 4 : 2;
-    std::vector<uint32_t> host(tables * N);
+    const uint32_t lo_bits = std::min<uint32_t>(nttb::kLoBits, max_log_n);
+    const uint32_t hi_len = 1u << (max_log_n - lo_bits), lo_len = 1u << lo_bits;
+    const size_t per_base = (size_t)hi_len + lo_len;
+    std::vector<uint32_t> host(4 * per_base);
     std::vector<nttb::BModulus> mods(n_moduli);
     for (uint32_t l = 0; l < n_moduli; l++) {
         const nttb::LimbHost& H = P.limbs[l];
         const uint64_t q = H.q;
+        // base^e R for e = i 2^lo_bits (hi part) and e = i (lo part)
         auto powers = [&](uint32_t* dst, uint64_t base) {
             uint64_t x = 1;
-            for (uint64_t e = 0; e < N; e++) {
-                dst[e] = nttb::h_to_mont32(x, q);
+            for (uint32_t i = 0; i < lo_len; i++) {
+                dst[hi_len + i] = nttb::h_to_mont32(x, q);
                 x = nttb::h_mulmod(x, base, q);
+            }
+            const uint64_t step = x;  // base^(2^lo_bits)
+            x = 1;
+            for (uint32_t i = 0; i < hi_len; i++) {
+                dst[i] = nttb::h_to_mont32(x, q);
+                x = nttb::h_mulmod(x, step, q);
             }
         };
         powers(host.data(), H.omega);
-        powers(host.data() + N, H.omega_inv);
+        powers(host.data() + per_base, H.omega_inv);
         if (nega) {
-            powers(host.data() + 2 * N, H.psi);
-            powers(host.data() + 3 * N, H.psi_inv);
+            powers(host.data() + 2 * per_base, H.psi);
+            powers(host.data() + 3 * per_base, H.psi_inv);
         }
         uint32_t* d = nullptr;
         if (cudaMalloc(&d, host.size() * 4) != cudaSuccess ||
@@ -796,10 +895,9 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
         nttb::BModulus& M = mods[l];
         M.ar.q = (uint32_t)q;
         M.ar.qinv = nttb::h_neg_inv32((uint32_t)q);
-        M.tw = d;
-        M.tw_inv = d + N;
-        M.psi = nega ? d + 2 * N : nullptr;
-        M.psi_inv = nega ? d + 3 * N : nullptr;
+        M.pw = d;
+        M.lo_bits = lo_bits;
+        M.hi_len = hi_len;
         for (uint32_t L = 0; L < 25; L++) M.ninv[L] = nttb::h_to_mont32(nttb::h_invmod((1ull << L) % q, q), q);
         M.r2 = nttb::h_to_mont32(nttb::h_to_mont32(1, q), q);
     }
@@ -893,11 +991,21 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
                                  nttb_batch_config* out) {
     if (!plan || !jobs || n_jobs == 0) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: no jobs");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // Sample of the mix: up to two jobs per (log_n, direction, twist), at
-    // most 4 limbs each, on scratch buffers (the caller's data is untouched).
+    // Sample of the mix on scratch buffers (the caller's data is untouched):
+    // up to two jobs per (log_n, direction, twist, product) with at most 8
+    // limbs each, then further jobs until the sample holds 32 M residues, so
+    // that every candidate is timed on enough work to fill the GPU.
     std::vector<nttb_batch_job> sample;
     std::vector<uint32_t> seen(64 * 8, 0);
+    std::vector<char> taken(n_jobs, 0);
     size_t words = 0;
+    auto take = [&](uint32_t j) {
+        nttb_batch_job c = jobs[j];
+        c.n_limbs = std::min<uint32_t>(c.n_limbs, 8);
+        sample.push_back(c);
+        words += ((size_t)c.n_limbs << c.log_n) * ((c.flags & NTTB_BATCH_POLYMUL) ? 2 : 1);
+        taken[j] = 1;
+    };
     for (uint32_t j = 0; j < n_jobs; j++) {
         const nttb_batch_job& J = jobs[j];
         if (J.log_n < 1 || J.log_n > plan->p.max_log) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: job %u log_n", j);
@@ -905,11 +1013,10 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
                              ((J.flags & NTTB_BATCH_POLYMUL) ? 4 : 0);
         if (seen[key] >= 2) continue;
         seen[key]++;
-        nttb_batch_job c = J;
-        c.n_limbs = std::min<uint32_t>(J.n_limbs, 4);
-        sample.push_back(c);
-        words += ((size_t)c.n_limbs << c.log_n) * ((c.flags & NTTB_BATCH_POLYMUL) ? 2 : 1);
+        take(j);
     }
+    for (uint32_t j = 0; j < n_jobs && words < (32u << 20); j++)
+        if (!taken[j]) take(j);
     uint32_t* scratch = nullptr;
     if (cudaMalloc(&scratch, words * 4) != cudaSuccess) return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_autotune: scratch");
     cudaMemsetAsync(scratch, 0, words * 4, s);
@@ -923,7 +1030,7 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
         }
     }
     const uint32_t shapes[4][2] = {{4096, 256}, {8192, 256}, {8192, 512}, {16384, 512}};
-    const uint32_t lags[2] = {1, 4};
+    const uint32_t lags[2] = {1, 4}, groups[3] = {1, 3, 4};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -932,12 +1039,14 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
     int rc = 0;
     for (const auto& sh : shapes)
         for (uint32_t split = 0; split < 2; split++)
-            for (uint32_t lag : lags) {
+            for (uint32_t lag : lags)
+                for (uint32_t grp : groups) {
                 nttb_batch_config c = nttb::default_config();
                 c.tile_elems = sh[0];
                 c.threads = sh[1];
                 c.split = split;
                 c.lag = lag;
+                c.group = grp;
                 Batch* b = nullptr;
                 if (nttb::create_batch(&plan->p, sample.data(), (uint32_t)sample.size(), c, &b)) continue;
                 float t_min = 1e30f;
@@ -956,7 +1065,7 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
                     best = t_min;
                     best_cfg = c;
                 }
-            }
+                }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(scratch);

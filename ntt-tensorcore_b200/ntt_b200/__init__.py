@@ -49,8 +49,9 @@ class BatchJob(ctypes.Structure):
 
 
 class BatchConfig(ctypes.Structure):
-    """nttb_batch_config: tile_elems, threads, split, lag, ctas_per_sm."""
-    _fields_ = [("tile_elems", _u32), ("threads", _u32), ("split", _u32), ("lag", _u32), ("ctas_per_sm", _u32)]
+    """nttb_batch_config: tile_elems, threads, split, lag, ctas_per_sm, group."""
+    _fields_ = [("tile_elems", _u32), ("threads", _u32), ("split", _u32), ("lag", _u32), ("ctas_per_sm", _u32),
+                ("group", _u32)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

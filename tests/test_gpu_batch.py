@@ -15,9 +15,10 @@ PRIMES = nb.generate_primes(31, 21, 12)  # q == 1 mod 2^21: negacyclic up to 2^2
 
 CONFIGS = [
     None,  # the default
-    {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 1},
-    {"tile_elems": 8192, "threads": 512, "split": 0, "lag": 3},
-    {"tile_elems": 16384, "threads": 512, "split": 1, "lag": 4, "ctas_per_sm": 1},
+    {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 1, "group": 4},
+    {"tile_elems": 8192, "threads": 512, "split": 0, "lag": 3, "group": 3},
+    {"tile_elems": 8192, "threads": 256, "split": 1, "lag": 2, "group": 4},
+    {"tile_elems": 16384, "threads": 512, "split": 1, "lag": 4, "ctas_per_sm": 1, "group": 4},
 ]
 
 
@@ -123,6 +124,7 @@ def test_batch_autotune(torch_cuda):
     before = [to_host(j[1], np.uint32).copy() for j in jobs]
     cfg = plan.autotune(spec(jobs))
     assert cfg["tile_elems"] in (4096, 8192, 16384) and cfg["split"] in (0, 1) and cfg["lag"] >= 1
+    assert cfg["group"] in (3, 4)
     for j, b0 in zip(jobs, before):  # autotuning leaves the jobs' data alone
         assert (to_host(j[1], np.uint32) == b0).all()
     b = plan.batch(spec(jobs))
