@@ -45,10 +45,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "int8", "dmma", "scalar"])
-    ap.add_argument("--workload", default="rns", choices=["rns", "uneven", "serve"],
+    ap.add_argument("--workload", default="rns", choices=["rns", "uneven", "serve", "q60"],
                     help="rns: the 24-limb 2^16 negacyclic batch (headline); uneven: 512 polynomials of "
                          "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch; "
-                         "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99")
+                         "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
+                         "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
     ap.add_argument("--profile-case", choices=["int8", "dmma", "batch"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
@@ -596,6 +597,95 @@ def run_serve(args, world, rank, local):
     }
 
 
+# ------------------------------------------------------------ 60-bit prime
+Q60 = 1152921504577486849  # largest 60-bit prime == 1 mod 2^21
+Q60_WORKLOAD = "q60_2^20_cyclic_fwd+inv"
+
+
+def run_q60(args, world, rank, local):
+    """One 2^20 polynomial mod the 60-bit prime per step (forward + inverse),
+    residues as uint64; also a batch of 16 polynomials per launch."""
+    import torch
+    import ntt_b200 as nb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    lg = 20
+    plan = nb.WidePlan(lg, [Q60])
+    rng = np.random.default_rng(60)
+    host = rng.integers(0, Q60, 1 << lg, dtype=np.uint64)
+    pool_n = 40  # 40 x 8 MB > 2x L2
+    pool = torch.from_numpy(host.view(np.int64)).to(dev).repeat(pool_n, 1)
+
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = nb.launch_count()
+        e0.record(stream)
+        for i in range(steps):
+            fn(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), nb.launch_count() - c0
+
+    def one(i):
+        buf = pool[i % pool_n]
+        plan.transform(buf, buf, 1, stream=stream)
+        plan.transform(buf, buf, 1, inverse=True, stream=stream)
+
+    def sixteen(i):
+        b = pool[(16 * i) % 32:(16 * i) % 32 + 16]
+        plan.transform(b, b, 16, stream=stream)
+        plan.transform(b, b, 16, inverse=True, stream=stream)
+
+    for i in range(max(3, args.warmup)):
+        one(i)
+        sixteen(i)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    ms, launches = timed(one, args.steps)
+    ms16, _ = timed(sixteen, max(3, args.steps // 8))
+    clk = clocks.stop()
+    got = pool[0].cpu().numpy().view(np.uint64)
+    assert (got == host).all(), "q60 round trip failed"
+    coeffs = 2 << lg
+    value = world * coeffs * args.steps / (ms / 1e3)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = 16 * coeffs / (ms / args.steps / 1e3) / 1e9  # 8 B read + 8 B write per residue per transform
+    cpu = None
+    try:
+        from oracle import oracle as O
+        if O.ref() is not None:
+            x = host.copy()
+            t0 = time.perf_counter()
+            y = O.ref_ntt_host(x, Q60)
+            O.ref_ntt_host(y, Q60, inverse=True)
+            dt = time.perf_counter() - t0
+            cpu = {"value": coeffs / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "1 x 2^20 forward + inverse (ntt_host, __int128)"}
+    except Exception as e:  # reference library missing on this host
+        cpu = {"unavailable": str(e)[:200]}
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic: seeded uniform residues",
+        "config": {"workload": Q60_WORKLOAD, "n": 1 << lg, "q": Q60, "l2": "rotating 40 x 8 MB", "parallelism": "replicas x%d" % world},
+        "batch16": {"value": world * 16 * coeffs * max(3, args.steps // 8) / (ms16 / 1e3),
+                    "ms_per_step": ms16 / max(3, args.steps // 8)},
+        "roofline": {"bound": "hbm", "kernel": "scalar_pass (M64)", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "note": "one polynomial per step: launch-latency bound"},
+        "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk, "e2e": None,
+    }
+
+
 # ----------------------------------------------------- small profiling cases
 def profile_case(name):
     """Small, self-checking cases for ncu captures (a few launches, < 1 GB):
@@ -638,8 +728,9 @@ def main():
         profile_case(args.profile_case)
         return
     world, rank, local = dist_setup(args)
-    if args.workload in ("uneven", "serve") and args.impl == "ours":
-        r = run_uneven(args, world, rank, local) if args.workload == "uneven" else run_serve(args, world, rank, local)
+    if args.workload in ("uneven", "serve", "q60") and args.impl == "ours":
+        fn = {"uneven": run_uneven, "serve": run_serve, "q60": run_q60}[args.workload]
+        r = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(r))
         if world > 1:
