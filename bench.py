@@ -375,6 +375,39 @@ def run_ours(args, world, rank, local):
     return result, qs
 
 
+# --------------------------------------------- reference CPU path beside
+def cpu_sample(jobs, moduli, budget_s=10.0):
+    """The reference's ntt_host (oracle/_ref) on all host threads over a
+    bounded sample of a job mix: jobs = (log_n, limbs, inverse, negacyclic,
+    product) tuples taken in order until ~budget_s of work.  Products are
+    forward a, forward b, pointwise, inverse (3 transforms per residue)."""
+    from oracle import oracle as O
+    if O.ref() is None:
+        return {"unavailable": "reference library oracle/_ref not built"}
+    rng = np.random.default_rng(11)
+    done, coeffs, used, t0 = 0, 0, 1, time.perf_counter()
+    for lg, limbs, inv, nega, prod in jobs:
+        qs = moduli[:limbs]
+        q = np.array(qs, dtype=np.uint64)[:, None]
+        x = (rng.integers(0, 1 << 62, (1, limbs, 1 << lg), dtype=np.uint64) % q).copy()
+        if prod:
+            y = (rng.integers(0, 1 << 62, (1, limbs, 1 << lg), dtype=np.uint64) % q).copy()
+            used = O.ref_host_batch(x, qs, negacyclic=nega)
+            O.ref_host_batch(y, qs, negacyclic=nega)
+            x = np.ascontiguousarray((x * y) % q[None])  # residues < 2^31: the product fits
+            O.ref_host_batch(x, qs, inverse=True, negacyclic=nega)
+            coeffs += 3 * limbs << lg
+        else:
+            used = O.ref_host_batch(x, qs, inverse=inv, negacyclic=nega)
+            coeffs += limbs << lg
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": coeffs / dt, "unit": UNIT, "cores": used, "kind": "reference",
+            "sample": "%d jobs of the mix (ntt_host per (poly, limb), all host threads)" % done}
+
+
 # ------------------------------------------------------- uneven workload
 UNEVEN_JOBS = 512
 UNEVEN_WORKLOAD = "uneven_512polys_logN12-20_limbs1-32_mixed_dir"
@@ -475,6 +508,8 @@ def run_uneven(args, world, rank, local):
     }
     batch.close()
     plan.close()
+    if rank == 0 and world == 1:
+        result["cpu_baseline"] = cpu_sample([(a, min(b, 8), c, False, False) for a, b, c in shapes], qs)
     return result
 
 
@@ -583,6 +618,7 @@ def run_serve(args, world, rank, local):
         levels["%d%%" % int(frac * 100)] = phase(frac * peak, args.serve_seconds)
     st = srv.stats()
     srv.close()
+    cpu = cpu_sample([(lg, limbs, False, True, True) for _, _, lg, limbs, _ in pool], qs) if rank == 0 else None
     return {
         "metric": METRIC, "value": sat["coeffs_per_s"], "unit": UNIT, "n_gpus": world, "steps": sat["requests"],
         "warmup": 1, "ms_per_step": 1e3 / sat["achieved_rps"], "higher_is_better": True, "scaling": "weak",
@@ -594,6 +630,7 @@ def run_serve(args, world, rank, local):
                   "mean_batch_requests": st["batched_requests"] / max(1, st["batches"]),
                   "peak_region_bytes_in_use": st["peak_bytes_in_use"], "resident_bytes": st["resident_bytes"]},
         "e2e": {"value": sat["coeffs_per_s"], "unit": UNIT, "note": "host buffers in, host buffers out"},
+        "cpu_baseline": cpu,
     }
 
 

@@ -126,20 +126,26 @@ struct ClArgs {
 };
 
 // ---- device arithmetic ------------------------------------------------------------
+// 32 x 32 + 64 -> 64 multiply-add (one mad.wide.u32).
+__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
+    uint64_t r;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(a), "r"(b), "l"(c));
+    return r;
+}
 __device__ __forceinline__ uint32_t redc64(uint64_t v, uint32_t q, uint32_t qinv) {
     const uint32_t m = (uint32_t)v * qinv;
-    return (uint32_t)((v + (uint64_t)m * q) >> 32);  // [0, 2q) for v < q * 2^32
+    return (uint32_t)(mad_wide(m, q, v) >> 32);  // [0, 2q) for v < q * 2^32
 }
 // Planes c_a <= 256 * 255^2 (K = 256 byte products), so c0 + 256 c1 and
 // c2 + 256 c3 fit in 32 bits; v = sum_a 256^a c_a < 2^49.
 __device__ __forceinline__ uint32_t combine_redc(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t q,
                                                  uint32_t qinv) {
     const uint32_t lo = c0 + (c1 << 8), hi = c2 + (c3 << 8);
-    return redc64((uint64_t)lo + ((uint64_t)hi << 16), q, qinv);
+    return redc64(mad_wide(hi, 65536u, (uint64_t)lo), q, qinv);
 }
 // a < 2q, b < q -> a*b*2^-32 mod q in [0, 2q)
 __device__ __forceinline__ uint32_t mont_lazy(uint32_t a, uint32_t b, uint32_t q, uint32_t qinv) {
-    return redc64((uint64_t)a * b, q, qinv);
+    return redc64(mad_wide(a, b, 0ull), q, qinv);
 }
 __device__ __forceinline__ uint32_t canon(uint32_t x, uint32_t q) { return x >= q ? x - q : x; }
 
