@@ -124,7 +124,7 @@ def test_batch_autotune(torch_cuda):
     before = [to_host(j[1], np.uint32).copy() for j in jobs]
     cfg = plan.autotune(spec(jobs))
     assert cfg["tile_elems"] in (4096, 8192, 16384) and cfg["split"] in (0, 1) and cfg["lag"] >= 1
-    assert cfg["group"] in (3, 4)
+    assert cfg["group"] in (1, 3, 4)
     for j, b0 in zip(jobs, before):  # autotuning leaves the jobs' data alone
         assert (to_host(j[1], np.uint32) == b0).all()
     b = plan.batch(spec(jobs))
