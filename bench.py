@@ -51,7 +51,7 @@ def parse():
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
                          "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
-    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch"], default=None,
+    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
@@ -728,7 +728,8 @@ def profile_case(name):
     """Small, self-checking cases for ncu captures (a few launches, < 1 GB):
     int8 / dmma: forward+inverse of the 24-limb 2^16 negacyclic batch, four
     launches; batch: a ~600 MB uneven batch (log2 N 12..20, 1..8 limbs, mixed
-    directions) launched twice."""
+    directions) launched twice; batch_tc: the same with log2 N 17..20 on
+    tensor-core tiles."""
     import torch
     import ntt_b200 as nb
     if name in ("int8", "dmma"):
@@ -744,14 +745,18 @@ def profile_case(name):
         qs = nb.generate_primes(31, 21, 8)
         rng = np.random.default_rng(1)
         jobs, bufs, words = [], [], 0
+        lo = 17 if name == "batch_tc" else 12
         while words < 150_000_000:
-            lg, limbs = int(rng.integers(12, 21)), int(rng.integers(1, 9))
+            lg, limbs = int(rng.integers(lo, 21)), int(rng.integers(1, 9))
             t = torch.randint(0, 1 << 30, (limbs << lg,), dtype=torch.int32, device="cuda") % int(min(qs))
             bufs.append(t)
             words += limbs << lg
             jobs.append((t, lg, limbs, 0, bool(rng.integers(0, 2)), False))
         plan = nb.BatchPlan(qs, 20)
-        b = plan.batch(jobs, {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 4})
+        cfg = {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 4, "group": 3}
+        if name == "batch_tc":
+            cfg.update(split=0, tensor=1)
+        b = plan.batch(jobs, cfg)
         b.launch()
         b.launch()
         torch.cuda.synchronize()

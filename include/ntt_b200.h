@@ -201,6 +201,9 @@ typedef struct {
     uint32_t lag;         /* two-pass units between a unit's first and second pass in the queue (1..64) */
     uint32_t ctas_per_sm; /* 0: as many as fit */
     uint32_t group;       /* radix-2 stages per register group inside a tile: 1, 3 or 4 */
+    uint32_t tensor;      /* 1: two-pass units of 2^13 .. 2^20 residues run tensor-core tiles (INT8
+                             DFT-64 + radix-2 DFT of up to 16 points); needs threads 256, tile_elems
+                             4096 or 8192 (units above the tile size take them) */
 } nttb_batch_config;
 
 /* flags: NTTB_NEGACYCLIC to allow negacyclic jobs (moduli then need 2^(max_log_n+1) | q-1). */
@@ -226,6 +229,8 @@ NTTB_API int nttb_batch_launch(nttb_batch* batch, void* stream);
 NTTB_API int nttb_batch_graph_launch(nttb_batch* batch, void* stream);
 NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t* tiles, uint64_t* ws_bytes,
                              nttb_batch_config* config);
+/* CTAs of the persistent launch (SMs x resident CTAs per SM, at most the tile count). */
+NTTB_API int nttb_batch_ctas(const nttb_batch* batch, uint32_t* ctas);
 
 /* ------------------------------------------------------------- serving
  * No reference counterpart (the reference has no request loop).  A server

@@ -28,8 +28,9 @@
 // until every pass A tile of its unit has signalled; a pass A tile first waits
 // until the previous user of its workspace slot has finished pass B.  Every
 // awaited tile has a smaller ticket, so it belongs to a CTA that is already
-// running: no deadlock.  Workspace slots form a ring of S > lag slots, so the
-// workspace is S x (largest unit), not the size of the batch.
+// running: no deadlock.  Workspace slots form one ring per size class 2^L of
+// S_L > lag slots (enough for ~1024 pass A tiles in flight), so the workspace
+// is bounded by the rings, not by the size of the batch.
 //
 // Inside a tile, radix-2 stages run in register groups of 1, 3 or 4: one
 // thread loads the 2, 8 or 16 elements that a group's stages combine,
@@ -56,17 +57,20 @@
 #include "engines.hpp"
 #include "plan.hpp"
 #include "profiler.hpp"
+#include "tc_arith.cuh"
+#include "tcgen05.cuh"
 
 namespace nttb {
 
-// bit 0: a queue dependency wait ran out of budget
+// bit 0: a queue dependency wait ran out of budget; bit 1: a tensor-core
+// tile's wait on its MMA or image copy did
 __device__ uint32_t g_batch_error;
 
 namespace {
 
 constexpr uint32_t BF_INV = 1, BF_PRE_PSI = 2, BF_POST_TW = 4, BF_STORE_T = 8, BF_POST_SCALE = 16, BF_POST_PSI = 32,
                    BF_PRE_MUL = 64;
-constexpr uint32_t UF_INV = 1, UF_NEGA = 2;
+constexpr uint32_t UF_INV = 1, UF_NEGA = 2, UF_TC = 4;  // UF_TC: tensor-core tiles
 constexpr uint32_t kMaxRows = 32;
 
 // Power tables: x^e R for e < 2^max_log as hi[e >> kLoBits] * lo[e & lo_mask]
@@ -116,6 +120,7 @@ struct BArgs {
     const BUnit* units;
     const BTile* tiles;
     uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u
+    const uint8_t* images;  // per modulus: DFT-64 byte-plane images (forward, inverse, negacyclic forward)
     uint32_t n_tiles, max_log;
 };
 
@@ -339,6 +344,306 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
     }
 }
 
+// Thread 0 of a tile: waits until the tile's inputs are complete (pass B:
+// every pass A tile of its unit; pass A: the previous owner of its workspace
+// slot and the units it depends on).  False if a wait ran out of budget.
+__device__ __forceinline__ bool wait_deps(const BArgs& a, const BUnit& u, uint32_t ui, uint32_t pass) {
+    bool ok = true;
+    if (pass == 1) {
+        ok = wait_ge(a.ctr + 1 + 2 * ui, u.tiles_a);
+    } else {
+        if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, a.units[u.prev].tiles_b);
+        for (int d = 0; d < 2; d++) {
+            const int32_t w = u.after[d];
+            if (w < 0) continue;
+            const BUnit& W = a.units[w];  // complete = its last pass has signalled every tile
+            ok = wait_ge(a.ctr + (W.lg1 ? 2u : 1u) + 2 * (uint32_t)w, W.lg1 ? W.tiles_b : W.tiles_a) && ok;
+        }
+    }
+    return ok;
+}
+
+// ---- tensor-core tiles ----------------------------------------------------------------
+// A two-pass unit of 2^13 .. 2^20 residues whose pass lengths are len = 64 r'
+// (r' = 1, 2, 4, 8, 16) runs its tiles on the tensor cores.  A tile is the
+// pass's DFT of length len over V = 128 / r' consecutive columns (8192
+// residues), with j = r' a2 + b2 and output d = k1 + 64 k2:
+//   level 1: for each of the 128 vectors (column v, b2), a DFT-64 over a2 --
+//            the INT8 byte-plane contraction (M = 128, N = 256, K = 256 bytes)
+//            against the modulus's DFT-64 image -- times every factor that is
+//            geometric in k1: the inner twiddle omega_len^(b2 k1), pass A's
+//            omega_n^(col k1), the inverse's psi^-(N1 k1) and n^-1, the
+//            negacyclic input twist psi^(b2 N2 + col) (its psi^(a2 n / 64)
+//            part is folded into the forward image), generated as two
+//            interleaved chains in the epilogue;
+//   level 2: for each (column, k1), a DFT-r' over b2 on the CUDA cores
+//            (radix 2 in registers) times the factors that depend on k2
+//            (pass A: omega_n^(64 col k2); negacyclic inverse: psi^-(64 N1 k2)).
+// Pass A stores transposed (ws[col N1 + d]) and pass B in natural order
+// (x[col + N1 d]): the CUDA-core tiles' layouts, so results are identical.
+// The data of a tile crosses shared memory twice (operand A, then the level-1
+// outputs W over it); the 64 KB image stays resident while consecutive tiles
+// use the same modulus and direction.
+constexpr uint32_t kTcA = 0;              // operand A: 128 rows x 256 B, SW128 (two K blocks), then W
+constexpr uint32_t kTcImg = 32768;        // DFT-64 image (64 KB)
+constexpr uint32_t kTcFac = 98304;        // level-2 factors [128] and butterfly twiddles [8]
+constexpr uint32_t kTcBar = kTcFac + 1024;  // mbarriers: [0] MMA commit, [1] image copy
+constexpr size_t kTcSmem = kTcBar + 64 + 1024;  // + alignment slack
+constexpr uint32_t kImgBytes = 65536;
+
+struct TcState {
+    uint8_t* base;     // 1024-aligned dynamic shared memory
+    uint32_t taddr;    // 256 TMEM columns
+    uint32_t ph_mma, ph_img;
+    uint32_t img_key;  // image in shared memory: (modulus << 2 | variant) + 1, 0 none
+};
+
+__host__ __device__ constexpr uint32_t bitrev_c(uint32_t x, uint32_t bits) {
+    uint32_t r = 0;
+    for (uint32_t i = 0; i < bits; i++) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+}
+
+__device__ __forceinline__ void tc_wait(uint64_t* bar, uint32_t ph) {
+    if (!tc::mbar_wait_bounded(bar, ph)) atomicOr(&g_batch_error, 2u);
+}
+
+// Level 2 of a tile: DFT-2^RL over b2 for each (column v, k1), canonical out.
+// Pass A threads walk k1 fastest (ws rows are contiguous in d); pass B threads
+// walk v fastest (x rows are contiguous in the column), with k1 spread so that
+// the W reads of a warp hit 32 distinct banks.
+template <uint32_t RL>
+__device__ __forceinline__ void tc_level2(const BUnit& u, uint32_t pass, uint32_t v0, uint32_t N1, const M32& ar,
+                                          const uint32_t* W, const uint32_t* fac, bool use_fac) {
+    constexpr uint32_t R = 1u << RL, lgV = 7 - RL, V = 1u << lgV, kPairs = 64u * V;
+    constexpr uint32_t sh = lgV >= 5 ? 0u : 5u - lgV;
+    uint32_t tw2[R > 1 ? R / 2 : 1];
+#pragma unroll
+    for (uint32_t j = 0; j < R / 2; j++) tw2[j] = fac[128 + j];
+#pragma unroll 1
+    for (uint32_t p = threadIdx.x; p < kPairs; p += 256) {
+        uint32_t v, k1;
+        if (pass == 0) {
+            k1 = p & 63u;
+            v = p >> 6;
+        } else {
+            v = p & (V - 1u);
+            const uint32_t qq = p >> lgV;
+            k1 = (qq & 32u) | ((qq & 31u) >> sh) | ((qq & ((1u << sh) - 1u)) << (5u - sh));
+        }
+        uint32_t x[R];
+#pragma unroll
+        for (uint32_t i = 0; i < R; i++) {
+            const uint32_t m = bitrev_c(i, RL) * V + v;
+            x[i] = tca::canon(W[m * 64u + (k1 & 32u) + ((k1 ^ m) & 31u)], ar.q);
+        }
+#pragma unroll
+        for (uint32_t s = 0; s < RL; s++) {
+            const uint32_t half = 1u << s;
+#pragma unroll
+            for (uint32_t k = 0; k < R; k++) {
+                if (k & half) continue;
+                const uint32_t j = k & (half - 1u);
+                const uint32_t y = j == 0 ? x[k + half] : ar.mul(x[k + half], tw2[j << (RL - 1 - s)]);
+                const uint32_t u0 = x[k];
+                x[k] = ar.add(u0, y);
+                x[k + half] = ar.sub(u0, y);
+            }
+        }
+        if (pass == 0) {
+            uint32_t* o = u.ws + (size_t)(v0 + v) * N1 + k1;
+#pragma unroll
+            for (uint32_t k2 = 0; k2 < R; k2++) o[64u * k2] = use_fac ? ar.mul(x[k2], fac[v * R + k2]) : x[k2];
+        } else {
+            uint32_t* o = u.data + (size_t)k1 * N1 + v0 + v;
+#pragma unroll
+            for (uint32_t k2 = 0; k2 < R; k2++) o[(size_t)64u * k2 * N1] = use_fac ? ar.mul(x[k2], fac[k2]) : x[k2];
+        }
+    }
+}
+
+__device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile, TcState& st) {
+    const uint32_t tid = threadIdx.x;
+    const uint32_t L = u.log_n, n = 1u << L, shift = a.max_log - L;
+    const bool inv = u.flags & UF_INV, nega = u.flags & UF_NEGA;
+    const uint32_t N1 = 1u << u.lg1;
+    const uint32_t lg = pass == 0 ? u.lg1 : L - u.lg1;  // pass length 64 r'
+    const uint32_t rl = lg - 6, rp = 1u << rl;
+    const uint32_t lgV = 7 - rl, V = 1u << lgV;
+    const uint32_t C = pass == 0 ? n >> u.lg1 : N1;     // columns of the pass's matrix
+    const uint32_t v0 = tile << lgV;
+    const uint32_t* src = pass == 0 ? u.data : u.ws;
+    const bool pre = pass == 0 && u.pre_mul;
+    const BModulus& M = a.mods[u.mod0];
+    const M32 ar = M.ar;
+    const uint32_t q = ar.q, qinv = ar.qinv;
+    const uint32_t wb = inv ? PW_OMEGA_INV : PW_OMEGA;
+    const uint32_t variant = inv ? 1u : (pass == 0 && nega ? 2u : 0u);
+    const uint32_t key = ((u.mod0 << 2) | variant) + 1u;
+    const bool new_img = key != st.img_key;
+    uint8_t* base = st.base;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base + kTcBar);
+    if (new_img && tid == 0) {
+        const uint8_t* img = a.images + ((size_t)u.mod0 * 3 + variant) * kImgBytes;
+        tc::mbar_expect_tx(bar + 1, kImgBytes);
+#pragma unroll
+        for (uint32_t k = 0; k < 4; k++) tc::bulk_g2s(base + kTcImg + k * 16384u, img + k * 16384u, 16384u, bar + 1);
+    }
+    // level-2 constants: factors, then the DFT-r' butterfly twiddles omega_r'^j
+    uint32_t* fac = reinterpret_cast<uint32_t*>(base + kTcFac);
+    const bool use_fac = rp > 1 && (pass == 0 || (inv && nega));
+    if (use_fac) {
+        if (pass == 0) {
+            if (tid < 128) {
+                const uint32_t fv = tid >> rl, k2 = tid & (rp - 1u);
+                fac[tid] = pw(M, ar, wb, ((64u * (v0 + fv) * k2) & (n - 1u)) << shift);
+            }
+        } else if (tid < rp) {
+            fac[tid] = pw(M, ar, PW_PSI_INV, (64u * N1 * tid) << shift);
+        }
+    }
+    if (tid >= 128 && tid < 128 + rp / 2) fac[tid] = pw(M, ar, wb, (((n >> rl) * (tid - 128)) & (n - 1u)) << shift);
+    // operand A: row m = (b2, v) = b2 V + v holds column v0 + v's elements
+    // j = r' a2 + b2 in K order a2; thread (m, hh) loads 16-byte chunks hh, hh + 2, ..
+    {
+        const uint32_t mm = tid & 127u, hh = tid >> 7;
+        const size_t off0 = (size_t)(mm >> lgV) * C + v0 + (mm & (V - 1u));
+        const size_t step = (size_t)rp * C;  // between consecutive a2
+        uint32_t xs[32];
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++)
+#pragma unroll
+            for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcg(src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
+        if (pre) {
+#pragma unroll
+            for (uint32_t j = 0; j < 8; j++)
+#pragma unroll
+                for (uint32_t t = 0; t < 4; t++)
+                    xs[4 * j + t] = ar.mul(xs[4 * j + t], __ldcg(u.pre_mul + off0 + (size_t)(8u * j + 4u * hh + t) * step));
+        }
+        uint8_t* A = base + kTcA;
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++)
+            *reinterpret_cast<uint4*>(A + tc::sw128_offset(mm, 16u * (2u * j + hh), 128)) =
+                make_uint4(xs[4 * j], xs[4 * j + 1], xs[4 * j + 2], xs[4 * j + 3]);
+    }
+    tc::fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+        if (new_img) tc_wait(bar + 1, st.ph_img);
+        tc::fence_after_sync();
+        tca::issue_k256(st.taddr, tc::smem_u32(base + kTcA), 128, tc::smem_u32(base + kTcImg), 256, 256);
+        tc::commit(bar);
+    }
+    if (new_img) {
+        st.ph_img ^= 1u;
+        st.img_key = key;
+    }
+    // level-1 twiddles of this thread's vector: base * ratio^k1 for k1 = 32 h ..
+    const uint32_t wq = tid >> 5, quarter = wq & 3u, h = wq >> 2, lane = tid & 31u;
+    const uint32_t m = quarter * 32u + lane, b2 = m >> lgV, col = v0 + (m & (V - 1u));
+    const uint32_t er = (n >> lg) * b2 + (pass == 0 ? col : 0u);  // < n
+    uint32_t ratio = pw(M, ar, wb, er << shift);
+    uint32_t start = pw(M, ar, wb, ((er * 32u * h) & (n - 1u)) << shift);
+    if (pass == 0 && !inv && nega) start = ar.mul(start, pw(M, ar, PW_PSI, (b2 * C + col) << shift));
+    if (pass == 1 && inv) {
+        start = ar.mul(start, M.ninv[L]);
+        if (nega) {
+            ratio = ar.mul(ratio, pw(M, ar, PW_PSI_INV, N1 << shift));
+            start = ar.mul(start, pw(M, ar, PW_PSI_INV, (col + 32u * h * N1) << shift));
+        }
+    }
+    if (pre) start = ar.mul(start, M.r2);  // the product's Montgomery factor 2^-32
+    __syncwarp();
+    tc_wait(bar, st.ph_mma);
+    st.ph_mma ^= 1u;
+    tc::fence_after_sync();
+    // level-1 epilogue: W[m][k1] at m * 64 + (k1 & 32) + ((k1 ^ m) & 31), in [0, 2q)
+    {
+        const uint32_t r2 = tca::canon(tca::mont_lazy(ratio, ratio, q, qinv), q);
+        uint32_t tw_e = start;
+        uint32_t tw_o = tca::canon(tca::mont_lazy(start, ratio, q, qinv), q);
+        const uint32_t tcol = st.taddr + h * 128u + ((quarter * 32u) << 16);
+        uint32_t* Wrow = reinterpret_cast<uint32_t*>(base + kTcA) + m * 64u + 32u * h;
+#pragma unroll 1
+        for (uint32_t part = 0; part < 4; part++) {
+            uint32_t c0[8], c1[8], c2[8], c3[8];
+            tca::ld_planes8(tcol + 8u * part, c0, c1, c2, c3);
+#pragma unroll
+            for (uint32_t i = 0; i < 8; i += 2) {
+                const uint32_t k = 8u * part + i;
+                Wrow[k ^ lane] = tca::mont_lazy(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
+                Wrow[(k + 1u) ^ lane] =
+                    tca::mont_lazy(tca::combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
+                tw_e = tca::canon(tca::mont_lazy(tw_e, r2, q, qinv), q);
+                tw_o = tca::canon(tca::mont_lazy(tw_o, r2, q, qinv), q);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    const uint32_t* W = reinterpret_cast<const uint32_t*>(base + kTcA);
+    switch (rl) {
+        case 0: tc_level2<0>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+        case 1: tc_level2<1>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+        case 2: tc_level2<2>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+        case 3: tc_level2<3>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+        default: tc_level2<4>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+    }
+}
+
+// The persistent queue with tensor-core tiles (256 threads, two CTAs per SM,
+// 256 TMEM columns each); units without UF_TC run the CUDA-core tile.
+template <uint32_t G>
+__global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__ BArgs a) {
+    extern __shared__ __align__(1024) uint8_t tc_raw[];
+    __shared__ uint32_t s_ticket, s_taddr;
+    __shared__ M32 s_ar[kMaxRows];
+    TcState st;
+    st.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(st.base + kTcBar);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(bar, 1);
+        tc::mbar_init(bar + 1, 1);
+    }
+    if (threadIdx.x < 32) tc::tmem_alloc(&s_taddr, 256);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    st.taddr = s_taddr;
+    st.ph_mma = st.ph_img = 0;
+    st.img_key = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_ticket = atomicAdd(a.ctr, 1u);
+        __syncthreads();
+        const uint32_t ticket = s_ticket;
+        if (ticket >= a.n_tiles) break;
+        const BTile tl = a.tiles[ticket];
+        const BUnit u = a.units[tl.unit];
+        const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
+        if (threadIdx.x == 0) {
+            if (!wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
+            __threadfence();
+        }
+        __syncthreads();
+        if (u.flags & UF_TC) {
+            run_tc_tile(a, u, pass, tile, st);
+        } else {
+            run_tile<256, G>(a, u, pass, tile, reinterpret_cast<uint32_t*>(st.base), s_ar);
+            st.img_key = 0;  // the tile overwrote the image
+        }
+        __threadfence();
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (threadIdx.x == 0)
+            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.ctr + 1 + 2 * tl.unit + pass) : "memory");
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) tc::tmem_dealloc(st.taddr, 256);
+}
+
 template <uint32_t E, uint32_t T, uint32_t G>
 // more resident CTAs for the small register groups
 __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T) batch_queue(const __grid_constant__ BArgs a) {
@@ -354,19 +659,7 @@ __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T
         const BUnit u = a.units[tl.unit];
         const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
         if (threadIdx.x == 0) {
-            bool ok = true;
-            if (pass == 1) {
-                ok = wait_ge(a.ctr + 1 + 2 * tl.unit, u.tiles_a);
-            } else {
-                if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, a.units[u.prev].tiles_b);
-                for (int d = 0; d < 2; d++) {
-                    const int32_t w = u.after[d];
-                    if (w < 0) continue;
-                    const BUnit& W = a.units[w];  // complete = its last pass has signalled every tile
-                    ok = wait_ge(a.ctr + (W.lg1 ? 2u : 1u) + 2 * (uint32_t)w, W.lg1 ? W.tiles_b : W.tiles_a) && ok;
-                }
-            }
-            if (!ok) atomicOr(&g_batch_error, 1u);
+            if (!wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
             __threadfence();
         }
         __syncthreads();
@@ -380,27 +673,67 @@ __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T
 
 // ---- host ------------------------------------------------------------------------
 struct Variant {
-    uint32_t E, T, G;
+    uint32_t E, T, G, tensor;
     void (*fn)(BArgs);
 };
 const Variant kVariants[] = {
-    {4096, 256, 1, batch_queue<4096, 256, 1>},    {4096, 256, 3, batch_queue<4096, 256, 3>},
-    {4096, 256, 4, batch_queue<4096, 256, 4>},    {8192, 256, 1, batch_queue<8192, 256, 1>},
-    {8192, 256, 3, batch_queue<8192, 256, 3>},    {8192, 256, 4, batch_queue<8192, 256, 4>},
-    {8192, 512, 1, batch_queue<8192, 512, 1>},    {8192, 512, 3, batch_queue<8192, 512, 3>},
-    {8192, 512, 4, batch_queue<8192, 512, 4>},    {16384, 512, 1, batch_queue<16384, 512, 1>},
-    {16384, 512, 3, batch_queue<16384, 512, 3>},  {16384, 512, 4, batch_queue<16384, 512, 4>},
+    {4096, 256, 1, 0, batch_queue<4096, 256, 1>},    {4096, 256, 3, 0, batch_queue<4096, 256, 3>},
+    {4096, 256, 4, 0, batch_queue<4096, 256, 4>},    {8192, 256, 1, 0, batch_queue<8192, 256, 1>},
+    {8192, 256, 3, 0, batch_queue<8192, 256, 3>},    {8192, 256, 4, 0, batch_queue<8192, 256, 4>},
+    {8192, 512, 1, 0, batch_queue<8192, 512, 1>},    {8192, 512, 3, 0, batch_queue<8192, 512, 3>},
+    {8192, 512, 4, 0, batch_queue<8192, 512, 4>},    {16384, 512, 1, 0, batch_queue<16384, 512, 1>},
+    {16384, 512, 3, 0, batch_queue<16384, 512, 3>},  {16384, 512, 4, 0, batch_queue<16384, 512, 4>},
+    // tensor-core tiles for the two-pass units, CUDA-core tiles of 4096 / 8192 for the rest
+    {4096, 256, 1, 1, batch_queue_tc<1>},            {4096, 256, 3, 1, batch_queue_tc<3>},
+    {4096, 256, 4, 1, batch_queue_tc<4>},            {8192, 256, 1, 1, batch_queue_tc<1>},
+    {8192, 256, 3, 1, batch_queue_tc<3>},            {8192, 256, 4, 1, batch_queue_tc<4>},
 };
 
-const Variant* find_variant(uint32_t E, uint32_t T, uint32_t G) {
+const Variant* find_variant(uint32_t E, uint32_t T, uint32_t G, uint32_t tensor) {
     for (const Variant& v : kVariants)
-        if (v.E == E && v.T == T && v.G == G) return &v;
+        if (v.E == E && v.T == T && v.G == G && v.tensor == tensor) return &v;
     return nullptr;
 }
 
-// tile elements + root powers + padding, in words
 // padded tile (E + E/32 + one word per vector) + root powers + slack, in bytes
 size_t smem_bytes(uint32_t E) { return ((size_t)E + E / 16 + kMaxRows + E / 2) * 4 + 64; }
+size_t smem_bytes(const Variant* v) { return v->tensor ? kTcSmem : smem_bytes(v->E); }
+
+// CTAs of a variant resident on the whole device (the persistent grid): the
+// kernel asks for the largest shared-memory carveout, so that the tensor-tile
+// kernel's ~100 KB CTAs fit two per SM.
+int resident_ctas(const Variant* v, uint32_t ctas_per_sm) {
+    const size_t smem = smem_bytes(v);
+    cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(v->fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v->fn, (int)v->T, smem) != cudaSuccess) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    if (v->tensor) {
+        // The runtime's answer for the tcgen05 kernel is one CTA per SM; its
+        // registers and shared memory fit two (and TMEM holds two 256-column
+        // allocations), so count from the resources themselves.
+        cudaFuncAttributes fa{};
+        int smem_sm = 0, regs_sm = 0, reserved = 0;
+        cudaFuncGetAttributes(&fa, v->fn);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        const size_t per_smem = fa.sharedSizeBytes + smem + (size_t)reserved;
+        const size_t per_regs = (size_t)((fa.numRegs * 32 + 255) / 256 * 256) * (v->T / 32);
+        int fit = 2;  // TMEM: 512 columns per SM
+        if (per_smem) fit = std::min<int>(fit, (int)(smem_sm / per_smem));
+        if (per_regs) fit = std::min<int>(fit, (int)(regs_sm / per_regs));
+        occ = std::max(occ, fit);
+    }
+    if (occ < 1) occ = 1;
+    if (ctas_per_sm && (int)ctas_per_sm < occ) occ = (int)ctas_per_sm;
+    return sms * occ;
+}
 
 uint32_t ilog2(uint64_t x) {
     uint32_t l = 0;
@@ -440,13 +773,16 @@ nttb_batch_config default_config() {
     c.lag = 2;
     c.ctas_per_sm = 0;
     c.group = 3;
+    c.tensor = 0;
     return c;
 }
 
 int check_config(const nttb_batch_config& c) {
-    if (!find_variant(c.tile_elems, c.threads, c.group))
+    if (c.tensor > 1) return fail(NTTB_ERR_INVALID_ARG, "batch config: tensor must be 0 or 1");
+    if (!find_variant(c.tile_elems, c.threads, c.group, c.tensor))
         return fail(NTTB_ERR_INVALID_ARG,
-                    "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512, group 1, 3 or 4");
+                    c.tensor ? "batch config: tensor tiles need 256 threads, tile_elems 4096 or 8192, group 1, 3 or 4"
+                             : "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512, group 1, 3 or 4");
     if (c.split > 1) return fail(NTTB_ERR_INVALID_ARG, "batch config: split must be 0 or 1");
     if (c.lag < 1 || c.lag > 64) return fail(NTTB_ERR_INVALID_ARG, "batch config: lag must be in [1, 64]");
     return 0;
@@ -463,14 +799,73 @@ void free_batch(Batch* b) {
     delete b;
 }
 
+// Pass geometry of a unit of 2^L residues (rows: limbs per single-pass tile).
+struct UnitShape {
+    uint32_t lg1 = 0, per = 1, va = 0, vb = 0, tiles_a = 1, tiles_b = 0;
+    bool tc = false;
+};
+bool unit_shape(const BatchPlan& P, const nttb_batch_config& cfg, uint32_t L, UnitShape* s) {
+    const uint32_t E = cfg.tile_elems, lgE = ilog2(E), n = 1u << L;
+    *s = UnitShape();
+    // tensor-core two-pass units: both pass lengths 64 r', r' in 1..16
+    s->tc = cfg.tensor && P.images && L > lgE && L >= 13 && L <= 20;
+    if (L <= lgE) {
+        s->per = std::min<uint32_t>(E >> L, kMaxRows);
+        return true;
+    }
+    uint32_t lg1 = cfg.split ? L / 2 : (L + 1) / 2;
+    if (s->tc) {
+        lg1 = std::max<uint32_t>(lg1, std::max<uint32_t>(6, L - 10));
+        lg1 = std::min<uint32_t>(lg1, std::min<uint32_t>(10, L - 6));
+        s->va = 128u >> (lg1 - 6);  // 8192 residues per tile: V = 128 / r' columns of length 64 r'
+        s->vb = 128u >> (L - lg1 - 6);
+    } else {
+        if (lg1 > lgE) lg1 = lgE;
+        if (L - lg1 > lgE) lg1 = L - lgE;
+        if (lg1 > lgE || lg1 == 0) return false;
+        s->va = std::min(E >> lg1, n >> lg1);
+        s->vb = std::min(E >> (L - lg1), 1u << lg1);
+    }
+    s->lg1 = lg1;
+    s->tiles_a = (n >> lg1) / s->va;
+    s->tiles_b = (1u << lg1) / s->vb;
+    return true;
+}
+
+// Workspace of the two-pass units: one ring per size class 2^L, S_L slots of
+// 2^L words each: at least 16 units and more than the lag, and for a batch
+// (count given) enough for ~1024 pass A tiles in flight unless the class has
+// fewer units.  Runners (count null) keep 16 per class: their job lists are
+// small.  A unit waits for the previous owner of its slot (same class) to
+// finish its pass B.
+struct WsLayout {
+    uint64_t base[25] = {};  // words
+    uint32_t slots[25] = {};
+    uint64_t words = 0;
+};
+WsLayout ws_layout(const BatchPlan& P, const nttb_batch_config& cfg, const uint32_t* count) {
+    WsLayout w;
+    for (uint32_t L = 1; L <= P.max_log; L++) {
+        UnitShape sh;
+        if (!unit_shape(P, cfg, L, &sh) || !sh.lg1) continue;
+        if (count && !count[L]) continue;
+        uint32_t S = std::max<uint32_t>(16, cfg.lag + 2);
+        if (count) S = std::min(std::max(S, (1024 + sh.tiles_a - 1) / sh.tiles_a), count[L]);
+        w.base[L] = w.words;
+        w.slots[L] = S;
+        w.words += (uint64_t)S << L;
+    }
+    return w;
+}
+
 // Units, queue order and workspace ring of one batch (host work only).
 // Units of phase 0 (plain jobs, forward halves of products) come first,
 // largest first; phase 1 holds the inverse units of products, which depend
 // on phase-0 units.  Every pass B tile deferred by the lag is flushed at the
 // phase boundary, so each awaited tile precedes its waiter in the queue.
 int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, const nttb_batch_config& cfg,
-               std::vector<BUnit>& units, std::vector<BTile>& tiles, uint32_t* ws_words_out, uint32_t* slots_out) {
-    const uint32_t E = cfg.tile_elems, lgE = ilog2(E);
+               std::vector<BUnit>& units, std::vector<BTile>& tiles, const WsLayout* fixed, WsLayout* layout_out) {
+    const uint32_t E = cfg.tile_elems;
     struct Pending {
         BUnit u;
         uint64_t work;
@@ -483,16 +878,11 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
                          uint32_t n_limbs, uint32_t uf, uint32_t phase, std::vector<uint32_t>* ids,
                          const std::vector<uint32_t>* dep_a, const std::vector<uint32_t>* dep_b) -> int {
         const uint32_t n = 1u << L;
-        uint32_t lg1 = 0, per = 1;
-        if (L <= lgE) {
-            per = std::min<uint32_t>(E >> L, kMaxRows);
-        } else {
-            lg1 = cfg.split ? L / 2 : (L + 1) / 2;
-            if (lg1 > lgE) lg1 = lgE;
-            if (L - lg1 > lgE) lg1 = L - lgE;
-            if (lg1 > lgE || lg1 == 0)
-                return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u too large for tile %u", j, L, E);
-        }
+        UnitShape sh;
+        if (!unit_shape(P, cfg, L, &sh))
+            return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u too large for tile %u", j, L, E);
+        const uint32_t lg1 = sh.lg1, per = sh.per;
+        const bool tcu = sh.tc;
         uint32_t k = 0;
         for (uint32_t l0 = 0; l0 < n_limbs; l0 += per, k++) {
             Pending p{};
@@ -501,18 +891,13 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
             u.pre_mul = pre_mul ? pre_mul + (size_t)l0 * n : nullptr;
             u.mod0 = first + l0;
             u.log_n = L;
-            u.flags = uf;
+            u.flags = uf | (tcu ? UF_TC : 0u);
             u.lg1 = lg1;
             u.rows = lg1 ? 1u : std::min(per, n_limbs - l0);
-            if (lg1) {
-                const uint32_t N1 = 1u << lg1, N2 = n >> lg1;
-                u.va = std::min(E / N1, N2);
-                u.vb = std::min(E / N2, N1);
-                u.tiles_a = N2 / u.va;
-                u.tiles_b = N1 / u.vb;
-            } else {
-                u.tiles_a = 1;
-            }
+            u.va = sh.va;
+            u.vb = sh.vb;
+            u.tiles_a = sh.tiles_a;
+            u.tiles_b = sh.tiles_b;
             u.prev = -1;
             u.after[0] = u.after[1] = -1;
             p.work = (uint64_t)u.rows * n * L;
@@ -559,19 +944,20 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
     });
     std::vector<int32_t> index_of(list.size());
     for (size_t i = 0; i < list.size(); i++) index_of[list[i].id] = (int32_t)i;
-    uint32_t max_two = 0, n_two = 0;
+    uint32_t count[25] = {};
     for (const Pending& p : list)
-        if (p.u.lg1) {
-            max_two = std::max(max_two, 1u << p.u.log_n);
-            n_two++;
-        }
+        if (p.u.lg1) count[p.u.log_n]++;
+    const WsLayout lay = fixed ? *fixed : ws_layout(P, cfg, count);
+    for (uint32_t L = 1; L < 25; L++)
+        if (count[L] && !lay.slots[L]) return fail(NTTB_ERR_INVALID_ARG, "batch: no workspace ring for log_n %u", L);
     const uint32_t lag = cfg.lag;
-    const uint32_t S = n_two ? std::max(lag + 2, std::min<uint32_t>(n_two, std::max<uint32_t>(16, lag + 2))) : 0;
     units.clear();
     tiles.clear();
-    std::vector<int32_t> slot_owner(S, -1);
+    std::vector<std::vector<int32_t>> slot_owner(25);
+    for (uint32_t L = 1; L < 25; L++) slot_owner[L].assign(lay.slots[L], -1);
+    uint32_t next_slot[25] = {};
     std::deque<uint32_t> pend_b;
-    uint32_t two_idx = 0, phase = 0;
+    uint32_t phase = 0;
     auto emit_b = [&](uint32_t ui) {
         for (uint32_t t = 0; t < units[ui].tiles_b; t++) tiles.push_back({ui, 0x80000000u | t});
     };
@@ -590,10 +976,11 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
         BUnit u = p.u;
         for (int d = 0; d < 2; d++) u.after[d] = p.after_id[d] >= 0 ? index_of[p.after_id[d]] : -1;
         if (u.lg1) {
-            const uint32_t slot = two_idx++ % S;
-            u.ws = reinterpret_cast<uint32_t*>((uintptr_t)slot * max_two * 4u);  // offset, rebased later
-            u.prev = slot_owner[slot];
-            slot_owner[slot] = (int32_t)ui;
+            const uint32_t L = u.log_n, slot = next_slot[L]++ % lay.slots[L];
+            // word offset, rebased on the workspace allocation later
+            u.ws = reinterpret_cast<uint32_t*>((uintptr_t)((lay.base[L] + ((uint64_t)slot << L)) * 4u));
+            u.prev = slot_owner[L][slot];
+            slot_owner[L][slot] = (int32_t)ui;
         }
         units.push_back(u);
         for (uint32_t t = 0; t < u.tiles_a; t++) tiles.push_back({ui, t});
@@ -606,8 +993,7 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
         }
     }
     flush();
-    *ws_words_out = max_two;
-    *slots_out = S;
+    if (layout_out) *layout_out = lay;
     return 0;
 }
 
@@ -615,17 +1001,17 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
     if (int rc = check_config(cfg)) return rc;
     std::vector<BUnit> units;
     std::vector<BTile> tiles;
-    uint32_t ws_words = 0, slots = 0;
-    if (int rc = plan_batch(*P, jobs, n_jobs, cfg, units, tiles, &ws_words, &slots)) return rc;
+    WsLayout lay;
+    if (int rc = plan_batch(*P, jobs, n_jobs, cfg, units, tiles, nullptr, &lay)) return rc;
     if (tiles.size() >= 0x7fffffffu || units.size() >= 0x7fffffffu)
         return fail(NTTB_ERR_INVALID_ARG, "batch: too many tiles");
     Batch* b = new Batch();
     b->plan = P;
     b->cfg = cfg;
-    b->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group);
+    b->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, cfg.tensor);
     b->n_units = (uint32_t)units.size();
     b->n_tiles = (uint32_t)tiles.size();
-    b->ws_bytes = (size_t)ws_words * slots * 4;
+    b->ws_bytes = (size_t)lay.words * 4;
     bool ok = true;
     ok = ok && cudaMalloc(&b->d_units, std::max<size_t>(1, units.size()) * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(BTile)) == cudaSuccess;
@@ -643,15 +1029,7 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
         free_batch(b);
         return fail(NTTB_ERR_CUDA, "batch: upload failed");
     }
-    const size_t smem = smem_bytes(cfg.tile_elems);
-    cudaFuncSetAttribute(b->var->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->var->fn, (int)cfg.threads, smem);
-    if (occ < 1) occ = 1;
-    if (cfg.ctas_per_sm && (int)cfg.ctas_per_sm < occ) occ = (int)cfg.ctas_per_sm;
-    b->grid = (int)std::min<uint64_t>((uint64_t)sms * occ, std::max<uint32_t>(1, b->n_tiles));
+    b->grid = (int)std::min<uint64_t>((uint64_t)resident_ctas(b->var, cfg.ctas_per_sm), std::max<uint32_t>(1, b->n_tiles));
     *out = b;
     return 0;
 }
@@ -666,13 +1044,14 @@ int launch_batch(Batch* b, cudaStream_t s, bool count) {
     a.ctr = b->d_ctr;
     a.n_tiles = b->n_tiles;
     a.max_log = b->plan->max_log;
+    a.images = b->plan->images;
     if (cudaMemsetAsync(b->d_ctr, 0, (1 + 2 * (size_t)b->n_units) * 4, s) != cudaSuccess)
         return fail(NTTB_ERR_CUDA, "batch: counter reset failed");
     if (count) {
         ProfScope prof("batch_queue", s);
-        b->var->fn<<<b->grid, b->var->T, smem_bytes(b->var->E), s>>>(a);
+        b->var->fn<<<b->grid, b->var->T, smem_bytes(b->var), s>>>(a);
     } else {
-        b->var->fn<<<b->grid, b->var->T, smem_bytes(b->var->E), s>>>(a);
+        b->var->fn<<<b->grid, b->var->T, smem_bytes(b->var), s>>>(a);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : fail(NTTB_ERR_CUDA, "batch: launch failed");
 }
@@ -691,6 +1070,7 @@ struct BatchRunner {
     BUnit* h_units = nullptr;  // pinned staging
     BTile* h_tiles = nullptr;
     size_t cap_units = 0, cap_tiles = 0, ws_bytes = 0;
+    WsLayout layout;
     int grid = 0;
     std::vector<BUnit> units;
     std::vector<BTile> tiles;
@@ -734,22 +1114,14 @@ int runner_create(BatchPlan* P, const nttb_batch_config& cfg, BatchRunner** out)
     auto* r = new BatchRunner();
     r->plan = P;
     r->cfg = cfg;
-    r->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group);
-    const size_t slots = std::max<size_t>(16, cfg.lag + 2);
-    r->ws_bytes = slots * ((size_t)4 << P->max_log);
-    if (cudaMalloc(&r->d_ws, r->ws_bytes) != cudaSuccess || runner_reserve(r, 256, 4096)) {
+    r->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, cfg.tensor);
+    r->layout = ws_layout(*P, cfg, nullptr);  // rings for every size class the plan allows
+    r->ws_bytes = (size_t)r->layout.words * 4;
+    if ((r->ws_bytes && cudaMalloc(&r->d_ws, r->ws_bytes) != cudaSuccess) || runner_reserve(r, 256, 4096)) {
         runner_destroy(r);
         return fail(NTTB_ERR_NO_MEMORY, "batch runner: allocation failed");
     }
-    const size_t smem = smem_bytes(cfg.tile_elems);
-    cudaFuncSetAttribute(r->var->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, r->var->fn, (int)cfg.threads, smem);
-    if (occ < 1) occ = 1;
-    if (cfg.ctas_per_sm && (int)cfg.ctas_per_sm < occ) occ = (int)cfg.ctas_per_sm;
-    r->grid = sms * occ;
+    r->grid = resident_ctas(r->var, cfg.ctas_per_sm);
     *out = r;
     return 0;
 }
@@ -768,9 +1140,7 @@ size_t runner_device_bytes(const BatchRunner* r) {
 // Plans the jobs, uploads the queue from pinned staging and launches, all on
 // `s`.  One run per runner may be in flight: the staging is reused.
 int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cudaStream_t s) {
-    uint32_t ws_words = 0, slots = 0;
-    if (int rc = plan_batch(*r->plan, jobs, n_jobs, r->cfg, r->units, r->tiles, &ws_words, &slots)) return rc;
-    if ((size_t)ws_words * slots * 4 > r->ws_bytes) return fail(NTTB_ERR_INVALID_ARG, "batch runner: workspace too small");
+    if (int rc = plan_batch(*r->plan, jobs, n_jobs, r->cfg, r->units, r->tiles, &r->layout, nullptr)) return rc;
     if (r->tiles.empty()) return 0;
     if (r->units.size() > r->cap_units || r->tiles.size() > r->cap_tiles) {
         cudaStreamSynchronize(s);  // the previous run may still read the queue
@@ -789,6 +1159,7 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
     a.ctr = r->d_ctr;
     a.n_tiles = (uint32_t)r->tiles.size();
     a.max_log = r->plan->max_log;
+    a.images = r->plan->images;
     bool ok = cudaMemcpyAsync(r->d_units, r->h_units, r->units.size() * sizeof(BUnit), cudaMemcpyHostToDevice, s) ==
               cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->d_tiles, r->h_tiles, r->tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice, s) ==
@@ -797,14 +1168,14 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
     if (!ok) return fail(NTTB_ERR_CUDA, "batch runner: queue upload failed");
     const int grid = (int)std::min<size_t>((size_t)r->grid, r->tiles.size());
     ProfScope prof("batch_queue", s);
-    r->var->fn<<<grid, r->var->T, smem_bytes(r->var->E), s>>>(a);
+    r->var->fn<<<grid, r->var->T, smem_bytes(r->var), s>>>(a);
     return cudaGetLastError() == cudaSuccess ? 0 : fail(NTTB_ERR_CUDA, "batch runner: launch failed");
 }
 
 size_t batch_plan_device_bytes(const BatchPlan* P) {
     const uint32_t lo = std::min<uint32_t>(kLoBits, P->max_log);
     return (size_t)P->limbs.size() * 4 * 4 * (((size_t)1 << (P->max_log - lo)) + ((size_t)1 << lo)) +
-           P->limbs.size() * sizeof(BModulus);
+           P->limbs.size() * sizeof(BModulus) + (P->images ? P->limbs.size() * 3 * (size_t)kImgBytes : 0);
 }
 
 uint32_t batch_device_errors(bool clear) {
@@ -901,6 +1272,34 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
         for (uint32_t L = 0; L < 25; L++) M.ninv[L] = nttb::h_to_mont32(nttb::h_invmod((1ull << L) % q, q), q);
         M.r2 = nttb::h_to_mont32(nttb::h_to_mont32(1, q), q);
     }
+    if (max_log_n >= 13) {
+        // DFT-64 images per modulus: forward (omega_64), inverse, and the
+        // negacyclic forward with psi_128^j on the input index
+        const size_t per = 3 * (size_t)nttb::kImgBytes;
+        std::vector<uint8_t> img(per * n_moduli, 0);
+        for (uint32_t l = 0; l < n_moduli; l++) {
+            const nttb::LimbHost& H = P.limbs[l];
+            const uint64_t q = H.q;
+            const uint64_t w64 = nttb::h_powmod(H.omega, N / 64, q), w64i = nttb::h_powmod(H.omega_inv, N / 64, q);
+            uint8_t* d = img.data() + per * l;
+            nttb::tc_build_image64(d, nttb::tc_dft_matrix(64, w64, q), q);
+            nttb::tc_build_image64(d + nttb::kImgBytes, nttb::tc_dft_matrix(64, w64i, q), q);
+            if (nega)
+                nttb::tc_build_image64(d + 2 * nttb::kImgBytes,
+                                       nttb::tc_dft_matrix(64, w64, q, 1, nttb::h_powmod(H.psi, N / 64, q)), q);
+        }
+        uint8_t* d = nullptr;
+        if (cudaMalloc(&d, img.size()) != cudaSuccess ||
+            cudaMemcpy(d, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            if (d) cudaFree(d);
+            for (void* a : P.allocations) cudaFree(a);
+            delete P.mods;
+            delete h;
+            return fail(NTTB_ERR_NO_MEMORY, "nttb_batch_plan_create: DFT-64 images");
+        }
+        P.allocations.push_back(d);
+        P.images = d;
+    }
     if (cudaMalloc(&P.mods->d, mods.size() * sizeof(nttb::BModulus)) != cudaSuccess ||
         cudaMemcpy(P.mods->d, mods.data(), mods.size() * sizeof(nttb::BModulus), cudaMemcpyHostToDevice) != cudaSuccess) {
         for (void* a : P.allocations) cudaFree(a);
@@ -987,6 +1386,12 @@ NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t*
     return NTTB_OK;
 }
 
+NTTB_API int nttb_batch_ctas(const nttb_batch* batch, uint32_t* ctas) {
+    if (!batch || !ctas) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_ctas: null argument");
+    *ctas = (uint32_t)batch->b->grid;
+    return NTTB_OK;
+}
+
 NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs, void* stream,
                                  nttb_batch_config* out) {
     if (!plan || !jobs || n_jobs == 0) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: no jobs");
@@ -1029,7 +1434,9 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
             off += (size_t)c.n_limbs << c.log_n;
         }
     }
-    const uint32_t shapes[4][2] = {{4096, 256}, {8192, 256}, {8192, 512}, {16384, 512}};
+    // {tile, threads, tensor}
+    const uint32_t shapes[6][3] = {{4096, 256, 0}, {8192, 256, 0}, {8192, 512, 0}, {16384, 512, 0},
+                                   {4096, 256, 1}, {8192, 256, 1}};
     const uint32_t lags[2] = {1, 4}, groups[3] = {1, 3, 4};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -1044,6 +1451,8 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
                 nttb_batch_config c = nttb::default_config();
                 c.tile_elems = sh[0];
                 c.threads = sh[1];
+                c.tensor = sh[2];
+                if (c.tensor && !plan->p.images) continue;
                 c.split = split;
                 c.lag = lag;
                 c.group = grp;

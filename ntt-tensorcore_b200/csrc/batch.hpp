@@ -18,6 +18,7 @@ struct BatchPlan {
     bool negacyclic = false;
     std::vector<LimbHost> limbs;
     Mods* mods = nullptr;
+    uint8_t* images = nullptr;  // DFT-64 images of the tensor-core tiles (max_log >= 13), 3 x 64 KB per modulus
     std::vector<void*> allocations;
     nttb_batch_config tuned{};
     bool have_tuned = false;

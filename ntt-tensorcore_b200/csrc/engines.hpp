@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "plan.hpp"
 
 namespace nttb {
@@ -19,5 +21,13 @@ int auto_engine32(const Plan32& p, bool src_u64);
 void engines_release32(Plan32* p);
 
 int fail(int code, const char* fmt, ...);
+
+// Byte-plane image of a 64 x 64 matrix W (mod q) as the INT8 contraction's
+// B operand: 256 rows ordered (k / 32, a, k % 32) x 256 bytes, K-major SW128
+// in two 128-byte K blocks (64 KB).  tc_dft_matrix(L, root, ...) returns
+// W[k][j] = scale * row_twist^k * col_twist^j * root^(j k).
+void tc_build_image64(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q);
+std::vector<uint64_t> tc_dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t row_twist = 1,
+                                    uint64_t col_twist = 1, uint64_t scale = 1);
 
 }  // namespace nttb

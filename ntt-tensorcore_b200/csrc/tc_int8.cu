@@ -63,6 +63,7 @@
 #include "engines.hpp"
 #include "plan.hpp"
 #include "profiler.hpp"
+#include "tc_arith.cuh"
 #include "tcgen05.cuh"
 
 namespace nttb {
@@ -72,6 +73,8 @@ namespace nttb {
 __device__ uint32_t g_tc_error;
 
 namespace {
+
+using namespace tca;
 
 constexpr uint32_t kMatBytes64 = 64 * 1024;  // DFT-64 byte-plane image (256 rows x 256 B)
 constexpr uint32_t kMatBytes16 = 4 * 1024;   // DFT-16 byte-plane image (64 rows x 64 B)
@@ -125,44 +128,7 @@ struct ClArgs {
     uint32_t n_stages, n_limbs, units, pad_;
 };
 
-// ---- device arithmetic ------------------------------------------------------------
-// 32 x 32 + 64 -> 64 multiply-add (one mad.wide.u32).
-__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
-    uint64_t r;
-    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(r) : "r"(a), "r"(b), "l"(c));
-    return r;
-}
-__device__ __forceinline__ uint32_t redc64(uint64_t v, uint32_t q, uint32_t qinv) {
-    const uint32_t m = (uint32_t)v * qinv;
-    return (uint32_t)(mad_wide(m, q, v) >> 32);  // [0, 2q) for v < q * 2^32
-}
-// Planes c_a <= 256 * 255^2 (K = 256 byte products), so c0 + 256 c1 and
-// c2 + 256 c3 fit in 32 bits; v = sum_a 256^a c_a < 2^49.
-__device__ __forceinline__ uint32_t combine_redc(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t q,
-                                                 uint32_t qinv) {
-    const uint32_t lo = c0 + (c1 << 8), hi = c2 + (c3 << 8);
-    return redc64(mad_wide(hi, 65536u, (uint64_t)lo), q, qinv);
-}
-// a < 2q, b < q -> a*b*2^-32 mod q in [0, 2q)
-__device__ __forceinline__ uint32_t mont_lazy(uint32_t a, uint32_t b, uint32_t q, uint32_t qinv) {
-    return redc64(mad_wide(a, b, 0ull), q, qinv);
-}
-__device__ __forceinline__ uint32_t canon(uint32_t x, uint32_t q) { return x >= q ? x - q : x; }
-
 __device__ __forceinline__ void flag_error(uint32_t bit) { atomicOr(&g_tc_error, bit); }
-
-// Issues the K = 256-byte contraction (8 MMAs of K = 32) into TMEM columns
-// [tmem, tmem + N).  The caller commits.
-__device__ __forceinline__ void issue_k256(uint32_t tmem, uint32_t a0, uint32_t a_rows, uint32_t b0, uint32_t b_rows,
-                                           uint32_t N) {
-    const uint32_t idesc = tc::idesc_u8(128, N);
-#pragma unroll
-    for (uint32_t ks = 0; ks < 8; ks++) {
-        const uint32_t ka = a0 + (ks >> 2) * a_rows * 128u + (ks & 3u) * 32u;
-        const uint32_t kb = b0 + (ks >> 2) * b_rows * 128u + (ks & 3u) * 32u;
-        tc::mma_i8(tmem, tc::desc_k_sw128(ka), tc::desc_k_sw128(kb), idesc, ks > 0);
-    }
-}
 
 // Same contraction with operand A in the stage B level-1 layout: SW64, four
 // 64-byte K blocks of `a_rows` rows each.
@@ -181,17 +147,6 @@ __device__ __forceinline__ void issue_k256_a64(uint32_t tmem, uint32_t a0, uint3
 // bits [6][5][4:3][2:0] of m -> bits [6][3][5:4][2:0].
 __device__ __forceinline__ uint32_t beta(uint32_t m) {
     return ((m >> 3) & 3u) * 16u + ((m >> 5) & 1u) * 8u + (m & 7u) + (m >> 6) * 64u;
-}
-
-// Eight outputs' four planes (a = 0..3 at columns col + 32a) of this thread's
-// TMEM lane (one N = 128 output half: columns a * 32 + k % 32).
-__device__ __forceinline__ void ld_planes8(uint32_t col, uint32_t (&c0)[8], uint32_t (&c1)[8], uint32_t (&c2)[8],
-                                           uint32_t (&c3)[8]) {
-    tc::ld_32x32b_x8(col + 0, c0);
-    tc::ld_32x32b_x8(col + 32, c1);
-    tc::ld_32x32b_x8(col + 64, c2);
-    tc::ld_32x32b_x8(col + 96, c3);
-    tc::ld_wait();
 }
 
 // Shared state of one CTA.
@@ -774,6 +729,13 @@ int launch_stages(Int8Cache* c, ClArgs& a, cudaStream_t s) {
 }
 
 }  // namespace
+
+// DFT-64 byte-plane images for other kernels (the batch engine's tensor tiles).
+void tc_build_image64(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) { build_image64(img, W, q); }
+std::vector<uint64_t> tc_dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t row_twist, uint64_t col_twist,
+                                    uint64_t scale) {
+    return dft_matrix(L, root, q, row_twist, col_twist, scale);
+}
 
 bool int8_serves(const Plan32& p, bool src_u64) { return !src_u64 && p.log_n == 16; }
 

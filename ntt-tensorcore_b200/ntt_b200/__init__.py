@@ -49,9 +49,9 @@ class BatchJob(ctypes.Structure):
 
 
 class BatchConfig(ctypes.Structure):
-    """nttb_batch_config: tile_elems, threads, split, lag, ctas_per_sm, group."""
+    """nttb_batch_config: tile_elems, threads, split, lag, ctas_per_sm, group, tensor."""
     _fields_ = [("tile_elems", _u32), ("threads", _u32), ("split", _u32), ("lag", _u32), ("ctas_per_sm", _u32),
-                ("group", _u32)]
+                ("group", _u32), ("tensor", _u32)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -129,6 +129,7 @@ def lib():
         "nttb_batch_plan_create": (_int, [_vp, _u32, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_batch_plan_destroy": (_int, [_vp]),
         "nttb_batch_default_config": (_int, [ctypes.POINTER(BatchConfig)]),
+        "nttb_batch_ctas": (_int, [_vp, ctypes.POINTER(_u32)]),
         "nttb_batch_autotune": (_int, [_vp, _vp, _u32, _vp, ctypes.POINTER(BatchConfig)]),
         "nttb_batch_create": (_int, [_vp, _vp, _u32, ctypes.POINTER(BatchConfig), ctypes.POINTER(_vp)]),
         "nttb_batch_destroy": (_int, [_vp]),
@@ -253,7 +254,10 @@ class Batch:
     def info(self):
         u, t, w, cfg = _u64(), _u64(), _u64(), BatchConfig()
         _check(lib().nttb_batch_info(self._h, ctypes.byref(u), ctypes.byref(t), ctypes.byref(w), ctypes.byref(cfg)))
-        return {"units": int(u.value), "tiles": int(t.value), "ws_bytes": int(w.value), "config": cfg.as_dict()}
+        g = _u32()
+        _check(lib().nttb_batch_ctas(self._h, ctypes.byref(g)))
+        return {"units": int(u.value), "tiles": int(t.value), "ws_bytes": int(w.value), "config": cfg.as_dict(),
+                "ctas": int(g.value)}
 
     def close(self):
         if getattr(self, "_h", None):

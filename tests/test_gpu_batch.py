@@ -19,6 +19,14 @@ CONFIGS = [
     {"tile_elems": 8192, "threads": 512, "split": 0, "lag": 3, "group": 3},
     {"tile_elems": 8192, "threads": 256, "split": 1, "lag": 2, "group": 4},
     {"tile_elems": 16384, "threads": 512, "split": 1, "lag": 4, "ctas_per_sm": 1, "group": 4},
+    {"tile_elems": 4096, "threads": 256, "split": 0, "lag": 2, "group": 3, "tensor": 1},
+    {"tile_elems": 8192, "threads": 256, "split": 1, "lag": 1, "group": 1, "tensor": 1},
+]
+
+TENSOR = [
+    {"tile_elems": 4096, "threads": 256, "split": 0, "lag": 2, "group": 3, "tensor": 1},
+    {"tile_elems": 4096, "threads": 256, "split": 1, "lag": 4, "group": 4, "tensor": 1},
+    {"tile_elems": 8192, "threads": 256, "split": 0, "lag": 1, "group": 1, "tensor": 1},
 ]
 
 
@@ -181,3 +189,82 @@ def test_batch_polymul_fused(torch_cuda, nega):
             for l in range(limbs):
                 ref = O.polymul_negacyclic(a[l].astype(np.uint64), b[l].astype(np.uint64), PRIMES[first + l])
                 assert (got[l] == ref).all()
+
+
+@pytest.mark.parametrize("config", TENSOR)
+def test_batch_tensor_tiles_every_size(torch_cuda, config):
+    """Tensor-core tiles (INT8 DFT-64 + DFT-r' on the CUDA cores) for every
+    two-pass size 2^13 .. 2^20, both directions and twists, in one launch with
+    CUDA-core units of the smaller sizes."""
+    rng = np.random.default_rng(31 + config["split"])
+    plan = nb.BatchPlan(PRIMES, 20, negacyclic=True)
+    jobs = []
+    for lg in range(13, 21):
+        for inv in (False, True):
+            for nega in (False, True):
+                limbs = 1 if lg >= 18 else 2
+                first = int(rng.integers(0, len(PRIMES) - limbs + 1))
+                x = np.stack([rng.integers(0, PRIMES[first + l], 1 << lg, dtype=np.uint64)
+                              for l in range(limbs)]).astype(np.uint32)
+                jobs.append([x, to_dev(torch_cuda, x.reshape(-1)), lg, limbs, first, inv, nega])
+    jobs += make_jobs(torch_cuda, rng, 12, (1, 12), (1, 3), len(PRIMES))
+    b = plan.batch(spec(jobs), config)
+    assert b.info()["config"]["tensor"] == 1
+    b.launch()
+    check(torch_cuda, jobs)
+
+
+def test_batch_tensor_round_trip_and_graph(torch_cuda):
+    """Forward then inverse batches on tensor tiles return the input; a graph
+    replay gives the launch's results."""
+    rng = np.random.default_rng(41)
+    plan = nb.BatchPlan(PRIMES, 20, negacyclic=True)
+    cfg = TENSOR[0]
+    jobs = make_jobs(torch_cuda, rng, 16, (12, 20), (1, 3), len(PRIMES))
+    fwd = [(j[1], j[2], j[3], j[4], False, j[6]) for j in jobs]
+    inv = [(j[1], j[2], j[3], j[4], True, j[6]) for j in jobs]
+    bf, bi = plan.batch(fwd, cfg), plan.batch(inv, cfg)
+    for rep in range(2):
+        if rep:
+            bf.graph_launch()
+            bi.graph_launch()
+        else:
+            bf.launch()
+            bi.launch()
+        torch_cuda.cuda.synchronize()
+        for j in jobs:
+            assert (to_host(j[1], np.uint32).reshape(j[0].shape) == j[0]).all(), j[2:]
+    assert nb.device_errors() == 0
+
+
+@pytest.mark.parametrize("nega", [True, False])
+def test_batch_tensor_polymul(torch_cuda, nega):
+    """Products whose transforms run on tensor tiles (2^13 .. 2^17) next to
+    small CUDA-core products, one launch."""
+    rng = np.random.default_rng(51 + nega)
+    plan = nb.BatchPlan(PRIMES, 17, negacyclic=nega)
+    prods = []
+    for lg in [4, 9, 12, 13, 14, 15, 16, 17, 13, 16]:
+        limbs = int(rng.integers(1, 4))
+        first = int(rng.integers(0, len(PRIMES) - limbs + 1))
+        mods = PRIMES[first:first + limbs]
+        a = np.stack([rng.integers(0, q, 1 << lg, dtype=np.uint64) for q in mods]).astype(np.uint32)
+        b = np.stack([rng.integers(0, q, 1 << lg, dtype=np.uint64) for q in mods]).astype(np.uint32)
+        prods.append((a, b, to_dev(torch_cuda, a.reshape(-1)), to_dev(torch_cuda, b.reshape(-1)), lg, limbs, first))
+    jobs = [(p[2], p[4], p[5], p[6], "mul", nega, p[3]) for p in prods]
+    plan.batch(jobs, TENSOR[1]).launch()
+    torch_cuda.cuda.synchronize()
+    for a, b, da, db, lg, limbs, first in prods:
+        got = to_host(da, np.uint32).reshape(a.shape).astype(np.uint64)
+        want = expect_product(a, b, PRIMES[first:first + limbs], nega)
+        assert (got == want).all(), (lg, limbs, int((got != want).sum()))
+    assert nb.device_errors() == 0
+
+
+def test_batch_tensor_rejects_bad_config(torch_cuda):
+    plan = nb.BatchPlan(PRIMES[:2], 14, negacyclic=False)
+    d = torch_cuda.zeros(1 << 14, dtype=torch_cuda.int32, device="cuda")
+    for bad in ({"tile_elems": 8192, "threads": 512, "tensor": 1}, {"tile_elems": 16384, "threads": 512, "tensor": 1},
+                {"tensor": 2}):
+        with pytest.raises(nb.NTTError):
+            plan.batch([(d, 14, 1, 0, False, False)], bad)
