@@ -499,7 +499,8 @@ def run_uneven(args, world, rank, local):
                    "workspace_bytes": info["ws_bytes"], "tuned": tuned, "l2": "inputs 7.9 GB >> L2",
                    "parallelism": "replicas x%d" % world},
         "graph_replay": {"value": world * coeffs * args.steps / (g_ms / 1e3), "ms_per_step": g_ms / args.steps},
-        "roofline": {"bound": "hbm", "kernel": "batch_queue", "achieved": alg_bytes / avg_s / 1e9, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "batch_queue_tc" if info["config"].get("tensor") else "batch_queue",
+                     "achieved": alg_bytes / avg_s / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": alg_bytes / avg_s / 1e9 / peak, "traffic": None,
                      "model_bytes_per_launch": model_bytes, "model_frac": model_bytes / avg_s / 1e9 / peak,
                      "alg_bytes_per_launch": alg_bytes,

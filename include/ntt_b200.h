@@ -201,9 +201,9 @@ typedef struct {
     uint32_t lag;         /* two-pass units between a unit's first and second pass in the queue (1..64) */
     uint32_t ctas_per_sm; /* 0: as many as fit */
     uint32_t group;       /* radix-2 stages per register group inside a tile: 1, 3 or 4 */
-    uint32_t tensor;      /* 1: two-pass units of 2^13 .. 2^20 residues run tensor-core tiles (INT8
-                             DFT-64 + radix-2 DFT of up to 16 points); needs threads 256, tile_elems
-                             4096 or 8192 (units above the tile size take them) */
+    uint32_t tensor;      /* 1: two-pass units of 2^13 .. 2^20 residues (the sizes above the tile) run
+                             tensor-core tiles (INT8 DFT-64 + radix-2 DFT of up to 16 points) where the
+                             shape allows: threads 256 and tile_elems 4096 or 8192; otherwise ignored */
 } nttb_batch_config;
 
 /* flags: NTTB_NEGACYCLIC to allow negacyclic jobs (moduli then need 2^(max_log_n+1) | q-1). */

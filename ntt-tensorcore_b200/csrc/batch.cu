@@ -767,22 +767,21 @@ namespace {
 
 nttb_batch_config default_config() {
     nttb_batch_config c{};
-    c.tile_elems = 8192;
+    c.tile_elems = 4096;
     c.threads = 256;
-    c.split = 0;
-    c.lag = 2;
+    c.split = 1;
+    c.lag = 4;
     c.ctas_per_sm = 0;
     c.group = 3;
-    c.tensor = 0;
+    c.tensor = 1;
     return c;
 }
 
 int check_config(const nttb_batch_config& c) {
     if (c.tensor > 1) return fail(NTTB_ERR_INVALID_ARG, "batch config: tensor must be 0 or 1");
-    if (!find_variant(c.tile_elems, c.threads, c.group, c.tensor))
+    if (!find_variant(c.tile_elems, c.threads, c.group, 0))
         return fail(NTTB_ERR_INVALID_ARG,
-                    c.tensor ? "batch config: tensor tiles need 256 threads, tile_elems 4096 or 8192, group 1, 3 or 4"
-                             : "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512, group 1, 3 or 4");
+                    "batch config: tile_elems/threads must be 4096/256, 8192/256, 8192/512 or 16384/512, group 1, 3 or 4");
     if (c.split > 1) return fail(NTTB_ERR_INVALID_ARG, "batch config: split must be 0 or 1");
     if (c.lag < 1 || c.lag > 64) return fail(NTTB_ERR_INVALID_ARG, "batch config: lag must be in [1, 64]");
     return 0;
@@ -799,6 +798,12 @@ void free_batch(Batch* b) {
     delete b;
 }
 
+// Tensor-core tiles are used where the configuration has a tensor kernel
+// (256 threads, CUDA-core tiles of 4096 or 8192 residues for the other units).
+bool tensor_tiles(const nttb_batch_config& cfg) {
+    return cfg.tensor && find_variant(cfg.tile_elems, cfg.threads, cfg.group, 1);
+}
+
 // Pass geometry of a unit of 2^L residues (rows: limbs per single-pass tile).
 struct UnitShape {
     uint32_t lg1 = 0, per = 1, va = 0, vb = 0, tiles_a = 1, tiles_b = 0;
@@ -808,7 +813,7 @@ bool unit_shape(const BatchPlan& P, const nttb_batch_config& cfg, uint32_t L, Un
     const uint32_t E = cfg.tile_elems, lgE = ilog2(E), n = 1u << L;
     *s = UnitShape();
     // tensor-core two-pass units: both pass lengths 64 r', r' in 1..16
-    s->tc = cfg.tensor && P.images && L > lgE && L >= 13 && L <= 20;
+    s->tc = tensor_tiles(cfg) && P.images && L > lgE && L >= 13 && L <= 20;
     if (L <= lgE) {
         s->per = std::min<uint32_t>(E >> L, kMaxRows);
         return true;
@@ -1008,7 +1013,10 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
     Batch* b = new Batch();
     b->plan = P;
     b->cfg = cfg;
-    b->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, cfg.tensor);
+    // without tensor-core units the CUDA-core kernel runs (more CTAs per SM)
+    bool any_tc = false;
+    for (const BUnit& u : units) any_tc = any_tc || (u.flags & UF_TC);
+    b->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, cfg.tensor && any_tc ? 1u : 0u);
     b->n_units = (uint32_t)units.size();
     b->n_tiles = (uint32_t)tiles.size();
     b->ws_bytes = (size_t)lay.words * 4;
@@ -1114,7 +1122,7 @@ int runner_create(BatchPlan* P, const nttb_batch_config& cfg, BatchRunner** out)
     auto* r = new BatchRunner();
     r->plan = P;
     r->cfg = cfg;
-    r->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, cfg.tensor);
+    r->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, tensor_tiles(cfg) ? 1u : 0u);
     r->layout = ws_layout(*P, cfg, nullptr);  // rings for every size class the plan allows
     r->ws_bytes = (size_t)r->layout.words * 4;
     if ((r->ws_bytes && cudaMalloc(&r->d_ws, r->ws_bytes) != cudaSuccess) || runner_reserve(r, 256, 4096)) {

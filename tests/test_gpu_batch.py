@@ -261,10 +261,14 @@ def test_batch_tensor_polymul(torch_cuda, nega):
     assert nb.device_errors() == 0
 
 
-def test_batch_tensor_rejects_bad_config(torch_cuda):
-    plan = nb.BatchPlan(PRIMES[:2], 14, negacyclic=False)
-    d = torch_cuda.zeros(1 << 14, dtype=torch_cuda.int32, device="cuda")
-    for bad in ({"tile_elems": 8192, "threads": 512, "tensor": 1}, {"tile_elems": 16384, "threads": 512, "tensor": 1},
-                {"tensor": 2}):
-        with pytest.raises(nb.NTTError):
-            plan.batch([(d, 14, 1, 0, False, False)], bad)
+def test_batch_tensor_flag_where_the_shape_allows(torch_cuda):
+    """tensor = 1 with a 512-thread shape runs the CUDA-core tiles (same
+    results); tensor = 2 is refused."""
+    rng = np.random.default_rng(61)
+    plan = nb.BatchPlan(PRIMES[:4], 16, negacyclic=True)
+    jobs = make_jobs(torch_cuda, rng, 6, (13, 16), (1, 2), 4)
+    b = plan.batch(spec(jobs), {"tile_elems": 8192, "threads": 512, "tensor": 1})
+    b.launch()
+    check(torch_cuda, jobs)
+    with pytest.raises(nb.NTTError):
+        plan.batch(spec(jobs), {"tensor": 2})
