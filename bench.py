@@ -489,6 +489,15 @@ def run_uneven(args, world, rank, local):
     # units of two passes move each residue twice (through the workspace ring)
     two_pass = sum(b << a for a, b, _ in shapes if a > {4096: 12, 8192: 13, 16384: 14}[info["config"]["tile_elems"]])
     model_bytes = 8 * (coeffs - two_pass) + 16 * two_pass
+    traffic, traffic_src = None, None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            bpr = json.load(f).get("batch_queue_tc_bytes_per_residue")
+        if bpr and info["config"].get("tensor"):
+            traffic = bpr * coeffs
+            traffic_src = "ncu DRAM bytes per residue of a 150 M-residue capture, scaled to this launch's residues"
+    except OSError:
+        pass
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -501,7 +510,8 @@ def run_uneven(args, world, rank, local):
         "graph_replay": {"value": world * coeffs * args.steps / (g_ms / 1e3), "ms_per_step": g_ms / args.steps},
         "roofline": {"bound": "hbm", "kernel": "batch_queue_tc" if info["config"].get("tensor") else "batch_queue",
                      "achieved": alg_bytes / avg_s / 1e9, "peak": peak,
-                     "unit": "GB/s", "frac": alg_bytes / avg_s / 1e9 / peak, "traffic": None,
+                     "unit": "GB/s", "frac": alg_bytes / avg_s / 1e9 / peak, "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "model_bytes_per_launch": model_bytes, "model_frac": model_bytes / avg_s / 1e9 / peak,
                      "alg_bytes_per_launch": alg_bytes,
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"},
