@@ -108,7 +108,13 @@ struct BUnit {
     uint32_t tiles_a, tiles_b;
     int32_t prev;      // two-pass unit that held the same workspace slot before, or -1
     int32_t after[2];  // units that must be complete before this one starts, or -1
+    // what pass A waits for, self-contained: counter ctr[2 + 2 prev] >= need[0],
+    // ctr[after_ctr[d]] >= need[1 + d] (the last pass of unit after[d])
+    uint32_t need[3];
+    uint32_t after_ctr[2];
+    uint32_t pad_;
 };
+static_assert(sizeof(BUnit) % 16 == 0, "unit records are copied in 16-byte pieces");
 
 struct BTile {
     uint32_t unit;
@@ -352,17 +358,12 @@ __device__ __forceinline__ bool wait_deps(const BArgs& a, const BUnit& u, uint32
     if (pass == 1) {
         ok = wait_ge(a.ctr + 1 + 2 * ui, u.tiles_a);
     } else {
-        if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, a.units[u.prev].tiles_b);
-        for (int d = 0; d < 2; d++) {
-            const int32_t w = u.after[d];
-            if (w < 0) continue;
-            const BUnit& W = a.units[w];  // complete = its last pass has signalled every tile
-            ok = wait_ge(a.ctr + (W.lg1 ? 2u : 1u) + 2 * (uint32_t)w, W.lg1 ? W.tiles_b : W.tiles_a) && ok;
-        }
+        if (u.prev >= 0) ok = wait_ge(a.ctr + 2 + 2 * (uint32_t)u.prev, u.need[0]);
+        for (int d = 0; d < 2; d++)
+            if (u.after[d] >= 0) ok = wait_ge(a.ctr + u.after_ctr[d], u.need[1 + d]) && ok;
     }
     return ok;
 }
-
 // ---- tensor-core tiles ----------------------------------------------------------------
 // A two-pass unit of 2^13 .. 2^20 residues whose pass lengths are len = 64 r'
 // (r' = 1, 2, 4, 8, 16) runs its tiles on the tensor cores.  A tile is the
@@ -376,26 +377,38 @@ __device__ __forceinline__ bool wait_deps(const BArgs& a, const BUnit& u, uint32
 //            negacyclic input twist psi^(b2 N2 + col) (its psi^(a2 n / 64)
 //            part is folded into the forward image), generated as two
 //            interleaved chains in the epilogue;
-//   level 2: for each (column, k1), a DFT-r' over b2 on the CUDA cores
-//            (radix 2 in registers) times the factors that depend on k2
-//            (pass A: omega_n^(64 col k2); negacyclic inverse: psi^-(64 N1 k2)).
+//   level 2: for each (column, k1), a DFT-r' over b2, times the factors that
+//            depend on k2 (pass A: omega_n^(64 col k2); negacyclic inverse:
+//            psi^-(64 N1 k2), which for pass B is psi_max^-(2^max_log k2 / r')
+//            whatever n is, so it lives in that image's rows).
+//            r' = 8, 16: a second INT8 contraction (M = 128 rows (column, k1)
+//            per MMA, N = 4 r', K = 4 r' bytes, SW32 / SW64 operands) against a
+//            small DFT-r' image; r' <= 4: radix 2 in registers.
 // Pass A stores transposed (ws[col N1 + d]) and pass B in natural order
 // (x[col + N1 d]): the CUDA-core tiles' layouts, so results are identical.
 // The data of a tile crosses shared memory twice (operand A, then the level-1
-// outputs W over it); the 64 KB image stays resident while consecutive tiles
-// use the same modulus and direction.
-constexpr uint32_t kTcA = 0;              // operand A: 128 rows x 256 B, SW128 (two K blocks), then W
+// outputs over it); each image stays resident while consecutive tiles use the
+// same modulus and direction.
+constexpr uint32_t kTcA = 0;              // operand A: 128 rows x 256 B, SW128 (two K blocks), then level 2's
 constexpr uint32_t kTcImg = 32768;        // DFT-64 image (64 KB)
-constexpr uint32_t kTcFac = 98304;        // level-2 factors [128] and butterfly twiddles [8]
-constexpr uint32_t kTcBar = kTcFac + 1024;  // mbarriers: [0] MMA commit, [1] image copy
+constexpr uint32_t kTcImg2 = 98304;       // DFT-16 (4 KB) or DFT-8 (1 KB) image
+constexpr uint32_t kTcFac = 102400;       // level-2 factors [128] and butterfly twiddles [8]
+constexpr uint32_t kTcBar = kTcFac + 1024;  // mbarriers: [0] MMA commits, [1] DFT-64 image, [2] DFT-r' image
 constexpr size_t kTcSmem = kTcBar + 64 + 1024;  // + alignment slack
+// Per-modulus image blob: DFT-64 forward / inverse / negacyclic forward
+// (64 KB each), DFT-16 forward / inverse / negacyclic inverse (4 KB each),
+// DFT-8 forward / inverse / negacyclic inverse (1 KB each).
 constexpr uint32_t kImgBytes = 65536;
+constexpr uint32_t kImg16Off = 3 * kImgBytes, kImg8Off = kImg16Off + 3 * 4096;
+constexpr uint32_t kImgPerMod = kImg8Off + 3 * 1024;
 
 struct TcState {
-    uint8_t* base;     // 1024-aligned dynamic shared memory
-    uint32_t taddr;    // 256 TMEM columns
-    uint32_t ph_mma, ph_img;
-    uint32_t img_key;  // image in shared memory: (modulus << 2 | variant) + 1, 0 none
+    uint8_t* base;      // 1024-aligned dynamic shared memory
+    uint32_t taddr;     // 256 TMEM columns
+    uint32_t ph_mma, ph_img, ph_img2;
+    uint32_t pend_img, pend_img2;  // an image copy in flight that no tile has waited for yet
+    uint32_t img_key;   // DFT-64 image in shared memory: (modulus << 2 | variant) + 1, 0 none
+    uint32_t img2_key;  // DFT-r' image: ((modulus << 2 | variant) << 1 | r' == 16) + 1, 0 none
 };
 
 __host__ __device__ constexpr uint32_t bitrev_c(uint32_t x, uint32_t bits) {
@@ -408,10 +421,10 @@ __device__ __forceinline__ void tc_wait(uint64_t* bar, uint32_t ph) {
     if (!tc::mbar_wait_bounded(bar, ph)) atomicOr(&g_batch_error, 2u);
 }
 
-// Level 2 of a tile: DFT-2^RL over b2 for each (column v, k1), canonical out.
-// Pass A threads walk k1 fastest (ws rows are contiguous in d); pass B threads
-// walk v fastest (x rows are contiguous in the column), with k1 spread so that
-// the W reads of a warp hit 32 distinct banks.
+// Level 2 on the CUDA cores (r' <= 4): DFT-2^RL over b2 for each (column v,
+// k1), canonical out.  Pass A threads walk k1 fastest (ws rows are contiguous
+// in d); pass B threads walk v fastest (x rows are contiguous in the column),
+// with k1 spread so that the W reads of a warp hit 32 distinct banks.
 template <uint32_t RL>
 __device__ __forceinline__ void tc_level2(const BUnit& u, uint32_t pass, uint32_t v0, uint32_t N1, const M32& ar,
                                           const uint32_t* W, const uint32_t* fac, bool use_fac) {
@@ -462,36 +475,129 @@ __device__ __forceinline__ void tc_level2(const BUnit& u, uint32_t pass, uint32_
     }
 }
 
+// Row of the level-2 operand holding (column v, k1): pass A rows run k1 within
+// a column (low three bits XOR v, so that the level-1 epilogue's stores of a
+// warp hit distinct banks), pass B rows run the columns within a k1.
+__device__ __forceinline__ uint32_t l2_row(uint32_t pass, uint32_t v, uint32_t k1, uint32_t lgV) {
+    return pass == 0 ? (v << 6) + (k1 ^ (v & 7u)) : (k1 << lgV) + v;
+}
+// Byte offset of (row, word b2) in the level-2 operand: SW64 (r' = 16,
+// 64-byte rows) or SW32 (r' = 8, 32-byte rows).
+__device__ __forceinline__ uint32_t l2_off(uint32_t row, uint32_t b2, uint32_t rl) {
+    return rl == 4 ? tc::sw64_offset(row, 4u * b2) : tc::sw32_offset(row, 4u * b2);
+}
+
+// Geometry of a tensor tile.
+struct TcGeo {
+    uint32_t L, n, shift, N1, lg, rl, rp, lgV, V, C, v0;
+    const uint32_t* src;
+    bool pre, mma2, inv, nega;
+    uint32_t variant, variant2, key, key2;
+};
+__device__ __forceinline__ TcGeo tc_geo(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile) {
+    TcGeo g;
+    g.L = u.log_n;
+    g.n = 1u << g.L;
+    g.shift = a.max_log - g.L;
+    g.inv = u.flags & UF_INV;
+    g.nega = u.flags & UF_NEGA;
+    g.N1 = 1u << u.lg1;
+    g.lg = pass == 0 ? u.lg1 : g.L - u.lg1;  // pass length 64 r'
+    g.rl = g.lg - 6;
+    g.rp = 1u << g.rl;
+    g.lgV = 7 - g.rl;
+    g.V = 1u << g.lgV;
+    g.C = pass == 0 ? g.n >> u.lg1 : g.N1;   // columns of the pass's matrix
+    g.v0 = tile << g.lgV;
+    g.src = pass == 0 ? u.data : u.ws;
+    g.pre = pass == 0 && u.pre_mul;
+    g.mma2 = g.rl >= 3;  // level 2 on the tensor cores
+    g.variant = g.inv ? 1u : (pass == 0 && g.nega ? 2u : 0u);
+    g.variant2 = g.inv ? (pass == 1 && g.nega ? 2u : 1u) : 0u;  // DFT-r' image
+    g.key = ((u.mod0 << 2) | g.variant) + 1u;
+    g.key2 = g.mma2 ? ((((u.mod0 << 2) | g.variant2) << 1) | (g.rl == 4 ? 1u : 0u)) + 1u : 0u;
+    return g;
+}
+
+// Image copies for a tile whose images differ from those in shared memory
+// (thread 0 issues; every thread tracks the keys and the pending copies,
+// which the MMA issuer waits for).
+__device__ __forceinline__ void tc_images(const BArgs& a, const BUnit& u, const TcGeo& g, TcState& st) {
+    uint64_t* bar = reinterpret_cast<uint64_t*>(st.base + kTcBar);
+    const uint8_t* blob = a.images + (size_t)u.mod0 * kImgPerMod;
+    if (g.key != st.img_key) {
+        if (threadIdx.x == 0) {
+            const uint8_t* img = blob + (size_t)g.variant * kImgBytes;
+            tc::mbar_expect_tx(bar + 1, kImgBytes);
+#pragma unroll
+            for (uint32_t k = 0; k < 4; k++)
+                tc::bulk_g2s(st.base + kTcImg + k * 16384u, img + k * 16384u, 16384u, bar + 1);
+        }
+        st.img_key = g.key;
+        st.pend_img = 1;
+    }
+    if (g.mma2 && g.key2 != st.img2_key) {
+        if (threadIdx.x == 0) {
+            const uint32_t bytes = g.rl == 4 ? 4096u : 1024u;
+            const uint8_t* img = blob + (g.rl == 4 ? kImg16Off : kImg8Off) + g.variant2 * bytes;
+            tc::mbar_expect_tx(bar + 2, bytes);
+            tc::bulk_g2s(st.base + kTcImg2, img, bytes, bar + 2);
+        }
+        st.img2_key = g.key2;
+        st.pend_img2 = 1;
+    }
+}
+
+// Operand A: row m = (b2, v) = b2 V + v holds column v0 + v's elements
+// j = r' a2 + b2 in K order a2; thread (m, hh) fills 16-byte chunks hh,
+// hh + 2, ..  A product's inverse multiplies by the pointwise operand on the way.
+__device__ __forceinline__ void tc_operand(const BUnit& u, const TcGeo& g, const M32& ar, uint8_t* A) {
+    const uint32_t mm = threadIdx.x & 127u, hh = threadIdx.x >> 7;
+    const size_t off0 = (size_t)(mm >> g.lgV) * g.C + g.v0 + (mm & (g.V - 1u));
+    const size_t step = (size_t)g.rp * g.C;  // between consecutive a2
+    uint32_t xs[32];
+#pragma unroll
+    for (uint32_t j = 0; j < 8; j++)
+#pragma unroll
+        for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcg(g.src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
+    if (g.pre) {
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++)
+#pragma unroll
+            for (uint32_t t = 0; t < 4; t++)
+                xs[4 * j + t] = ar.mul(xs[4 * j + t], __ldcg(u.pre_mul + off0 + (size_t)(8u * j + 4u * hh + t) * step));
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 8; j++)
+        *reinterpret_cast<uint4*>(A + tc::sw128_offset(mm, 16u * (2u * j + hh), 128)) =
+            make_uint4(xs[4 * j], xs[4 * j + 1], xs[4 * j + 2], xs[4 * j + 3]);
+}
+
+// Publishes a tile's completion (thread 0, after a CTA barrier that followed
+// the tile's stores): release at gpu scope, cumulative over the CTA's stores.
+__device__ __forceinline__ void signal_done(uint32_t* counter) {
+    __threadfence();
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
+}
+
 __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile, TcState& st) {
     const uint32_t tid = threadIdx.x;
-    const uint32_t L = u.log_n, n = 1u << L, shift = a.max_log - L;
-    const bool inv = u.flags & UF_INV, nega = u.flags & UF_NEGA;
-    const uint32_t N1 = 1u << u.lg1;
-    const uint32_t lg = pass == 0 ? u.lg1 : L - u.lg1;  // pass length 64 r'
-    const uint32_t rl = lg - 6, rp = 1u << rl;
-    const uint32_t lgV = 7 - rl, V = 1u << lgV;
-    const uint32_t C = pass == 0 ? n >> u.lg1 : N1;     // columns of the pass's matrix
-    const uint32_t v0 = tile << lgV;
-    const uint32_t* src = pass == 0 ? u.data : u.ws;
-    const bool pre = pass == 0 && u.pre_mul;
+    const TcGeo g = tc_geo(a, u, pass, tile);
+    const uint32_t L = g.L, n = g.n, shift = g.shift, N1 = g.N1, lg = g.lg, rl = g.rl, rp = g.rp, lgV = g.lgV;
+    const uint32_t V = g.V, C = g.C, v0 = g.v0;
+    const bool inv = g.inv, nega = g.nega, pre = g.pre, mma2 = g.mma2;
     const BModulus& M = a.mods[u.mod0];
     const M32 ar = M.ar;
     const uint32_t q = ar.q, qinv = ar.qinv;
     const uint32_t wb = inv ? PW_OMEGA_INV : PW_OMEGA;
-    const uint32_t variant = inv ? 1u : (pass == 0 && nega ? 2u : 0u);
-    const uint32_t key = ((u.mod0 << 2) | variant) + 1u;
-    const bool new_img = key != st.img_key;
     uint8_t* base = st.base;
     uint64_t* bar = reinterpret_cast<uint64_t*>(base + kTcBar);
-    if (new_img && tid == 0) {
-        const uint8_t* img = a.images + ((size_t)u.mod0 * 3 + variant) * kImgBytes;
-        tc::mbar_expect_tx(bar + 1, kImgBytes);
-#pragma unroll
-        for (uint32_t k = 0; k < 4; k++) tc::bulk_g2s(base + kTcImg + k * 16384u, img + k * 16384u, 16384u, bar + 1);
-    }
-    // level-2 constants: factors, then the DFT-r' butterfly twiddles omega_r'^j
+    tc_images(a, u, g, st);
+    // level-2 constants: factors, then (CUDA-core level 2) the DFT-r'
+    // butterfly twiddles omega_r'^j.  Pass B's negacyclic factors sit in the
+    // DFT-r' image when level 2 runs on the tensor cores.
     uint32_t* fac = reinterpret_cast<uint32_t*>(base + kTcFac);
-    const bool use_fac = rp > 1 && (pass == 0 || (inv && nega));
+    const bool use_fac = rp > 1 && (pass == 0 || (inv && nega && !mma2));
     if (use_fac) {
         if (pass == 0) {
             if (tid < 128) {
@@ -502,46 +608,24 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
             fac[tid] = pw(M, ar, PW_PSI_INV, (64u * N1 * tid) << shift);
         }
     }
-    if (tid >= 128 && tid < 128 + rp / 2) fac[tid] = pw(M, ar, wb, (((n >> rl) * (tid - 128)) & (n - 1u)) << shift);
-    // operand A: row m = (b2, v) = b2 V + v holds column v0 + v's elements
-    // j = r' a2 + b2 in K order a2; thread (m, hh) loads 16-byte chunks hh, hh + 2, ..
-    {
-        const uint32_t mm = tid & 127u, hh = tid >> 7;
-        const size_t off0 = (size_t)(mm >> lgV) * C + v0 + (mm & (V - 1u));
-        const size_t step = (size_t)rp * C;  // between consecutive a2
-        uint32_t xs[32];
-#pragma unroll
-        for (uint32_t j = 0; j < 8; j++)
-#pragma unroll
-            for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcg(src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
-        if (pre) {
-#pragma unroll
-            for (uint32_t j = 0; j < 8; j++)
-#pragma unroll
-                for (uint32_t t = 0; t < 4; t++)
-                    xs[4 * j + t] = ar.mul(xs[4 * j + t], __ldcg(u.pre_mul + off0 + (size_t)(8u * j + 4u * hh + t) * step));
-        }
-        uint8_t* A = base + kTcA;
-#pragma unroll
-        for (uint32_t j = 0; j < 8; j++)
-            *reinterpret_cast<uint4*>(A + tc::sw128_offset(mm, 16u * (2u * j + hh), 128)) =
-                make_uint4(xs[4 * j], xs[4 * j + 1], xs[4 * j + 2], xs[4 * j + 3]);
-    }
+    if (!mma2 && tid >= 128 && tid < 128 + rp / 2)
+        fac[tid] = pw(M, ar, wb, (((n >> rl) * (tid - 128)) & (n - 1u)) << shift);
+    tc_operand(u, g, ar, base + kTcA);
     tc::fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
-        if (new_img) tc_wait(bar + 1, st.ph_img);
+        if (st.pend_img) tc_wait(bar + 1, st.ph_img);
         tc::fence_after_sync();
         tca::issue_k256(st.taddr, tc::smem_u32(base + kTcA), 128, tc::smem_u32(base + kTcImg), 256, 256);
         tc::commit(bar);
     }
-    if (new_img) {
+    if (st.pend_img) {
         st.ph_img ^= 1u;
-        st.img_key = key;
+        st.pend_img = 0;
     }
     // level-1 twiddles of this thread's vector: base * ratio^k1 for k1 = 32 h ..
     const uint32_t wq = tid >> 5, quarter = wq & 3u, h = wq >> 2, lane = tid & 31u;
-    const uint32_t m = quarter * 32u + lane, b2 = m >> lgV, col = v0 + (m & (V - 1u));
+    const uint32_t m = quarter * 32u + lane, b2 = m >> lgV, vv = m & (V - 1u), col = v0 + vv;
     const uint32_t er = (n >> lg) * b2 + (pass == 0 ? col : 0u);  // < n
     uint32_t ratio = pw(M, ar, wb, er << shift);
     uint32_t start = pw(M, ar, wb, ((er * 32u * h) & (n - 1u)) << shift);
@@ -558,37 +642,120 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
     tc_wait(bar, st.ph_mma);
     st.ph_mma ^= 1u;
     tc::fence_after_sync();
-    // level-1 epilogue: W[m][k1] at m * 64 + (k1 & 32) + ((k1 ^ m) & 31), in [0, 2q)
+    // level-1 epilogue, values in [0, 2q): the level-2 operand (row (v, k1),
+    // word b2) when level 2 runs on the tensor cores, else W[m][k1] at
+    // m * 64 + (k1 & 32) + ((k1 ^ m) & 31)
     {
         const uint32_t r2 = tca::canon(tca::mont_lazy(ratio, ratio, q, qinv), q);
         uint32_t tw_e = start;
         uint32_t tw_o = tca::canon(tca::mont_lazy(start, ratio, q, qinv), q);
         const uint32_t tcol = st.taddr + h * 128u + ((quarter * 32u) << 16);
         uint32_t* Wrow = reinterpret_cast<uint32_t*>(base + kTcA) + m * 64u + 32u * h;
+        uint8_t* A2 = base + kTcA;
 #pragma unroll 1
         for (uint32_t part = 0; part < 4; part++) {
             uint32_t c0[8], c1[8], c2[8], c3[8];
             tca::ld_planes8(tcol + 8u * part, c0, c1, c2, c3);
+            uint32_t y[8];
 #pragma unroll
             for (uint32_t i = 0; i < 8; i += 2) {
-                const uint32_t k = 8u * part + i;
-                Wrow[k ^ lane] = tca::mont_lazy(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
-                Wrow[(k + 1u) ^ lane] =
+                y[i] = tca::mont_lazy(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
+                y[i + 1] =
                     tca::mont_lazy(tca::combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
                 tw_e = tca::canon(tca::mont_lazy(tw_e, r2, q, qinv), q);
                 tw_o = tca::canon(tca::mont_lazy(tw_o, r2, q, qinv), q);
             }
+            if (mma2) {
+#pragma unroll
+                for (uint32_t i = 0; i < 8; i++) {
+                    const uint32_t k1 = 32u * h + 8u * part + i;
+                    *reinterpret_cast<uint32_t*>(A2 + l2_off(l2_row(pass, vv, k1, lgV), b2, rl)) = y[i];
+                }
+            } else {
+#pragma unroll
+                for (uint32_t i = 0; i < 8; i++) Wrow[(8u * part + i) ^ lane] = y[i];
+            }
         }
     }
+    if (!mma2) {
+        tc::fence_before_sync();
+        __syncthreads();
+        const uint32_t* W = reinterpret_cast<const uint32_t*>(base + kTcA);
+        switch (rl) {
+            case 0: tc_level2<0>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+            case 1: tc_level2<1>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+            default: tc_level2<2>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+        }
+        return;
+    }
+    // level 2 on the tensor cores: M-tile t = rows 128 t .. into TMEM columns
+    // t * 4 r' + a r' + k2 (the level-1 accumulators are all read by now)
+    const uint32_t n_mt = 64u >> rl;  // 4 (r' = 16) or 8 (r' = 8) M-tiles of 128 rows
+    tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
-    const uint32_t* W = reinterpret_cast<const uint32_t*>(base + kTcA);
-    switch (rl) {
-        case 0: tc_level2<0>(u, pass, v0, N1, ar, W, fac, use_fac); break;
-        case 1: tc_level2<1>(u, pass, v0, N1, ar, W, fac, use_fac); break;
-        case 2: tc_level2<2>(u, pass, v0, N1, ar, W, fac, use_fac); break;
-        case 3: tc_level2<3>(u, pass, v0, N1, ar, W, fac, use_fac); break;
-        default: tc_level2<4>(u, pass, v0, N1, ar, W, fac, use_fac); break;
+    if (tid == 0) {
+        if (st.pend_img2) tc_wait(bar + 2, st.ph_img2);
+        tc::fence_after_sync();
+        const uint32_t a2 = tc::smem_u32(base + kTcA), bi = tc::smem_u32(base + kTcImg2);
+        const uint32_t idesc = tc::idesc_u8(128, 4u << rl);
+        for (uint32_t t = 0; t < n_mt; t++) {
+            if (rl == 4) {
+                tc::mma_i8(st.taddr + t * 64u, tc::desc_k_sw64(a2 + t * 8192u), tc::desc_k_sw64(bi), idesc, 0);
+                tc::mma_i8(st.taddr + t * 64u, tc::desc_k_sw64(a2 + t * 8192u + 32u), tc::desc_k_sw64(bi + 32u), idesc, 1);
+            } else {
+                tc::mma_i8(st.taddr + t * 32u, tc::desc_k_sw32(a2 + t * 4096u), tc::desc_k_sw32(bi), idesc, 0);
+            }
+        }
+        tc::commit(bar);
+    }
+    if (st.pend_img2) {
+        st.ph_img2 ^= 1u;
+        st.pend_img2 = 0;
+    }
+    __syncwarp();
+    tc_wait(bar, st.ph_mma);
+    st.ph_mma ^= 1u;
+    tc::fence_after_sync();
+    // level-2 epilogue: thread (quarter, h) reads lane 32 quarter + lane of the
+    // M-tiles h, h + 2, ..; 8 outputs k2 at a time (planes r' columns apart)
+#pragma unroll 1
+    for (uint32_t t = h; t < n_mt; t += 2) {
+        const uint32_t row = 128u * t + 32u * quarter + lane;
+        uint32_t v, k1;
+        if (pass == 0) {
+            v = row >> 6;
+            k1 = (row & 63u) ^ (v & 7u);
+        } else {
+            v = row & (V - 1u);
+            k1 = row >> lgV;
+        }
+        const uint32_t tc0 = st.taddr + t * (4u << rl) + ((quarter * 32u) << 16);
+#pragma unroll 1
+        for (uint32_t gq = 0; gq < rp / 8; gq++) {
+            uint32_t c0[8], c1[8], c2[8], c3[8];
+            tc::ld_32x32b_x8(tc0 + 8u * gq, c0);
+            tc::ld_32x32b_x8(tc0 + rp + 8u * gq, c1);
+            tc::ld_32x32b_x8(tc0 + 2u * rp + 8u * gq, c2);
+            tc::ld_32x32b_x8(tc0 + 3u * rp + 8u * gq, c3);
+            tc::ld_wait();
+            if (pass == 0) {
+                uint32_t* o = u.ws + (size_t)(v0 + v) * N1 + k1;
+#pragma unroll
+                for (uint32_t i = 0; i < 8; i++) {
+                    const uint32_t k2 = 8u * gq + i;
+                    const uint32_t y = tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
+                    o[64u * k2] = tca::canon(tca::mont_lazy(y, fac[v * rp + k2], q, qinv), q);
+                }
+            } else {
+                uint32_t* o = u.data + (size_t)k1 * N1 + v0 + v;
+#pragma unroll
+                for (uint32_t i = 0; i < 8; i++) {
+                    const uint32_t k2 = 8u * gq + i;
+                    o[(size_t)64u * k2 * N1] = tca::canon(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), q);
+                }
+            }
+        }
     }
 }
 
@@ -605,14 +772,16 @@ __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__
     if (threadIdx.x == 0) {
         tc::mbar_init(bar, 1);
         tc::mbar_init(bar + 1, 1);
+        tc::mbar_init(bar + 2, 1);
     }
     if (threadIdx.x < 32) tc::tmem_alloc(&s_taddr, 256);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     st.taddr = s_taddr;
-    st.ph_mma = st.ph_img = 0;
-    st.img_key = 0;
+    st.ph_mma = st.ph_img = st.ph_img2 = 0;
+    st.img_key = st.img2_key = 0;
+    st.pend_img = st.pend_img2 = 0;
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ctr, 1u);
         __syncthreads();
@@ -621,23 +790,18 @@ __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__
         const BTile tl = a.tiles[ticket];
         const BUnit u = a.units[tl.unit];
         const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
-        if (threadIdx.x == 0) {
-            if (!wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
-            __threadfence();
-        }
+        if (threadIdx.x == 0 && !wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
         __syncthreads();
         if (u.flags & UF_TC) {
             run_tc_tile(a, u, pass, tile, st);
         } else {
             run_tile<256, G>(a, u, pass, tile, reinterpret_cast<uint32_t*>(st.base), s_ar);
-            st.img_key = 0;  // the tile overwrote the image
+            st.img_key = st.img2_key = 0;  // the tile overwrote the images
         }
-        __threadfence();
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();
-        if (threadIdx.x == 0)
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.ctr + 1 + 2 * tl.unit + pass) : "memory");
+        if (threadIdx.x == 0) signal_done(a.ctr + 1 + 2 * tl.unit + pass);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -658,16 +822,11 @@ __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T
         const BTile tl = a.tiles[ticket];
         const BUnit u = a.units[tl.unit];
         const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
-        if (threadIdx.x == 0) {
-            if (!wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
-            __threadfence();
-        }
+        if (threadIdx.x == 0 && !wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
         __syncthreads();
         run_tile<T, G>(a, u, pass, tile, sm, s_ar);
-        __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0)
-            asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.ctr + 1 + 2 * tl.unit + pass) : "memory");
+        if (threadIdx.x == 0) signal_done(a.ctr + 1 + 2 * tl.unit + pass);
     }
 }
 
@@ -698,6 +857,18 @@ const Variant* find_variant(uint32_t E, uint32_t T, uint32_t G, uint32_t tensor)
 // padded tile (E + E/32 + one word per vector) + root powers + slack, in bytes
 size_t smem_bytes(uint32_t E) { return ((size_t)E + E / 16 + kMaxRows + E / 2) * 4 + 64; }
 size_t smem_bytes(const Variant* v) { return v->tensor ? kTcSmem : smem_bytes(v->E); }
+
+// Byte-plane image of an 8 x 8 matrix for the level-2 contraction: 32 rows
+// (a, k) x 32 bytes (j, p), K-major SW32 (1 KB).
+void build_image8(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) {
+    std::memset(img, 0, 1024);
+    for (uint32_t c = 0; c < 8; c++)
+        for (uint32_t b = 0; b < 8; b++)
+            for (uint32_t p = 0; p < 4; p++) {
+                const uint64_t v = h_mulmod(h_to_mont32(W[c * 8 + b], q), (1ull << (8 * p)) % q, q);
+                for (uint32_t a = 0; a < 4; a++) img[tc::sw32_offset(a * 8 + c, 4 * b + p)] = (uint8_t)(v >> (8 * a));
+            }
+}
 
 // CTAs of a variant resident on the whole device (the persistent grid): the
 // kernel asks for the largest shared-memory carveout, so that the tensor-tile
@@ -979,12 +1150,20 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
         }
         const uint32_t ui = (uint32_t)units.size();
         BUnit u = p.u;
-        for (int d = 0; d < 2; d++) u.after[d] = p.after_id[d] >= 0 ? index_of[p.after_id[d]] : -1;
+        for (int d = 0; d < 2; d++) {
+            u.after[d] = p.after_id[d] >= 0 ? index_of[p.after_id[d]] : -1;
+            if (u.after[d] >= 0) {  // complete = its last pass has signalled every tile
+                const BUnit& W = units[u.after[d]];
+                u.after_ctr[d] = (W.lg1 ? 2u : 1u) + 2u * (uint32_t)u.after[d];
+                u.need[1 + d] = W.lg1 ? W.tiles_b : W.tiles_a;
+            }
+        }
         if (u.lg1) {
             const uint32_t L = u.log_n, slot = next_slot[L]++ % lay.slots[L];
             // word offset, rebased on the workspace allocation later
             u.ws = reinterpret_cast<uint32_t*>((uintptr_t)((lay.base[L] + ((uint64_t)slot << L)) * 4u));
             u.prev = slot_owner[L][slot];
+            if (u.prev >= 0) u.need[0] = units[u.prev].tiles_b;
             slot_owner[L][slot] = (int32_t)ui;
         }
         units.push_back(u);
@@ -1183,7 +1362,7 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
 size_t batch_plan_device_bytes(const BatchPlan* P) {
     const uint32_t lo = std::min<uint32_t>(kLoBits, P->max_log);
     return (size_t)P->limbs.size() * 4 * 4 * (((size_t)1 << (P->max_log - lo)) + ((size_t)1 << lo)) +
-           P->limbs.size() * sizeof(BModulus) + (P->images ? P->limbs.size() * 3 * (size_t)kImgBytes : 0);
+           P->limbs.size() * sizeof(BModulus) + (P->images ? P->limbs.size() * (size_t)kImgPerMod : 0);
 }
 
 uint32_t batch_device_errors(bool clear) {
@@ -1283,7 +1462,7 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
     if (max_log_n >= 13) {
         // DFT-64 images per modulus: forward (omega_64), inverse, and the
         // negacyclic forward with psi_128^j on the input index
-        const size_t per = 3 * (size_t)nttb::kImgBytes;
+        const size_t per = nttb::kImgPerMod;
         std::vector<uint8_t> img(per * n_moduli, 0);
         for (uint32_t l = 0; l < n_moduli; l++) {
             const nttb::LimbHost& H = P.limbs[l];
@@ -1295,6 +1474,17 @@ NTTB_API int nttb_batch_plan_create(const uint64_t* moduli, uint32_t n_moduli, u
             if (nega)
                 nttb::tc_build_image64(d + 2 * nttb::kImgBytes,
                                        nttb::tc_dft_matrix(64, w64, q, 1, nttb::h_powmod(H.psi, N / 64, q)), q);
+            // DFT-16 and DFT-8 of level 2: forward, inverse, and the negacyclic
+            // inverse with psi_max^-(2^max_log k2 / r') on output k2
+            for (uint32_t r : {16u, 8u}) {
+                const uint64_t w = nttb::h_powmod(H.omega, N / r, q), wi = nttb::h_powmod(H.omega_inv, N / r, q);
+                uint8_t* o = d + (r == 16 ? nttb::kImg16Off : nttb::kImg8Off);
+                const uint32_t bytes = r == 16 ? 4096 : 1024;
+                auto build = r == 16 ? nttb::tc_build_image16 : nttb::build_image8;
+                build(o, nttb::tc_dft_matrix(r, w, q), q);
+                build(o + bytes, nttb::tc_dft_matrix(r, wi, q), q);
+                if (nega) build(o + 2 * bytes, nttb::tc_dft_matrix(r, wi, q, nttb::h_powmod(H.psi_inv, N / r, q)), q);
+            }
         }
         uint8_t* d = nullptr;
         if (cudaMalloc(&d, img.size()) != cudaSuccess ||
@@ -1445,7 +1635,7 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
     // {tile, threads, tensor}
     const uint32_t shapes[6][3] = {{4096, 256, 0}, {8192, 256, 0}, {8192, 512, 0}, {16384, 512, 0},
                                    {4096, 256, 1}, {8192, 256, 1}};
-    const uint32_t lags[2] = {1, 4}, groups[3] = {1, 3, 4};
+    const uint32_t lags[3] = {1, 4, 8}, groups[3] = {1, 3, 4};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

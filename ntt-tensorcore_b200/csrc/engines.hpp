@@ -27,6 +27,8 @@ int fail(int code, const char* fmt, ...);
 // in two 128-byte K blocks (64 KB).  tc_dft_matrix(L, root, ...) returns
 // W[k][j] = scale * row_twist^k * col_twist^j * root^(j k).
 void tc_build_image64(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q);
+// Byte-plane image of a 16 x 16 matrix: 64 rows (a, k) x 64 bytes, K-major SW64 (4 KB).
+void tc_build_image16(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q);
 std::vector<uint64_t> tc_dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t row_twist = 1,
                                     uint64_t col_twist = 1, uint64_t scale = 1);
 

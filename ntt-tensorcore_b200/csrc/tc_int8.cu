@@ -732,6 +732,7 @@ int launch_stages(Int8Cache* c, ClArgs& a, cudaStream_t s) {
 
 // DFT-64 byte-plane images for other kernels (the batch engine's tensor tiles).
 void tc_build_image64(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) { build_image64(img, W, q); }
+void tc_build_image16(uint8_t* img, const std::vector<uint64_t>& W, uint64_t q) { build_image16(img, W, q); }
 std::vector<uint64_t> tc_dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t row_twist, uint64_t col_twist,
                                     uint64_t scale) {
     return dft_matrix(L, root, q, row_twist, col_twist, scale);

@@ -161,6 +161,16 @@ __device__ __forceinline__ uint64_t desc_k_sw64(uint32_t addr) {
     d |= (uint64_t)4u << 61;                          // SWIZZLE_64B
     return d;
 }
+// K-major operand with 32-byte swizzle: 8-row x 32-byte atoms, SBO = 256 B.
+__device__ __forceinline__ uint64_t desc_k_sw32(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;
+    d |= (uint64_t)(256u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)6u << 61;                          // SWIZZLE_32B
+    return d;
+}
 // Instruction descriptor, kind::i8: u8 x u8 -> s32, both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_u8(uint32_t M, uint32_t N) {
     return (2u << 4)            // D format S32
@@ -204,6 +214,12 @@ __host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t row, uint32_t
     const uint32_t blk = kbyte >> 7, kb = kbyte & 127u;
     const uint32_t chunk = (kb >> 4) ^ (row & 7u);
     return blk * rows * 128u + (row >> 3) * 1024u + (row & 7u) * 128u + (chunk << 4) + (kb & 15u);
+}
+// Byte offset of (row, kbyte < 32) inside a K-major SW32 tile (16-byte chunk
+// index XOR bit 2 of the row).
+__host__ __device__ __forceinline__ uint32_t sw32_offset(uint32_t row, uint32_t kbyte) {
+    const uint32_t chunk = ((kbyte >> 4) & 1u) ^ ((row >> 2) & 1u);
+    return (row >> 3) * 256u + (row & 7u) * 32u + (chunk << 4) + (kbyte & 15u);
 }
 // Byte offset of (row, kbyte < 64) inside a K-major SW64 tile.
 __host__ __device__ __forceinline__ uint32_t sw64_offset(uint32_t row, uint32_t kbyte) {
