@@ -137,6 +137,17 @@ NTTB_API int nttb_rns_transform(const nttb_rns_plan* plan, uint32_t* d_dst, cons
  * per-(poly, limb) stage dependencies; other engines run two transforms. */
 NTTB_API int nttb_rns_forward_inverse(const nttb_rns_plan* plan, uint32_t* d_data, uint32_t n_polys, int engine,
                                       void* stream);
+/* Streams n_batches consecutive batches of n_polys polynomials from host
+ * memory h_src to h_dst (batch i at offset i * n_polys * n_limbs * n words):
+ * copy in, transform (mode 0 forward, 1 inverse, 2 forward then inverse),
+ * copy out, with the copies of neighbouring batches overlapping the
+ * transforms (three device buffers owned by the plan, two copy streams per
+ * direction).  Asynchronous: `stream` completes after the last copy back;
+ * h_src and h_dst must stay valid until then, and should be pinned
+ * (cudaHostAlloc / cudaHostRegister) for the copies to overlap.  No reference
+ * counterpart (the reference API takes device pointers only). */
+NTTB_API int nttb_rns_stream_host(nttb_rns_plan* plan, const uint32_t* h_src, uint32_t* h_dst, uint32_t n_polys,
+                                  uint32_t n_batches, int mode, int engine, void* stream);
 /* In-place transform that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc while transforming (a
  * memory manager that owns all device memory, a loop that must never enter

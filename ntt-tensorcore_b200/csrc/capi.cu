@@ -3,6 +3,8 @@
 // the engines; no arithmetic lives here beyond the small elementwise kernels.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -120,9 +122,47 @@ struct nttb_plan {
     uint64_t r2_64 = 0;
 };
 
+namespace nttb {
+// Streaming of host-resident batches through one RNS plan
+// (nttb_rns_stream_host): three device buffers in rotation, each batch's
+// copies split in two chunks on two copy streams per direction, so that the
+// host -> device copy of one batch, the transform of the previous one and the
+// device -> host copy of the one before overlap.  Events order every reuse.
+struct HostStream {
+    size_t words = 0;  // capacity of each buffer
+    uint32_t* dbuf[3] = {};
+    cudaStream_t in[2] = {}, out[2] = {};
+    cudaEvent_t start = nullptr, ev_in[3][2] = {}, ev_c[3] = {}, done[3][2] = {};
+    bool used[3] = {};
+    uint32_t next = 0;  // buffer of the next batch: the rotation continues across calls
+};
+void host_stream_free(HostStream* h) {
+    if (!h) return;
+    for (int c = 0; c < 2; c++) {
+        if (h->in[c]) cudaStreamSynchronize(h->in[c]);
+        if (h->out[c]) cudaStreamSynchronize(h->out[c]);
+    }
+    for (int k = 0; k < 3; k++) {
+        if (h->dbuf[k]) cudaFree(h->dbuf[k]);
+        if (h->ev_c[k]) cudaEventDestroy(h->ev_c[k]);
+        for (int c = 0; c < 2; c++) {
+            if (h->ev_in[k][c]) cudaEventDestroy(h->ev_in[k][c]);
+            if (h->done[k][c]) cudaEventDestroy(h->done[k][c]);
+        }
+    }
+    for (int c = 0; c < 2; c++) {
+        if (h->in[c]) cudaStreamDestroy(h->in[c]);
+        if (h->out[c]) cudaStreamDestroy(h->out[c]);
+    }
+    if (h->start) cudaEventDestroy(h->start);
+    delete h;
+}
+}  // namespace nttb
+
 struct nttb_rns_plan {
     Plan32 p;
     uint32_t* d_r2 = nullptr;  // R^2 mod q per limb (pointwise products)
+    nttb::HostStream* hs = nullptr;
 };
 
 struct nttb_wide_plan {
@@ -409,6 +449,7 @@ int nttb_rns_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_limb
 
 int nttb_rns_plan_destroy(nttb_rns_plan* P) {
     if (!P) return NTTB_OK;
+    nttb::host_stream_free(P->hs);
     engines_release32(&P->p);
     free_plan32(&P->p);
     if (P->d_r2) cudaFree(P->d_r2);
@@ -443,6 +484,83 @@ int nttb_rns_forward_inverse(const nttb_rns_plan* P, uint32_t* d, uint32_t n_pol
     }
     if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_forward_inverse: shape not served by the requested engine");
     return cuda_status("rns_forward_inverse");
+}
+
+int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_dst, uint32_t n_polys, uint32_t n_batches,
+                         int mode, int engine, void* stream) {
+    if (!P || !h_src || !h_dst) return fail(NTTB_ERR_INVALID_ARG, "rns_stream_host: null argument");
+    if (mode < 0 || mode > 2) return fail(NTTB_ERR_INVALID_ARG, "rns_stream_host: mode must be 0, 1 or 2");
+    if (n_polys == 0 || n_batches == 0) return NTTB_OK;
+    Plan32& p = P->p;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bw = (size_t)n_polys * p.n_limbs * p.n;
+    const int eng = engine == NTTB_ENGINE_AUTO ? auto_engine32(p, false) : engine;
+    nttb::HostStream*& H = P->hs;
+    if (!H || H->words < bw) {  // (re)build the buffers, streams and events
+        nttb::host_stream_free(H);
+        H = new nttb::HostStream();
+        bool ok = true;
+        for (int k = 0; k < 3 && ok; k++) {
+            ok = cudaMalloc(&H->dbuf[k], bw * 4) == cudaSuccess;
+            ok = ok && cudaEventCreateWithFlags(&H->ev_c[k], cudaEventDisableTiming) == cudaSuccess;
+            for (int c = 0; c < 2 && ok; c++) {
+                ok = cudaEventCreateWithFlags(&H->ev_in[k][c], cudaEventDisableTiming) == cudaSuccess;
+                ok = ok && cudaEventCreateWithFlags(&H->done[k][c], cudaEventDisableTiming) == cudaSuccess;
+            }
+        }
+        for (int c = 0; c < 2 && ok; c++) {
+            ok = cudaStreamCreateWithFlags(&H->in[c], cudaStreamNonBlocking) == cudaSuccess;
+            ok = ok && cudaStreamCreateWithFlags(&H->out[c], cudaStreamNonBlocking) == cudaSuccess;
+        }
+        ok = ok && cudaEventCreateWithFlags(&H->start, cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            nttb::host_stream_free(H);
+            H = nullptr;
+            return fail(NTTB_ERR_NO_MEMORY, "rns_stream_host: buffers");
+        }
+        H->words = bw;
+    }
+    // everything after the caller's earlier work on `stream`
+    cudaEventRecord(H->start, s);
+    for (int c = 0; c < 2; c++) {
+        cudaStreamWaitEvent(H->in[c], H->start, 0);
+        cudaStreamWaitEvent(H->out[c], H->start, 0);
+    }
+    const size_t half = (bw / 2 + 63) & ~(size_t)63;  // chunk of a batch, 256-byte aligned
+    for (uint32_t i = 0; i < n_batches; i++) {
+        const int k = (int)(H->next++ % 3);
+        for (int c = 0; c < 2; c++) {
+            const size_t off = c ? half : 0, len = c ? (bw > half ? bw - half : 0) : std::min(half, bw);
+            if (H->used[k]) cudaStreamWaitEvent(H->in[c], H->done[k][c], 0);
+            if (len) cudaMemcpyAsync(H->dbuf[k] + off, h_src + i * bw + off, len * 4, cudaMemcpyHostToDevice, H->in[c]);
+            cudaEventRecord(H->ev_in[k][c], H->in[c]);
+            cudaStreamWaitEvent(s, H->ev_in[k][c], 0);
+        }
+        int rc = 0;
+        if (mode == 2) {
+            rc = eng == NTTB_ENGINE_INT8 ? int8_forward_inverse32(p, H->dbuf[k], n_polys, s)
+                                         : run_transform32(p, H->dbuf[k], H->dbuf[k], false, n_polys, false, eng, s);
+            if (!rc && eng != NTTB_ENGINE_INT8)
+                rc = run_transform32(p, H->dbuf[k], H->dbuf[k], false, n_polys, true, eng, s);
+        } else {
+            rc = run_transform32(p, H->dbuf[k], H->dbuf[k], false, n_polys, mode == 1, eng, s);
+        }
+        if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_stream_host: shape not served by the requested engine");
+        if (rc) return fail(NTTB_ERR_CUDA, "rns_stream_host: launch failed");
+        cudaEventRecord(H->ev_c[k], s);
+        for (int c = 0; c < 2; c++) {
+            const size_t off = c ? half : 0, len = c ? (bw > half ? bw - half : 0) : std::min(half, bw);
+            cudaStreamWaitEvent(H->out[c], H->ev_c[k], 0);
+            if (len) cudaMemcpyAsync(h_dst + i * bw + off, H->dbuf[k] + off, len * 4, cudaMemcpyDeviceToHost, H->out[c]);
+            cudaEventRecord(H->done[k][c], H->out[c]);
+        }
+        H->used[k] = true;
+    }
+    // the caller's stream completes after the last copy back
+    for (int k = 0; k < 3; k++)
+        if (H->used[k])
+            for (int c = 0; c < 2; c++) cudaStreamWaitEvent(s, H->done[k][c], 0);
+    return cuda_status("rns_stream_host");
 }
 
 int nttb_rns_pointwise_mul(const nttb_rns_plan* P, uint32_t* out, const uint32_t* a, const uint32_t* b,

@@ -114,6 +114,7 @@ def lib():
         "nttb_rns_pointwise_mul": (_int, [_vp, _vp, _vp, _vp, _u32, _vp]),
         "nttb_rns_transform_noalloc": (_int, [_vp, _vp, _u32, _int, _vp]),
         "nttb_rns_forward_inverse": (_int, [_vp, _vp, _u32, _int, _vp]),
+        "nttb_rns_stream_host": (_int, [_vp, _vp, _vp, _u32, _u32, _int, _int, _vp]),
         "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
@@ -163,7 +164,9 @@ def _ptr(x):
         return None
     if isinstance(x, int):
         return x
-    return x.data_ptr()  # torch tensor
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()  # torch tensor
+    return x.ctypes.data  # numpy array
 
 
 def _stream(stream):
@@ -491,6 +494,15 @@ class RnsPlan:
     def forward_inverse(self, data, n_polys, engine="auto", stream=None):
         """Forward then inverse in place (one persistent launch on the INT8 engine)."""
         _check(lib().nttb_rns_forward_inverse(self._h, _ptr(data), n_polys, _engine(engine), _stream(stream)))
+
+    def stream_host(self, h_src, h_dst, n_polys, n_batches, mode="forward_inverse", engine="auto", stream=None):
+        """Host-resident batches through the GPU (nttb_rns_stream_host): h_src,
+        h_dst are pinned CPU tensors or numpy arrays of n_batches * n_polys *
+        n_limbs * n words; mode "forward", "inverse" or "forward_inverse".
+        Asynchronous on `stream`."""
+        m = {"forward": 0, "inverse": 1, "forward_inverse": 2}[mode]
+        _check(lib().nttb_rns_stream_host(self._h, _ptr(h_src), _ptr(h_dst), n_polys, n_batches, m, _engine(engine),
+                                          _stream(stream)))
 
     def transform_noalloc(self, data, n_polys, inverse=False, stream=None):
         """In-place transform that allocates no device memory (static scratch;
