@@ -486,6 +486,28 @@ __device__ __forceinline__ uint32_t l2_row(uint32_t pass, uint32_t v, uint32_t k
 __device__ __forceinline__ uint32_t l2_off(uint32_t row, uint32_t b2, uint32_t rl) {
     return rl == 4 ? tc::sw64_offset(row, 4u * b2) : tc::sw32_offset(row, 4u * b2);
 }
+// Stores the level-1 outputs k1 = k0 .. k0 + 7 (k0 a multiple of 8) of the
+// thread's vector (v, b2) into the level-2 operand: the same offsets as
+// l2_off(l2_row(..)), in closed form.  Pass B rows advance 512 bytes per k1
+// (both swizzles); pass A rows keep the atom row (k1 & 7) ^ (v & 7).
+template <uint32_t PASS, uint32_t RL>
+__device__ __forceinline__ void l2_store8(uint8_t* A2, const uint32_t (&y)[8], uint32_t v, uint32_t b2, uint32_t k0) {
+    if (PASS == 1) {
+        uint8_t* o = A2 + l2_off(l2_row(1, v, k0, 7 - RL), b2, RL);
+#pragma unroll
+        for (uint32_t i = 0; i < 8; i++) *reinterpret_cast<uint32_t*>(o + 512u * i) = y[i];
+    } else {
+        const uint32_t v7 = v & 7u;
+        uint8_t* o = A2 + (RL == 4 ? 4096u : 2048u) * v + (RL == 4 ? 512u : 256u) * (k0 >> 3) + 4u * (b2 & 3u);
+#pragma unroll
+        for (uint32_t i = 0; i < 8; i++) {
+            const uint32_t r = i ^ v7;  // row within the 8-row atom
+            const uint32_t off = RL == 4 ? 64u * r + ((((b2 >> 2) ^ (r >> 1)) & 3u) << 4)
+                                         : 32u * r + ((((b2 >> 2) ^ (r >> 2)) & 1u) << 4);
+            *reinterpret_cast<uint32_t*>(o + off) = y[i];
+        }
+    }
+}
 
 // Geometry of a tensor tile.
 struct TcGeo {
@@ -666,10 +688,13 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
                 tw_o = tca::canon(tca::mont_lazy(tw_o, r2, q, qinv), q);
             }
             if (mma2) {
-#pragma unroll
-                for (uint32_t i = 0; i < 8; i++) {
-                    const uint32_t k1 = 32u * h + 8u * part + i;
-                    *reinterpret_cast<uint32_t*>(A2 + l2_off(l2_row(pass, vv, k1, lgV), b2, rl)) = y[i];
+                const uint32_t k0 = 32u * h + 8u * part;
+                if (pass == 0) {
+                    if (rl == 4) l2_store8<0, 4>(A2, y, vv, b2, k0);
+                    else l2_store8<0, 3>(A2, y, vv, b2, k0);
+                } else {
+                    if (rl == 4) l2_store8<1, 4>(A2, y, vv, b2, k0);
+                    else l2_store8<1, 3>(A2, y, vv, b2, k0);
                 }
             } else {
 #pragma unroll
