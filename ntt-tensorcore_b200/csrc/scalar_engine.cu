@@ -26,6 +26,8 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     using E = typename A::elem;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t L = args.len, V = args.vec_per_tile, lgL = args.log_len;
+    // every extent is a power of two: index splits are shifts and masks
+    const uint32_t lgV = 31 - __clz(V), lgN1 = 31 - __clz(args.n1);
     const uint32_t stride = L >= 32 ? L + 1 : L;
     E* t = reinterpret_cast<E*>(smem_raw);
     E* tws = t + (size_t)V * stride;
@@ -54,7 +56,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
         uint32_t v, j;
         uint64_t pos;
-        if (kDIT) { v = idx % V; j = idx / V; } else { v = idx / L; j = idx % L; }
+        if (kDIT) { v = idx & (V - 1); j = idx >> lgV; } else { v = idx >> lgL; j = idx & (L - 1); }
         const uint32_t vec = v0 + v;
         if (MODE == MODE_COL) {
             pos = (uint64_t)j * N2 + vec;
@@ -62,7 +64,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
             pos = (uint64_t)vec * N2 + j;
         } else if (MODE == MODE_GATHER_T) {
             const uint64_t m = (uint64_t)vec * L + j;  // index into the transposed view
-            pos = (m % N1) * N2 + m / N1;
+            pos = (m & (N1 - 1)) * N2 + (m >> lgN1);
         } else {
             pos = (uint64_t)vec * L + j;
         }
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         for (uint32_t s = 0; s < lgL; s++) {
             const uint32_t half = 1u << s;
             for (uint32_t bf = threadIdx.x; bf < half_total; bf += blockDim.x) {
-                const uint32_t v = bf / Lh, j = bf % Lh;
+                const uint32_t v = bf >> (lgL - 1), j = bf & (Lh - 1);
                 const uint32_t p = j & (half - 1);
                 const uint32_t i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
                 E* row = t + (size_t)v * stride;
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         for (int s = (int)lgL - 1; s >= 0; s--) {
             const uint32_t half = 1u << s;
             for (uint32_t bf = threadIdx.x; bf < half_total; bf += blockDim.x) {
-                const uint32_t v = bf / Lh, j = bf % Lh;
+                const uint32_t v = bf >> (lgL - 1), j = bf & (Lh - 1);
                 const uint32_t p = j & (half - 1);
                 const uint32_t i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
                 E* row = t + (size_t)v * stride;
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     // ---- store ----
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
         uint32_t v, k;
-        if (MODE == MODE_GATHER_T) { v = idx / L; k = idx % L; } else { v = idx % V; k = idx / V; }
+        if (MODE == MODE_GATHER_T) { v = idx >> lgL; k = idx & (L - 1); } else { v = idx & (V - 1); k = idx >> lgV; }
         const uint32_t vec = v0 + v;
         const uint32_t kk = kDIT ? k : bitrev(k, (int)lgL);
         E x = t[(size_t)v * stride + kk];
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
             pos = (uint64_t)vec * L + k;
         } else {
             const uint64_t m = (uint64_t)vec * L + k;
-            pos = (m % N1) * N2 + m / N1;  // transpose n2 x n1 -> n1 x n2
+            pos = (m & (N1 - 1)) * N2 + (m >> lgN1);  // transpose n2 x n1 -> n1 x n2
         }
         if (flags & F_POST_PSI_INV) x = ar.mul(x, ld.psi_inv[pos]);
         else if (flags & F_POST_SCALE) x = ar.mul(x, ld.ninv_m);
