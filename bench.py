@@ -51,7 +51,7 @@ def parse():
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
                          "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
-    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc"], default=None,
+    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
@@ -716,10 +716,20 @@ def profile_case(name):
     int8 / dmma: forward+inverse of the 24-limb 2^16 negacyclic batch, four
     launches; batch: a ~600 MB uneven batch (log2 N 12..20, 1..8 limbs, mixed
     directions) launched twice; batch_tc: the same with log2 N 17..20 on
-    tensor-core tiles."""
+    tensor-core tiles; q60: forward + inverse of one 2^20 polynomial mod the
+    60-bit prime, four times."""
     import torch
     import ntt_b200 as nb
-    if name in ("int8", "dmma"):
+    if name == "q60":
+        plan = nb.WidePlan(20, [Q60])
+        x = np.random.default_rng(3).integers(0, Q60, 1 << 20, dtype=np.uint64)
+        d = torch.from_numpy(x.view(np.int64)).cuda()
+        for _ in range(4):
+            plan.transform(d, d, 1)
+            plan.transform(d, d, 1, inverse=True)
+        torch.cuda.synchronize()
+        assert (d.cpu().numpy().view(np.uint64) == x).all()
+    elif name in ("int8", "dmma"):
         qs = nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
         plan = nb.RnsPlan(LOG_N, qs, negacyclic=True)
         x = make_batch(qs, 7)

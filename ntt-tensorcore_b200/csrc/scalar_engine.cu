@@ -160,6 +160,15 @@ int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t
 
 inline uint32_t ilog2u(uint64_t x) { uint32_t l = 0; while ((1ull << l) < x) l++; return l; }
 
+// Vectors per tile: as many as the shared-memory tile holds, fewer while the
+// pass would have under ~1024 tiles (a single large polynomial otherwise
+// leaves most SMs idle).
+inline uint32_t tile_vectors(uint32_t e_max, uint32_t len, uint32_t n_vectors, uint32_t units) {
+    uint32_t v = e_max / len < n_vectors ? e_max / len : n_vectors;
+    while (v > 1 && (uint64_t)(n_vectors / v) * units < 1024) v >>= 1;
+    return v;
+}
+
 // Two-pass (or single-pass) forward/inverse over a plan.  E_max bounds the
 // shared-memory tile in elements.  Two-pass layout for n = N1 * N2:
 //   pass A: columns b of x as [N1][N2]: U[d][b] = DFT_N1 * root^(d*b), stored
@@ -205,7 +214,7 @@ int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const L
     a.n2 = N2;
     a.len = N1;
     a.log_len = lg1;
-    a.vec_per_tile = e_max / N1 < N2 ? e_max / N1 : N2;
+    a.vec_per_tile = tile_vectors(e_max, N1, N2, n_limbs * n_polys);
     a.flags = pre | F_POST_TW | F_STORE_T;
     int rc = launch_pass<S, A>(MODE_COL, a, d_limbs, N2, n_polys, s);
     if (rc) return rc;
@@ -216,7 +225,7 @@ int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const L
     a.n2 = N1;
     a.len = N2;
     a.log_len = lg2;
-    a.vec_per_tile = e_max / N2 < N1 ? e_max / N2 : N1;
+    a.vec_per_tile = tile_vectors(e_max, N2, N1, n_limbs * n_polys);
     a.flags = post;
     return launch_pass<S, A>(MODE_COL, a, d_limbs, N1, n_polys, s);
 }
