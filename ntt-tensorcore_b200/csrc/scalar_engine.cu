@@ -21,6 +21,14 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Shared-memory row layout: element i of a vector at i + (i >> pad_shift)
+// (one pad element per 32 words), so that the register groups' strided
+// loads and stores spread over the banks; rows `tile_stride` apart.
+template <class E>
+__host__ __device__ constexpr uint32_t pad_shift() { return sizeof(E) == 8 ? 4u : 5u; }
+template <class E>
+__host__ __device__ inline uint32_t tile_stride(uint32_t L) { return L + (L >> pad_shift<E>()) + 1; }
+
 template <class S, class A, int MODE>
 __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, const LimbDev<A>* limbs) {
     using E = typename A::elem;
@@ -28,7 +36,8 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     const uint32_t L = args.len, V = args.vec_per_tile, lgL = args.log_len;
     // every extent is a power of two: index splits are shifts and masks
     const uint32_t lgV = 31 - __clz(V), lgN1 = 31 - __clz(args.n1);
-    const uint32_t stride = L >= 32 ? L + 1 : L;
+    const uint32_t stride = tile_stride<E>(L);
+    constexpr uint32_t kPad = pad_shift<E>();
     E* t = reinterpret_cast<E*>(smem_raw);
     E* tws = t + (size_t)V * stride;
 
@@ -72,39 +81,90 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         if (flags & F_PRE_PSI) x = ar.mul(x, ld.psi[pos]);
         if (flags & F_PRE_TW) x = ar.mul(x, tw[((uint64_t)j * vec) & nmask]);
         const uint32_t jj = kDIT ? bitrev(j, (int)lgL) : j;
-        t[(size_t)v * stride + jj] = x;
+        t[(size_t)v * stride + jj + (jj >> kPad)] = x;
     }
     __syncthreads();
 
-    // ---- radix-2 stages ----
-    const uint32_t half_total = total >> 1, Lh = L >> 1;
+    // ---- radix-2 stages, up to three at a time in registers ----
+    // A group of r stages s0 .. s0+r-1 touches, for each base index with zero
+    // bits [s0, s0 + r), exactly the 2^r elements base + k 2^s0; one thread
+    // loads them, runs the group's butterflies (the same butterflies, in the
+    // same order, as one stage at a time) and stores them back.
+    constexpr uint32_t kG = 3, kGN = 1u << kG;
     if (kDIT) {
-        for (uint32_t s = 0; s < lgL; s++) {
-            const uint32_t half = 1u << s;
-            for (uint32_t bf = threadIdx.x; bf < half_total; bf += blockDim.x) {
-                const uint32_t v = bf >> (lgL - 1), j = bf & (Lh - 1);
-                const uint32_t p = j & (half - 1);
-                const uint32_t i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+        for (uint32_t s0 = 0; s0 < lgL; s0 += kG) {
+            const uint32_t r = lgL - s0 < kG ? lgL - s0 : kG, nk = 1u << r;
+            const uint32_t items = V << (lgL - r);
+            for (uint32_t it = threadIdx.x; it < items; it += blockDim.x) {
+                const uint32_t v = it & (V - 1), g = it >> lgV;
+                const uint32_t low = g & ((1u << s0) - 1), base = ((g >> s0) << (s0 + r)) | low;
                 E* row = t + (size_t)v * stride;
-                const E w = tws[p << (lgL - 1 - s)];
-                const E u = row[i0], y = ar.mul(row[i1], w);
-                row[i0] = ar.add(u, y);
-                row[i1] = ar.sub(u, y);
+                E x[kGN];
+#pragma unroll
+                for (uint32_t k = 0; k < kGN; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s0);
+                        x[k] = row[i + (i >> kPad)];
+                    }
+#pragma unroll
+                for (uint32_t tt = 0; tt < kG; tt++) {
+                    if (tt >= r) break;
+                    const uint32_t st = s0 + tt, half = 1u << tt;
+#pragma unroll
+                    for (uint32_t k = 0; k < kGN; k++) {
+                        if ((k & half) || k + half >= nk) continue;
+                        const uint32_t p = low + ((k & (half - 1)) << s0);
+                        const E y = ar.mul(x[k + half], tws[p << (lgL - 1 - st)]);
+                        const E u0 = x[k];
+                        x[k] = ar.add(u0, y);
+                        x[k + half] = ar.sub(u0, y);
+                    }
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kGN; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s0);
+                        row[i + (i >> kPad)] = x[k];
+                    }
             }
             __syncthreads();
         }
     } else {
-        for (int s = (int)lgL - 1; s >= 0; s--) {
-            const uint32_t half = 1u << s;
-            for (uint32_t bf = threadIdx.x; bf < half_total; bf += blockDim.x) {
-                const uint32_t v = bf >> (lgL - 1), j = bf & (Lh - 1);
-                const uint32_t p = j & (half - 1);
-                const uint32_t i0 = ((j >> s) << (s + 1)) | p, i1 = i0 + half;
+        // DIF: stages from lgL-1 down, groups [s_lo, s_lo + r)
+        for (int s_hi = (int)lgL - 1; s_hi >= 0; s_hi -= (int)kG) {
+            const uint32_t r = (uint32_t)s_hi + 1 < kG ? (uint32_t)s_hi + 1 : kG, nk = 1u << r;
+            const uint32_t s_lo = (uint32_t)s_hi + 1 - r, lgG = lgL - r;
+            const uint32_t items = V << lgG;
+            for (uint32_t it = threadIdx.x; it < items; it += blockDim.x) {
+                const uint32_t v = it >> lgG, g = it & ((1u << lgG) - 1);
+                const uint32_t low = g & ((1u << s_lo) - 1), base = ((g >> s_lo) << (s_lo + r)) | low;
                 E* row = t + (size_t)v * stride;
-                const E w = tws[p << (lgL - 1 - s)];
-                const E u = row[i0], y = row[i1];
-                row[i0] = ar.add(u, y);
-                row[i1] = ar.mul(ar.sub(u, y), w);
+                E x[kGN];
+#pragma unroll
+                for (uint32_t k = 0; k < kGN; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s_lo);
+                        x[k] = row[i + (i >> kPad)];
+                    }
+#pragma unroll
+                for (int tt = (int)kG - 1; tt >= 0; tt--) {
+                    if ((uint32_t)tt >= r) continue;
+                    const uint32_t st = s_lo + (uint32_t)tt, half = 1u << tt;
+#pragma unroll
+                    for (uint32_t k = 0; k < kGN; k++) {
+                        if ((k & half) || k + half >= nk) continue;
+                        const uint32_t p = low + ((k & (half - 1)) << s_lo);
+                        const E u0 = x[k], y = x[k + half];
+                        x[k] = ar.add(u0, y);
+                        x[k + half] = ar.mul(ar.sub(u0, y), tws[p << (lgL - 1 - st)]);
+                    }
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kGN; k++)
+                    if (k < nk) {
+                        const uint32_t i = base + (k << s_lo);
+                        row[i + (i >> kPad)] = x[k];
+                    }
             }
             __syncthreads();
         }
@@ -116,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         if (MODE == MODE_GATHER_T) { v = idx >> lgL; k = idx & (L - 1); } else { v = idx & (V - 1); k = idx >> lgV; }
         const uint32_t vec = v0 + v;
         const uint32_t kk = kDIT ? k : bitrev(k, (int)lgL);
-        E x = t[(size_t)v * stride + kk];
+        E x = t[(size_t)v * stride + kk + (kk >> kPad)];
         uint64_t pos;
         if (MODE == MODE_COL) {
             pos = (flags & F_STORE_T) ? (uint64_t)vec * N1 + k : (uint64_t)k * N2 + vec;
@@ -139,8 +199,7 @@ template <class S, class A>
 int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t n_vectors,
                 uint32_t n_polys, cudaStream_t s) {
     using E = typename A::elem;
-    const uint32_t stride = a.len >= 32 ? a.len + 1 : a.len;
-    const size_t smem = ((size_t)a.vec_per_tile * stride + (a.len >> 1) + 1) * sizeof(E);
+    const size_t smem = ((size_t)a.vec_per_tile * tile_stride<E>(a.len) + (a.len >> 1) + 1) * sizeof(E);
     dim3 grid(n_vectors / a.vec_per_tile, a.n_limbs, n_polys);
     if (grid.x == 0 || n_polys > 65535 || a.n_limbs > 65535) return 1;
     void (*k)(PassArgs, const LimbDev<A>*) = nullptr;
