@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="auto", choices=["auto", "int8", "dmma", "scalar"])
-    ap.add_argument("--workload", default="rns", choices=["rns", "uneven", "serve", "q60"],
+    ap.add_argument("--workload", default="rns", choices=["rns", "uneven", "serve", "q60", "aux"],
                     help="rns: the 24-limb 2^16 negacyclic batch (headline); uneven: 512 polynomials of "
                          "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch; "
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
@@ -711,6 +711,63 @@ def run_q60(args, world, rank, local):
 
 
 # ----------------------------------------------------- small profiling cases
+# ------------------------------------------------------ memory-bound helpers
+def run_aux(args, world, rank, local):
+    """The library's HBM-bound helper passes on inputs far larger than L2,
+    against the measured copy peak: the RNS pointwise product (12 B per
+    residue), the u64 transpose (16 B per word) and the in-place bit
+    reversal (16 B per word)."""
+    import torch
+    import ntt_b200 as nb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+
+    def timed(fn, steps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps / 1e3
+
+    out = {}
+    qs = nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
+    plan = nb.RnsPlan(LOG_N, qs, negacyclic=True)
+    polys = 64  # 64 x 24 x 2^16 residues = 402 MB per operand
+    words = polys * N_LIMBS << LOG_N
+    a = torch.randint(0, 1 << 30, (words,), dtype=torch.int32, device=dev)
+    b = torch.randint(0, 1 << 30, (words,), dtype=torch.int32, device=dev)
+    c = torch.empty_like(a)
+    t = timed(lambda: plan.pointwise_mul(c, a, b, polys, stream=stream), args.steps)
+    out["rns_pointwise_mul"] = {"bytes": 12 * words, "s": t, "gbs": 12 * words / t / 1e9}
+    del a, b, c
+    n = 1 << 13
+    x = torch.randint(0, 1 << 62, (n * n,), dtype=torch.int64, device=dev)
+    y = torch.empty_like(x)
+    t = timed(lambda: nb.transpose_u64(y, x, n, n, stream=stream), args.steps)
+    out["u64_transpose_8192x8192"] = {"bytes": 16 * n * n, "s": t, "gbs": 16 * n * n / t / 1e9}
+    t = timed(lambda: nb.bit_reverse_u64(x, n * n, stream=stream), args.steps)
+    out["u64_bit_reverse_2^26"] = {"bytes": 16 * n * n, "s": t, "gbs": 16 * n * n / t / 1e9}
+    for v in out.values():
+        v["frac"] = v["gbs"] / peak
+    return {"metric": "HBM GB/s of the memory-bound helper passes", "unit": "GB/s", "peak": peak,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
+            "kernels": out, "n_gpus": world, "steps": args.steps}
+
+
 def profile_case(name):
     """Small, self-checking cases for ncu captures (a few launches, < 1 GB):
     int8 / dmma: forward+inverse of the 24-limb 2^16 negacyclic batch, four
@@ -767,8 +824,8 @@ def main():
         profile_case(args.profile_case)
         return
     world, rank, local = dist_setup(args)
-    if args.workload in ("uneven", "serve", "q60") and args.impl == "ours":
-        fn = {"uneven": run_uneven, "serve": run_serve, "q60": run_q60}[args.workload]
+    if args.workload in ("uneven", "serve", "q60", "aux") and args.impl == "ours":
+        fn = {"uneven": run_uneven, "serve": run_serve, "q60": run_q60, "aux": run_aux}[args.workload]
         r = fn(args, world, rank, local)
         if rank == 0:
             print(json.dumps(r))

@@ -81,6 +81,35 @@ __global__ void bitrev_u64_kernel(uint64_t* data, uint64_t n, int log_n) {
     }
 }
 
+// In-place bit reversal by tiles, log_n >= 10.  With the index split as
+// (a, b, c) -- a the high 5 bits, c the low 5, b the log_n - 10 middle bits --
+// element (a, b, c) moves to (rev5(c), rev(b), rev5(a)).  One block takes the
+// 32 x 32 tiles of middle values b and rev(b) (b <= rev(b)), reads both with
+// 256-byte rows (c contiguous), and writes each to the other's place, again
+// with rows of consecutive positions.
+__global__ void bitrev_tiled_u64_kernel(uint64_t* data, int log_n) {
+    __shared__ uint64_t ta[32][33], tb[32][33];
+    const int M = log_n - 10;
+    const uint64_t n_mid = 1ull << M;
+    const uint32_t x = threadIdx.x, y = threadIdx.y;  // 32 x 8 threads
+    const uint32_t rx = __brev(x) >> 27;
+    for (uint64_t b = blockIdx.x; b < n_mid; b += gridDim.x) {
+        const uint64_t br = M ? (__brevll(b) >> (64 - M)) : 0;
+        if (br < b) continue;
+        for (uint32_t a = y; a < 32; a += 8) {
+            ta[a][x] = data[((uint64_t)a << (M + 5)) | (b << 5) | x];
+            tb[a][x] = data[((uint64_t)a << (M + 5)) | (br << 5) | x];
+        }
+        __syncthreads();
+        for (uint32_t a2 = y; a2 < 32; a2 += 8) {  // destination high bits a2 = rev5(c), low bits x = rev5(a)
+            const uint32_t c = __brev(a2) >> 27;
+            data[((uint64_t)a2 << (M + 5)) | (br << 5) | x] = ta[rx][c];
+            data[((uint64_t)a2 << (M + 5)) | (b << 5) | x] = tb[rx][c];
+        }
+        __syncthreads();
+    }
+}
+
 // out = a * b mod q with one Montgomery product and one correction by R^2.
 __global__ void pointwise_u64_kernel(uint64_t* out, const uint64_t* a, const uint64_t* b, uint64_t n, M64 ar,
                                      uint64_t r2) {
@@ -88,11 +117,31 @@ __global__ void pointwise_u64_kernel(uint64_t* out, const uint64_t* a, const uin
         out[i] = ar.mul(ar.mul(a[i], b[i]), r2);
 }
 
+// Rows of 2^log_n residues, row r reduced mod limb r % n_limbs.  With
+// log_n >= 2 and 16-byte aligned arrays, a thread takes four residues of one
+// row per step (16-byte accesses, one limb lookup per four residues).
 __global__ void pointwise_rns_kernel(uint32_t* out, const uint32_t* a, const uint32_t* b, uint32_t log_n,
                                      uint32_t n_limbs, uint64_t total, const LimbDev<M32>* limbs,
-                                     const uint32_t* r2s) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
+                                     const uint32_t* r2s, bool vec4) {
+    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+    if (vec4) {
+        const uint64_t quads = total >> 2;
+        for (uint64_t qi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < quads; qi += step) {
+            const uint32_t limb = (uint32_t)(((qi << 2) >> log_n) % n_limbs);
+            const M32 ar = limbs[limb].ar;
+            const uint32_t r2 = r2s[limb];
+            const uint4 x = __ldcs(reinterpret_cast<const uint4*>(a) + qi);
+            const uint4 y = __ldcs(reinterpret_cast<const uint4*>(b) + qi);
+            uint4 z;
+            z.x = ar.mul(ar.mul(x.x, y.x), r2);
+            z.y = ar.mul(ar.mul(x.y, y.y), r2);
+            z.z = ar.mul(ar.mul(x.z, y.z), r2);
+            z.w = ar.mul(ar.mul(x.w, y.w), r2);
+            __stcs(reinterpret_cast<uint4*>(out) + qi, z);
+        }
+        return;
+    }
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += step) {
         const uint32_t limb = (uint32_t)((i >> log_n) % n_limbs);
         const M32 ar = limbs[limb].ar;
         out[i] = ar.mul(ar.mul(a[i], b[i]), r2s[limb]);
@@ -418,7 +467,14 @@ int nttb_u64_pointwise_mul(const nttb_plan* P, uint64_t* out, const uint64_t* a,
 int nttb_u64_bit_reverse(uint64_t* d, uint64_t n, void* stream) {
     if (!d || !pow2(n)) return fail(NTTB_ERR_INVALID_ARG, "bit_reverse: n must be a power of two");
     ProfScope prof("bitrev_u64", (cudaStream_t)stream);
-    bitrev_u64_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d, n, (int)ilog2(n));
+    const int log_n = (int)ilog2(n);
+    if (log_n >= 10) {
+        const uint64_t mids = n >> 10;
+        bitrev_tiled_u64_kernel<<<(unsigned)(mids < 148 * 16 ? mids : 148 * 16), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+            d, log_n);
+    } else {
+        bitrev_u64_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d, n, log_n);
+    }
     return cuda_status("bit_reverse");
 }
 
@@ -568,8 +624,9 @@ int nttb_rns_pointwise_mul(const nttb_rns_plan* P, uint32_t* out, const uint32_t
     if (!P || !out || !a || !b) return fail(NTTB_ERR_INVALID_ARG, "rns_pointwise_mul: null argument");
     uint64_t total = (uint64_t)n_polys * P->p.n_limbs * P->p.n;
     ProfScope prof("pointwise_rns", (cudaStream_t)stream);
-    pointwise_rns_kernel<<<grid_for(total), 256, 0, (cudaStream_t)stream>>>(out, a, b, P->p.log_n, P->p.n_limbs,
-                                                                            total, P->p.d_limbs, P->d_r2);
+    const bool vec4 = P->p.log_n >= 2 && ((((uintptr_t)out) | ((uintptr_t)a) | ((uintptr_t)b)) & 15) == 0;
+    pointwise_rns_kernel<<<grid_for(vec4 ? total / 4 : total), 256, 0, (cudaStream_t)stream>>>(
+        out, a, b, P->p.log_n, P->p.n_limbs, total, P->p.d_limbs, P->d_r2, vec4);
     return cuda_status("rns_pointwise_mul");
 }
 

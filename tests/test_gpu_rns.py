@@ -179,3 +179,27 @@ def test_launch_accounting(torch_cuda):
     assert nb.launch_count() > c0
     assert sum(v[0] for v in prof.values()) == nb.launch_count() - c0
     assert all(v[1] > 0 for v in prof.values())
+
+
+@pytest.mark.parametrize("lg,polys,offset", [(10, 5, 0), (10, 3, 1), (1, 4, 0), (12, 2, 3)])
+def test_pointwise_mul_rows_and_alignment(torch_cuda, lg, polys, offset):
+    """The pointwise product row by row (row r mod limb r % n_limbs) against
+    numpy, on 16-byte aligned arrays (four residues per access) and on arrays
+    offset by a few words (one residue per access)."""
+    moduli = PRIMES17[:3]
+    n = 1 << lg
+    plan = nb.RnsPlan(lg, moduli, negacyclic=False)
+    a, b = rand_batch(polys, moduli, n, 5), rand_batch(polys, moduli, n, 6)
+    words = polys * len(moduli) * n
+    big = torch_cuda.zeros(3 * (words + 8), dtype=torch_cuda.int32, device="cuda")
+    da = big[offset:offset + words]
+    db = big[words + 8 + offset:2 * words + 8 + offset]
+    out = big[2 * words + 16 + offset:3 * words + 16 + offset]
+    da.copy_(to_dev(torch_cuda, a.reshape(-1)))
+    db.copy_(to_dev(torch_cuda, b.reshape(-1)))
+    plan.pointwise_mul(out, da, db, polys)
+    torch_cuda.cuda.synchronize()
+    got = to_host(out, np.uint32).reshape(polys, len(moduli), n).astype(np.uint64)
+    q = np.array(moduli, dtype=np.uint64)[None, :, None]
+    want = (a.astype(np.uint64) * b.astype(np.uint64)) % q
+    assert (got == want).all()

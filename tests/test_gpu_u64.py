@@ -192,3 +192,15 @@ def test_vs_reference_gpu_kernels(torch_cuda, n, op):
         plan.transform(d, inverse=(op % 2 == 1), engine="scalar" if op < 2 else "auto")
     torch_cuda.cuda.synchronize()
     assert (to_host(d, np.uint64) == to_host(d_ref, np.uint64)).all()
+
+
+@pytest.mark.parametrize("lg", [1, 5, 9, 10, 11, 14, 20])
+def test_bit_reverse_every_path(torch_cuda, lg):
+    """In-place bit reversal: the element-wise kernel below 2^10, the tiled one
+    (32 x 32 tiles swapped through shared memory) from 2^10 on."""
+    n = 1 << lg
+    x = np.random.default_rng(lg).integers(0, 1 << 62, n, dtype=np.uint64)
+    d = to_dev(torch_cuda, x)
+    nb.bit_reverse_u64(d, n)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == O.bit_reverse(x)).all()
