@@ -53,8 +53,10 @@ NTTB_API const char* nttb_last_error(void);
 /* Device-side error bits raised by bounded waits in the persistent kernels
  * (bit 0: an INT8-engine mbarrier wait ran out of budget, bit 1: a wait on
  * another CTA of an INT8 cluster did, bit 2: an uneven-batch queue
- * dependency wait did; the work item ran on regardless and its output is
- * wrong).  Reads after a device synchronize; clear != 0 resets them. */
+ * dependency wait did, bit 3: a batch tensor tile's wait on its MMA or image
+ * copy did; the work item ran on regardless and its output is wrong).  Every
+ * such wait gives up after about 2 s of device time.  Reads after a device
+ * synchronize; clear != 0 resets them. */
 NTTB_API int nttb_device_errors(uint32_t* flags, int clear);
 
 /* ------------------------------------------------ modular parameters (host)
@@ -242,6 +244,12 @@ NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t*
                              nttb_batch_config* config);
 /* CTAs of the persistent launch (SMs x resident CTAs per SM, at most the tile count). */
 NTTB_API int nttb_batch_ctas(const nttb_batch* batch, uint32_t* ctas);
+/* Test hook for the failure path: makes the second pass of two-pass unit
+ * `unit` wait for one first-pass tile more than exist, so that its bounded
+ * device wait runs out (about 2 s): the launch still completes, with that
+ * unit's result unreliable and bit 2 set in nttb_device_errors.  Recreate
+ * the batch afterwards. */
+NTTB_API int nttb_batch_test_stall(nttb_batch* batch, uint32_t unit);
 
 /* ------------------------------------------------------------- serving
  * No reference counterpart (the reference has no request loop).  A server

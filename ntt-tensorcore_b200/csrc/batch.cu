@@ -131,10 +131,12 @@ struct BArgs {
 };
 
 __device__ __forceinline__ bool wait_ge(const uint32_t* p, uint32_t target) {
-    for (uint32_t i = 0; i < (1u << 24); i++) {
+    const uint64_t t0 = tc::globaltimer_ns();
+    for (uint32_t i = 0; i < (1u << 26); i++) {  // the iteration cap backs up the clock
         uint32_t v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
         if (v >= target) return true;
+        if ((i & 15) == 15 && tc::globaltimer_ns() - t0 > tc::kWaitBudgetNs) return false;
         __nanosleep(64);
     }
     return false;
@@ -1606,6 +1608,20 @@ NTTB_API int nttb_batch_info(const nttb_batch* batch, uint64_t* units, uint64_t*
     if (tiles) *tiles = batch->b->n_tiles;
     if (ws_bytes) *ws_bytes = batch->b->ws_bytes;
     if (config) *config = batch->b->cfg;
+    return NTTB_OK;
+}
+
+NTTB_API int nttb_batch_test_stall(nttb_batch* batch, uint32_t unit) {
+    if (!batch) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_test_stall: null batch");
+    Batch* b = batch->b;
+    if (unit >= b->n_units) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_test_stall: unit %u of %u", unit, b->n_units);
+    nttb::BUnit u{};
+    if (cudaMemcpy(&u, b->d_units + unit, sizeof u, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(NTTB_ERR_CUDA, "nttb_batch_test_stall: read");
+    if (!u.lg1) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_test_stall: unit %u has a single pass", unit);
+    u.tiles_a += 1;  // pass B now waits for one pass A tile more than there are
+    if (cudaMemcpy(b->d_units + unit, &u, sizeof u, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(NTTB_ERR_CUDA, "nttb_batch_test_stall: write");
     return NTTB_OK;
 }
 

@@ -59,12 +59,28 @@ __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gmem_src, u
         : "memory");
 }
 
+// Device clock in nanoseconds (%globaltimer) and the budget of every
+// bounded wait: far above any legitimate wait of these kernels (a whole
+// batch takes tens of milliseconds), short enough that a wait that can never
+// end gives up within a few seconds and the host sees the error.  An
+// iteration cap backs up the clock.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+constexpr uint64_t kWaitBudgetNs = 2000000000ull;
+
 // Bounded wait for the phase with the given parity.  Returns false when the
-// budget (~2^24 polls, well over a second) runs out.
+// time budget runs out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < (1u << 24); i++) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 0; i < (1u << 26); i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) __nanosleep(64);
+        if (i > 64) {
+            if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
+            __nanosleep(64);
+        }
     }
     return false;
 }
@@ -115,9 +131,13 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t pa
 }
 // Bounded wait (acquire at cluster scope) for arrivals made by other CTAs.
 __device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < (1u << 24); i++) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 0; i < (1u << 26); i++) {
         if (mbar_try_wait_cluster(bar, parity)) return true;
-        if (i > 64) __nanosleep(64);
+        if (i > 64) {
+            if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
+            __nanosleep(64);
+        }
     }
     return false;
 }

@@ -131,6 +131,7 @@ def lib():
         "nttb_batch_plan_destroy": (_int, [_vp]),
         "nttb_batch_default_config": (_int, [ctypes.POINTER(BatchConfig)]),
         "nttb_batch_ctas": (_int, [_vp, ctypes.POINTER(_u32)]),
+        "nttb_batch_test_stall": (_int, [_vp, _u32]),
         "nttb_batch_autotune": (_int, [_vp, _vp, _u32, _vp, ctypes.POINTER(BatchConfig)]),
         "nttb_batch_create": (_int, [_vp, _vp, _u32, ctypes.POINTER(BatchConfig), ctypes.POINTER(_vp)]),
         "nttb_batch_destroy": (_int, [_vp]),
@@ -253,6 +254,10 @@ class Batch:
 
     def graph_launch(self, stream=None):
         _check(lib().nttb_batch_graph_launch(self._h, _stream(stream)))
+
+    def test_stall(self, unit):
+        """Failure-path test hook (nttb_batch_test_stall)."""
+        _check(lib().nttb_batch_test_stall(self._h, unit))
 
     def info(self):
         u, t, w, cfg = _u64(), _u64(), _u64(), BatchConfig()

@@ -272,3 +272,35 @@ def test_batch_tensor_flag_where_the_shape_allows(torch_cuda):
     check(torch_cuda, jobs)
     with pytest.raises(nb.NTTError):
         plan.batch(spec(jobs), {"tensor": 2})
+
+
+def test_batch_wait_timeout_is_reported_and_recoverable(torch_cuda):
+    """Failure path without a GPU fault: a planted unsatisfiable dependency
+    (the test hook raises the first-pass tile count that one unit's second
+    pass waits for) makes that bounded device wait run out; the launch
+    completes, nttb_device_errors reports it, the units of other sizes are
+    still exact, and the context stays usable for a fresh batch."""
+    import time
+    rng = np.random.default_rng(81)
+    plan = nb.BatchPlan(PRIMES[:4], 16, negacyclic=True)
+    assert nb.device_errors() == 0
+    for config in (TENSOR[0], {"tile_elems": 4096, "threads": 256, "tensor": 0}):
+        jobs = make_jobs(torch_cuda, rng, 4, (14, 16), (1, 1), 4)
+        b = plan.batch(spec(jobs), config)
+        b.test_stall(0)  # units run largest first: unit 0 belongs to the largest job
+        t = time.time()
+        b.launch()
+        torch_cuda.cuda.synchronize()
+        assert time.time() - t < 30
+        flags = nb.device_errors()
+        assert flags & 4, flags
+        largest = max(j[2] for j in jobs)
+        for j in jobs:
+            if j[2] == largest:
+                continue  # the stalled unit, or one of its size
+            got = to_host(j[1], np.uint32).reshape(j[0].shape).astype(np.uint64)
+            assert (got == expect(j)).all()
+        b.close()
+    fresh = make_jobs(torch_cuda, rng, 6, (8, 16), (1, 2), 4)
+    plan.batch(spec(fresh)).launch()
+    check(torch_cuda, fresh)
