@@ -61,6 +61,19 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
 
     constexpr bool kDIT = (MODE == MODE_COL || MODE == MODE_GATHER_T);
 
+    // Column passes with at most one vector per thread of the block keep a
+    // thread on one column: its elements j (or outputs k) step by
+    // kThreads / V, so the negacyclic twist psi^(j N2 + col) and the
+    // four-step twiddle root^(k col) are geometric along them and are
+    // generated by one product per element instead of a table gather.
+    const bool chain = MODE == MODE_COL && V <= (uint32_t)kThreads;
+    const uint32_t lane_v = threadIdx.x & (V - 1), step_j = (uint32_t)kThreads >> lgV;
+    E psi_cur = 0, psi_step = 0;
+    if (chain && (flags & F_PRE_PSI) && (threadIdx.x >> lgV) < L) {
+        psi_cur = ld.psi[(uint64_t)(threadIdx.x >> lgV) * N2 + v0 + lane_v];
+        const uint64_t e = (uint64_t)step_j * N2;
+        psi_step = e < args.n ? ld.psi[e] : tw[0];  // tw[0] = 1 (Montgomery form)
+    }
     // ---- load ----
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
         uint32_t v, j;
@@ -78,7 +91,14 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
             pos = (uint64_t)vec * L + j;
         }
         E x = (E)src[pos];
-        if (flags & F_PRE_PSI) x = ar.mul(x, ld.psi[pos]);
+        if (flags & F_PRE_PSI) {
+            if (chain) {
+                x = ar.mul(x, psi_cur);
+                psi_cur = ar.mul(psi_cur, psi_step);
+            } else {
+                x = ar.mul(x, ld.psi[pos]);
+            }
+        }
         if (flags & F_PRE_TW) x = ar.mul(x, tw[((uint64_t)j * vec) & nmask]);
         const uint32_t jj = kDIT ? bitrev(j, (int)lgL) : j;
         t[(size_t)v * stride + jj + (jj >> kPad)] = x;
@@ -170,6 +190,12 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         }
     }
 
+    E tw_cur = 0, tw_step = 0;
+    if (chain && (flags & F_POST_TW) && (threadIdx.x >> lgV) < L) {
+        const uint64_t col = v0 + lane_v;
+        tw_cur = tw[((uint64_t)(threadIdx.x >> lgV) * col) & nmask];
+        tw_step = tw[((uint64_t)step_j * col) & nmask];
+    }
     // ---- store ----
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
         uint32_t v, k;
@@ -180,7 +206,14 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         uint64_t pos;
         if (MODE == MODE_COL) {
             pos = (flags & F_STORE_T) ? (uint64_t)vec * N1 + k : (uint64_t)k * N2 + vec;
-            if (flags & F_POST_TW) x = ar.mul(x, tw[((uint64_t)k * vec) & nmask]);
+            if (flags & F_POST_TW) {
+                if (chain) {
+                    x = ar.mul(x, tw_cur);
+                    tw_cur = ar.mul(tw_cur, tw_step);
+                } else {
+                    x = ar.mul(x, tw[((uint64_t)k * vec) & nmask]);
+                }
+            }
         } else if (MODE == MODE_ROW_NAT) {
             pos = (uint64_t)vec + (uint64_t)N1 * k;
         } else if (MODE == MODE_GATHER_T) {
