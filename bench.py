@@ -15,6 +15,7 @@ max over ranks.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--engine auto|int8|dmma|scalar]
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -170,6 +171,69 @@ def cpu_reference(qs, steps, warmup, threads=0):
     assert (y == x).all(), "reference round trip failed"
     return {"value": coeffs * steps / dt, "unit": UNIT, "cores": used, "kind": kind,
             "sample": "%d x (24 limbs x 2^16 negacyclic forward+inverse)" % steps, "seconds": dt}
+
+
+def reference_gpu_bar(qs, steps, warmup, device=0):
+    """The reference's own GPU kernels on the same workload: ntt_init per
+    modulus, then ntt_forward_optimized + ntt_inverse_optimized on every limb
+    (oracle/_ref, the reference sources compiled unmodified for sm_100a), in
+    the reference's uint64 words, queued on one stream and timed with CUDA
+    events.  The reference has no negacyclic code, so this is the cyclic
+    transform: the same data volume with the psi twist left out.  The
+    forward is checked against the reference's ntt_host on the same batch."""
+    import torch
+    from oracle import oracle as O
+    R = O.ref()
+    if R is None:
+        return {"unavailable": "reference library oracle/_ref/libntt_ref.so not built"}
+    torch.cuda.set_device(device)
+    dev = torch.device("cuda", device)
+    stream = torch.cuda.Stream(device=dev)
+    n = 1 << LOG_N
+    cfgs = (ctypes.c_void_p * N_LIMBS)(*[R.ref_ntt_init(n, int(q)) for q in qs])
+    try:
+        batch_bytes = N_LIMBS * n * 8
+        pool_n = max(8, int(np.ceil(2.4 * L2_BYTES / batch_bytes)))
+        host = [make_batch(qs, 2000 + i).astype(np.uint64) for i in range(4)]
+        pool = torch.empty((pool_n, N_LIMBS * n), dtype=torch.int64, device=dev)
+        for i in range(pool_n):
+            pool[i].copy_(torch.from_numpy(host[i % 4].reshape(-1).view(np.int64)))
+        torch.cuda.synchronize()
+
+        def run(buf, which):
+            R.ref_ntt_rns_optimized(cfgs, N_LIMBS, 1, ctypes.c_void_p(buf.data_ptr()), which, stream.cuda_stream)
+
+        # parity: the forward of one batch against ntt_host on the host
+        probe = pool[0].clone()
+        run(probe, 0)
+        torch.cuda.synchronize()
+        want = host[0].copy()
+        O.ref_host_batch(want, qs, inverse=False, negacyclic=False)
+        forward_ok = bool((probe.cpu().numpy().view(np.uint64) == want.reshape(-1)).all())
+        del probe
+        for i in range(max(3, warmup)):
+            run(pool[i % pool_n], 2)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(steps):
+            run(pool[i % pool_n], 2)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        round_trip_ok = all((pool[i].cpu().numpy().view(np.uint64) == host[i % 4].reshape(-1)).all()
+                            for i in range(min(pool_n, 4)))
+    finally:
+        for c in cfgs:
+            R.ref_ntt_cleanup(c)
+    coeffs = 2 * N_LIMBS * n
+    log_inner = 6
+    launches = N_LIMBS * (2 * (1 + LOG_N % log_inner + LOG_N // log_inner) + 1)
+    return {"value": coeffs * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "kernels": "ntt_forward_optimized + ntt_inverse_optimized per limb (cyclic; uint64 words)",
+            "launches_per_step": launches, "forward_matches_ntt_host": forward_ok,
+            "round_trip_ok": bool(round_trip_ok), "l2": "pool of %d batches (%.0f MB) > L2" %
+            (pool_n, pool_n * batch_bytes / 1e6)}
 
 
 def bounded_cpu_baseline(qs, budget_s=10.0):
@@ -846,6 +910,10 @@ def main():
                 "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
                                  "sample": r["sample"]},
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        import torch
+        if torch.cuda.is_available():
+            # the reference's own GPU kernels on the same batch (reported beside the CPU arm)
+            line["reference_gpu"] = reference_gpu_bar(qs, args.steps, args.warmup, local)
         print(json.dumps(line))
         return
     result, qs = run_ours(args, world, rank, local)

@@ -129,6 +129,27 @@ void ref_ntt_run(void* cfg, uint64_t* d_data, int op) {
     cudaDeviceSynchronize();
 }
 
+// The reference's optimized transforms (src/ntt_optimized.cu:515-557 forward,
+// :559-600 inverse) over a batch laid out [poly][limb][n], limb l with
+// cfgs[l] (one ntt_init per modulus), queued on `stream` with no
+// synchronisation: ntt_forward_batch's per-polynomial loop
+// (src/ntt_basic.cu:337-361) taken limb by limb, since every limb has its own
+// modulus.  which: 0 forward, 1 inverse, 2 forward then inverse.
+void ref_ntt_rns_optimized(void* const* cfgs, uint64_t n_limbs, uint64_t n_polys, uint64_t* d_data, int which,
+                           void* stream) {
+    auto s = (cudaStream_t)stream;
+    for (int pass = 0; pass < 2; pass++) {
+        if ((which == 0 && pass == 1) || (which == 1 && pass == 0)) continue;
+        for (uint64_t p = 0; p < n_polys; p++)
+            for (uint64_t l = 0; l < n_limbs; l++) {
+                auto* c = (const ntt::NTTConfig*)cfgs[l];
+                uint64_t* d = d_data + (p * n_limbs + l) * c->n;
+                if (pass == 0) ntt::ntt_forward_optimized(d, c, s);
+                else ntt::ntt_inverse_optimized(d, c, s);
+            }
+    }
+}
+
 }  // extern "C"
 
 // ---- K-limb reference host code (include/ntt_arbitrary.cuh) ----

@@ -194,6 +194,35 @@ def test_vs_reference_gpu_kernels(torch_cuda, n, op):
     assert (to_host(d, np.uint64) == to_host(d_ref, np.uint64)).all()
 
 
+@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+def test_reference_optimized_on_rns_moduli(torch_cuda):
+    """The reference's ntt_forward_optimized / ntt_inverse_optimized over the
+    24 distinct 31-bit moduli of the RNS batch (one ntt_init per modulus,
+    queued on one stream, no synchronisation inside) give the same bytes as
+    this library's uint64 transform per limb, and the round trip returns the input."""
+    import ctypes
+    R = O.ref()
+    n, limbs = 1 << 16, 24
+    qs = nb.generate_primes(31, 17, limbs)
+    x = np.stack([rand(n, int(q), 500 + l) for l, q in enumerate(qs)])
+    cfgs = (ctypes.c_void_p * limbs)(*[R.ref_ntt_init(n, int(q)) for q in qs])
+    stream = torch_cuda.cuda.Stream()
+    try:
+        d = to_dev(torch_cuda, x.reshape(-1))
+        R.ref_ntt_rns_optimized(cfgs, limbs, 1, ctypes.c_void_p(d.data_ptr()), 0, stream.cuda_stream)
+        torch_cuda.cuda.synchronize()
+        fwd = to_host(d, np.uint64).reshape(limbs, n)
+        R.ref_ntt_rns_optimized(cfgs, limbs, 1, ctypes.c_void_p(d.data_ptr()), 1, stream.cuda_stream)
+        torch_cuda.cuda.synchronize()
+        assert (to_host(d, np.uint64).reshape(limbs, n) == x).all()
+    finally:
+        for c in cfgs:
+            R.ref_ntt_cleanup(c)
+    for l, q in enumerate(qs):
+        ours = run_u64(torch_cuda, nb.Plan(n, int(q)), x[l])
+        assert (ours == fwd[l]).all(), "limb %d (q=%d) mismatches: %d" % (l, q, int((ours != fwd[l]).sum()))
+
+
 @pytest.mark.parametrize("lg", [1, 5, 9, 10, 11, 14, 20])
 def test_bit_reverse_every_path(torch_cuda, lg):
     """In-place bit reversal: the element-wise kernel below 2^10, the tiled one
