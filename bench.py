@@ -52,7 +52,7 @@ def parse():
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
                          "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
-    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60"], default=None,
+    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60", "move"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
@@ -779,8 +779,8 @@ def run_q60(args, world, rank, local):
 def run_aux(args, world, rank, local):
     """The library's HBM-bound helper passes on inputs far larger than L2,
     against the measured copy peak: the RNS pointwise product (12 B per
-    residue), the u64 transpose (16 B per word) and the in-place bit
-    reversal (16 B per word)."""
+    residue), the u64 transpose out of place and in place, and the in-place
+    bit reversal (16 B per word each; the last three on TMA tiles)."""
     import torch
     import ntt_b200 as nb
 
@@ -823,6 +823,8 @@ def run_aux(args, world, rank, local):
     y = torch.empty_like(x)
     t = timed(lambda: nb.transpose_u64(y, x, n, n, stream=stream), args.steps)
     out["u64_transpose_8192x8192"] = {"bytes": 16 * n * n, "s": t, "gbs": 16 * n * n / t / 1e9}
+    t = timed(lambda: nb.transpose_u64(x, x, n, n, stream=stream), args.steps)
+    out["u64_transpose_in_place_8192x8192"] = {"bytes": 16 * n * n, "s": t, "gbs": 16 * n * n / t / 1e9}
     t = timed(lambda: nb.bit_reverse_u64(x, n * n, stream=stream), args.steps)
     out["u64_bit_reverse_2^26"] = {"bytes": 16 * n * n, "s": t, "gbs": 16 * n * n / t / 1e9}
     for v in out.values():
@@ -838,9 +840,29 @@ def profile_case(name):
     launches; batch: a ~600 MB uneven batch (log2 N 12..20, 1..8 limbs, mixed
     directions) launched twice; batch_tc: the same with log2 N 17..20 on
     tensor-core tiles; q60: forward + inverse of one 2^20 polynomial mod the
-    60-bit prime, four times."""
+    60-bit prime, four times; move: the TMA tile kernels on 4096 x 4096
+    words (transpose, in-place transpose, bit reversal), one launch each."""
     import torch
     import ntt_b200 as nb
+    if name == "move":
+        # TMA tile kernels: 4096 x 4096 words (128 MB) transposed out of place,
+        # then in place, then bit-reversed in place; checked against numpy
+        n = 4096
+        x = np.random.default_rng(5).integers(0, 1 << 63, n * n, dtype=np.uint64)
+        src = torch.from_numpy(x.view(np.int64)).cuda()
+        dst = torch.empty_like(src)
+        nb.transpose_u64(dst, src, n, n)
+        nb.transpose_u64(dst, dst, n, n)
+        nb.bit_reverse_u64(dst, n * n)
+        torch.cuda.synchronize()
+        got = dst.cpu().numpy().view(np.uint64)
+        idx = np.arange(n * n, dtype=np.uint64)
+        rev = np.zeros_like(idx)
+        for b in range(24):
+            rev |= ((idx >> np.uint64(b)) & np.uint64(1)) << np.uint64(23 - b)
+        assert (got == x[rev]).all()
+        assert nb.device_errors() == 0
+        return
     if name == "q60":
         plan = nb.WidePlan(20, [Q60])
         x = np.random.default_rng(3).integers(0, Q60, 1 << 20, dtype=np.uint64)

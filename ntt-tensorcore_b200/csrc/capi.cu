@@ -243,11 +243,18 @@ const char* nttb_last_error(void) { return g_last_error.c_str(); }
 
 int nttb_device_errors(uint32_t* flags, int clear) {
     if (!flags) return fail(NTTB_ERR_INVALID_ARG, "device_errors: null argument");
-    *flags = int8_device_errors(clear != 0) | (batch_device_errors(clear != 0) << 2);
+    *flags = int8_device_errors(clear != 0) | (batch_device_errors(clear != 0) << 2) |
+             (tma_move_device_errors(clear != 0) << 4);
     return cuda_status("device_errors");
 }
 
 static bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
+// Status of a TMA tile-mover launch (0 launched, 2 CUDA error).
+static int tma_status(int t, const char* what) {
+    if (t == 0) return NTTB_OK;
+    const int rc = cuda_status(what);
+    return rc ? rc : fail(NTTB_ERR_CUDA, "%s: TMA tile launch failed", what);
+}
 static uint32_t ilog2(uint64_t n) { uint32_t l = 0; while ((1ull << l) < n) l++; return l; }
 
 int nttb_create_params(uint64_t q, uint64_t n, nttb_modular_params* out) {
@@ -435,10 +442,15 @@ int nttb_u64_transpose(uint64_t* dst, const uint64_t* src, uint64_t rows, uint64
         // The reference's helpers are called in place on square matrices
         // (tests/debug_rowmaj.cu:122-124); serve that race-free.
         if (rows != cols) return fail(NTTB_ERR_INVALID_ARG, "transpose: in place only for square matrices");
+        const int t = tma_transpose_square_inplace_u64(dst, rows, (cudaStream_t)stream);
+        if (t != 1) return tma_status(t, "transpose");
         ProfScope prof("transpose_square_inplace", (cudaStream_t)stream);
         transpose_square_inplace_kernel<<<grid_for(rows * cols), 256, 0, (cudaStream_t)stream>>>(dst, rows);
         return cuda_status("transpose");
     }
+    const int t = tma_transpose_u64(dst, src, rows, cols, (cudaStream_t)stream);
+    if (t != 1) return tma_status(t, "transpose");
+    // shapes that are not whole 32 x 32 tiles, or unaligned arrays
     dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
     if (grid.y > 65535) return fail(NTTB_ERR_UNSUPPORTED, "transpose: too many rows");
     ProfScope prof("transpose_u64", (cudaStream_t)stream);
@@ -466,8 +478,12 @@ int nttb_u64_pointwise_mul(const nttb_plan* P, uint64_t* out, const uint64_t* a,
 
 int nttb_u64_bit_reverse(uint64_t* d, uint64_t n, void* stream) {
     if (!d || !pow2(n)) return fail(NTTB_ERR_INVALID_ARG, "bit_reverse: n must be a power of two");
-    ProfScope prof("bitrev_u64", (cudaStream_t)stream);
     const int log_n = (int)ilog2(n);
+    if (log_n >= 10) {
+        const int t = tma_bit_reverse_u64(d, log_n, (cudaStream_t)stream);
+        if (t != 1) return tma_status(t, "bit_reverse");
+    }
+    ProfScope prof("bitrev_u64", (cudaStream_t)stream);
     if (log_n >= 10) {
         const uint64_t mids = n >> 10;
         bitrev_tiled_u64_kernel<<<(unsigned)(mids < 148 * 16 ? mids : 148 * 16), dim3(32, 8), 0, (cudaStream_t)stream>>>(

@@ -119,6 +119,13 @@ int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStre
 // Uneven-batch queue kernel (batch.cu): its bounded-wait error bits.
 uint32_t batch_device_errors(bool clear);
 
+// TMA tile mover (tma_move.cu).  Each returns 0 on launch, 1 when the shape
+// or alignment is not served (the caller uses the plain kernels), 2 on a CUDA error.
+int tma_transpose_u64(uint64_t* dst, const uint64_t* src, uint64_t rows, uint64_t cols, cudaStream_t stream);
+int tma_transpose_square_inplace_u64(uint64_t* d, uint64_t n, cudaStream_t stream);
+int tma_bit_reverse_u64(uint64_t* d, int log_n, cudaStream_t stream);
+uint32_t tma_move_device_errors(bool clear);
+
 // FP64 DMMA tensor-core engine (tc_dmma.cu).
 bool dmma_serves(const Plan32& p, bool src_u64);
 int dmma_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,

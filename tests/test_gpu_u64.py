@@ -136,6 +136,80 @@ def test_transpose_helpers(torch_cuda):
     assert (to_host(back, np.uint64) == x).all()
 
 
+@pytest.mark.parametrize("rows,cols", [(32, 32), (64, 128), (128, 64), (96, 4096), (4096, 96), (2048, 2048),
+                                       (33, 64), (64, 48), (1, 1000), (7, 3)])
+def test_transpose_every_shape(torch_cuda, rows, cols):
+    """Out-of-place transpose: TMA tiles where rows and cols are multiples of
+    32, the plain tiled kernel otherwise; both against numpy."""
+    x = np.random.default_rng(rows * 7919 + cols).integers(0, 1 << 63, rows * cols, dtype=np.uint64)
+    src = to_dev(torch_cuda, x)
+    dst = torch_cuda.full_like(src, -1)
+    nb.transpose_u64(dst, src, rows, cols)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(dst, np.uint64) == x.reshape(rows, cols).T.reshape(-1)).all()
+    assert nb.device_errors() == 0
+
+
+def test_transpose_unaligned_arrays(torch_cuda):
+    """Arrays that start 8 bytes past a 16-byte boundary take the plain kernel."""
+    rows, cols = 64, 96
+    x = np.random.default_rng(11).integers(0, 1 << 63, rows * cols, dtype=np.uint64)
+    src_buf = to_dev(torch_cuda, np.concatenate([np.zeros(1, np.uint64), x]))
+    dst_buf = torch_cuda.zeros(rows * cols + 1, dtype=torch_cuda.int64, device="cuda")
+    src, dst = src_buf[1:], dst_buf[1:]
+    assert src.data_ptr() % 16 == 8 and dst.data_ptr() % 16 == 8
+    nb.transpose_u64(dst, src, rows, cols)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(dst, np.uint64) == x.reshape(rows, cols).T.reshape(-1)).all()
+    assert int(dst_buf[0].item()) == 0
+
+
+def test_tma_paths_are_the_ones_that_run(torch_cuda):
+    """Whole tiles on 16-byte aligned arrays launch the TMA tile kernels (the
+    profiler names the kernel that ran); ragged shapes the plain ones."""
+    x = to_dev(torch_cuda, np.arange(64 * 64, dtype=np.uint64))
+    y = torch_cuda.empty_like(x)
+    nb.profile_start()
+    nb.transpose_u64(y, x, 64, 64)
+    nb.transpose_u64(x, x, 64, 64)
+    nb.bit_reverse_u64(x, 64 * 64)
+    nb.transpose_u64(y[:40 * 40], x[:40 * 40], 40, 40)
+    torch_cuda.cuda.synchronize()
+    ran = nb.profile_stop()
+    for name in ("tma_transpose_u64", "tma_transpose_square_inplace_u64", "tma_bitrev_u64", "transpose_u64"):
+        assert ran.get(name, (0, 0))[0] == 1, (name, ran)
+
+
+@pytest.mark.parametrize("n", [32, 64, 96, 1024, 4096, 40, 1])
+def test_transpose_square_in_place(torch_cuda, n):
+    """In-place transpose of a square matrix: TMA tile pairs for multiples of
+    32, the element-pair kernel otherwise."""
+    x = np.random.default_rng(n).integers(0, 1 << 63, n * n, dtype=np.uint64)
+    d = to_dev(torch_cuda, x)
+    nb.transpose_u64(d, d, n, n)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == x.reshape(n, n).T.reshape(-1)).all()
+    assert nb.device_errors() == 0
+
+
+@pytest.mark.parametrize("lg", [10, 12, 16, 22, 24])
+def test_bit_reverse_tma_and_unaligned(torch_cuda, lg):
+    """Bit reversal from 2^10 on runs on TMA tile pairs; the same array 8 bytes
+    off a 16-byte boundary takes the plain tiled kernel; both match the oracle."""
+    n = 1 << lg
+    x = np.random.default_rng(lg + 100).integers(0, 1 << 63, n, dtype=np.uint64)
+    want = O.bit_reverse(x)
+    d = to_dev(torch_cuda, x)
+    nb.bit_reverse_u64(d, n)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == want).all()
+    buf = to_dev(torch_cuda, np.concatenate([np.zeros(1, np.uint64), x]))
+    nb.bit_reverse_u64(buf[1:], n)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(buf[1:], np.uint64) == want).all()
+    assert nb.device_errors() == 0
+
+
 def test_pointwise_and_bitrev(torch_cuda):
     n = 1 << 12
     for q in (BABYBEAR, Q60):
