@@ -54,7 +54,9 @@ NTTB_API const char* nttb_last_error(void);
  * (bit 0: an INT8-engine mbarrier wait ran out of budget, bit 1: a wait on
  * another CTA of an INT8 cluster did, bit 2: an uneven-batch queue
  * dependency wait did, bit 3: a batch tensor tile's wait on its MMA or image
- * copy did; the work item ran on regardless and its output is wrong).  Every
+ * copy did; the work item ran on regardless and its output is wrong; bit 4:
+ * a TMA tile load of a transpose or bit reversal did not land, and that CTA
+ * stopped storing).  Every
  * such wait gives up after about 2 s of device time.  Reads after a device
  * synchronize; clear != 0 resets them. */
 NTTB_API int nttb_device_errors(uint32_t* flags, int clear);
@@ -108,14 +110,17 @@ NTTB_API int nttb_u64_four_step(const nttb_plan* plan, uint64_t* d_data, int inv
 NTTB_API int nttb_u64_rowmaj_forward(const nttb_plan* plan, uint64_t* d_data, void* stream);
 /* d_dst[c*rows + r] = d_src[r*cols + c].  Replaces rowmaj_to_pretransposed
  * (rows=N1, cols=N2) and rowmaj_from_pretransposed (rows=N2, cols=N1),
- * src/ntt_optimized.cu:922-934.  d_dst may equal d_src only for a square matrix. */
+ * src/ntt_optimized.cu:922-934.  d_dst may equal d_src only for a square matrix.
+ * rows and cols multiples of 32 with 16-byte aligned arrays run on TMA tiles;
+ * other shapes on a plain tiled kernel. */
 NTTB_API int nttb_u64_transpose(uint64_t* d_dst, const uint64_t* d_src, uint64_t rows, uint64_t cols, void* stream);
 /* d_out[i] = d_a[i] * d_b[i] mod q, i < n.  Replaces poly_multiply_ntt
  * (src/ntt_basic.cu:391-409). */
 NTTB_API int nttb_u64_pointwise_mul(const nttb_plan* plan, uint64_t* d_out, const uint64_t* d_a, const uint64_t* d_b,
                            void* stream);
 /* In-place bit-reversal permutation.  Replaces bit_reverse_permute
- * (src/ntt_basic.cu:259-265). */
+ * (src/ntt_basic.cu:259-265).  From n = 2^10 on, with a 16-byte aligned
+ * array, it runs on TMA tile pairs. */
 NTTB_API int nttb_u64_bit_reverse(uint64_t* d_data, uint64_t n, void* stream);
 
 /* ------------------------------------------ RNS batches of uint32 residues
