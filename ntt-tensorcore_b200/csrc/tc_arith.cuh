@@ -38,6 +38,11 @@ __device__ __forceinline__ uint32_t mont_lazy(uint32_t a, uint32_t b, uint32_t q
     return redc64(mad_wide(a, b, 0ull), q, qinv);
 }
 __device__ __forceinline__ uint32_t canon(uint32_t x, uint32_t q) { return x >= q ? x - q : x; }
+// a * b mod q in [0, 2q) for any a < 2^32 and b < q, given bs = floor(b * 2^32 / q)
+// (Shoup's product with a precomputed quotient): three single-width multiplies.
+__device__ __forceinline__ uint32_t shoup_lazy(uint32_t a, uint32_t b, uint32_t bs, uint32_t q) {
+    return a * b - __umulhi(a, bs) * q;
+}
 
 // Issues the K = 256-byte contraction (8 MMAs of K = 32, M = 128) into TMEM
 // columns [tmem, tmem + N).  A and B are K-major SW128 with two 128-byte K

@@ -94,11 +94,15 @@ constexpr uint32_t kBufBytes = 2 * kTileBytes;
 constexpr uint32_t kImgSlots = 3;            // 0: stage A forward, 1: inverse (A and B), 2: stage B forward
 constexpr uint32_t kBlobImg = 2 * kMatBytes16;
 // twiddle table of one direction (words): a_st2[2048] a_ratio[1024] b_st2[32]
-// b_ratio[16] q qinv (pad to 16 bytes); the forward table, then the inverse
+// b_ratio[16] q qinv (pad to 16 bytes) a_step[2048] b_step[32]; the forward
+// table, then the inverse
 //   stage A:  t_A(b, d)   = a_st2[2b + h] * a_ratio[b]^(d - 32h),   d in [32h, 32h + 32)
 //   stage B1: t_B1(b2, d2) = b_st2[2 b2 + h] * b_ratio[b2]^(d2 - 32h)  (Montgomery form)
+// a_step / b_step: (ratio^2 mod q, floor(ratio^2 * 2^32 / q)) in plain form,
+// the Shoup operands of the twiddle chains' step (every second output).
 constexpr uint32_t kTabAst = 0, kTabArat = 2048, kTabBst = 3072, kTabBrat = 3104, kTabQ = 3120;
-constexpr uint32_t kTabWords = 3124;
+constexpr uint32_t kTabAstep = 3124, kTabBstep = 5172;
+constexpr uint32_t kTabWords = 5204;
 constexpr uint32_t kBlobTab = kBlobImg + kImgSlots * kMatBytes64;
 constexpr uint32_t kBlobBytes = kBlobTab + 2 * kTabWords * 4;
 static_assert(kBlobBytes % 16 == 0, "per-limb blobs must stay 16-byte aligned");
@@ -227,9 +231,8 @@ __device__ __forceinline__ uint32_t lane_cols(const Cl& c) {
 // (rows 16 j..), staged at piece slot (j / 4, 4 (j % 4) + P) of tile w'.
 template <class Gate, class PartDone>
 __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qinv, uint32_t ratio, uint32_t start,
-                                           Gate gate, PartDone part_done) {
+                                           uint2 step, Gate gate, PartDone part_done) {
     const uint32_t m = c.quarter * 32u + c.lane, b = 128u * (2u * c.rank + c.w) + beta(m);
-    const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
     uint32_t tw_e = start;                                      // d = 32h
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
     const uint32_t col = lane_cols(c);
@@ -248,8 +251,8 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
                 y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
                 y[8 * sub + i + 1] =
                     mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
-                tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
-                tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+                tw_e = canon(shoup_lazy(tw_e, step.x, step.y, q), q);
+                tw_o = canon(shoup_lazy(tw_o, step.x, step.y, q), q);
             }
         }
         if (part == 0) gate();
@@ -268,9 +271,8 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
 // level 1), SW64, row r + 8 (d2 / 16) + 32 (d2 % 16), K word b2.
 template <class Gate>
 __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qinv, uint32_t ratio, uint32_t start,
-                                            Gate gate) {
+                                            uint2 step, Gate gate) {
     const uint32_t mv = c.quarter * 32u + c.lane, b2 = mv & 15u, r = mv >> 4;
-    const uint32_t r2 = canon(mont_lazy(ratio, ratio, q, qinv), q);
     uint32_t tw_e = start;
     uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
     const uint32_t col = lane_cols(c);
@@ -288,8 +290,8 @@ __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qi
                 y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
                 y[8 * sub + i + 1] =
                     mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
-                tw_e = canon(mont_lazy(tw_e, r2, q, qinv), q);
-                tw_o = canon(mont_lazy(tw_o, r2, q, qinv), q);
+                tw_e = canon(shoup_lazy(tw_e, step.x, step.y, q), q);
+                tw_o = canon(shoup_lazy(tw_o, step.x, step.y, q), q);
             }
         }
         if (part == 0) gate();
@@ -435,6 +437,7 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             // this thread's twiddle inputs, loaded now so the latency hides
             // behind the operand wait and the MMA
             uint32_t q, qinv, ratio, start;
+            uint2 step;
             {
                 const uint32_t* T = reinterpret_cast<const uint32_t*>(limb_blob + kBlobTab) + S.dir * kTabWords;
                 q = __ldg(T + kTabQ);
@@ -443,10 +446,12 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                     const uint32_t b = 128u * (2u * c.rank + c.w) + beta(c.quarter * 32u + c.lane);
                     ratio = __ldg(T + kTabArat + b);
                     start = __ldg(T + kTabAst + 2 * b + c.h);
+                    step = __ldg(reinterpret_cast<const uint2*>(T + kTabAstep) + b);
                 } else {
                     const uint32_t b2 = c.lane & 15u;  // row m' = 32 quarter + lane: b2 = m' % 16
                     ratio = __ldg(T + kTabBrat + b2);
                     start = __ldg(T + kTabBst + 2 * b2 + c.h);
+                    step = __ldg(reinterpret_cast<const uint2*>(T + kTabBstep) + b2);
                 }
             }
             if (s > 0) {  // this stage's 64 KB operand arrived from the four CTAs
@@ -488,10 +493,10 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                     send_pieces(c, S.kind, 2u * c.h + part, S.kind == 0 ? kBarIn1 : kBarIn0);
             };
             if (S.kind == 0) {
-                epilogue_a(c, q, qinv, ratio, start, mma_gate, part_done);
+                epilogue_a(c, q, qinv, ratio, start, step, mma_gate, part_done);
                 ph_mma ^= 1u;
             } else {
-                epilogue_b1(c, q, qinv, ratio, start, mma_gate);
+                epilogue_b1(c, q, qinv, ratio, start, step, mma_gate);
                 ph_mma ^= 1u;
                 tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
@@ -586,11 +591,17 @@ void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_
         t[kTabAst + 2 * b] = h_to_mont32(start_a[b], q);
         t[kTabAst + 2 * b + 1] = h_to_mont32(h_mulmod(start_a[b], h_powmod(ratio_a[b], 32, q), q), q);
         t[kTabArat + b] = h_to_mont32(ratio_a[b], q);
+        const uint64_t r2 = h_mulmod(ratio_a[b], ratio_a[b], q);
+        t[kTabAstep + 2 * b] = (uint32_t)r2;
+        t[kTabAstep + 2 * b + 1] = (uint32_t)((r2 << 32) / q);
     }
     for (uint32_t b2 = 0; b2 < 16; b2++) {
         t[kTabBst + 2 * b2] = h_to_mont32(1, q);
         t[kTabBst + 2 * b2 + 1] = h_to_mont32(h_powmod(ratio_b[b2], 32, q), q);
         t[kTabBrat + b2] = h_to_mont32(ratio_b[b2], q);
+        const uint64_t r2 = h_mulmod(ratio_b[b2], ratio_b[b2], q);
+        t[kTabBstep + 2 * b2] = (uint32_t)r2;
+        t[kTabBstep + 2 * b2 + 1] = (uint32_t)((r2 << 32) / q);
     }
 }
 
