@@ -67,6 +67,11 @@ struct M32 {
         uint32_t r = (uint32_t)((t + (uint64_t)m * q) >> 32);
         return r >= q ? r - q : r;
     }
+    // Shoup product a * w mod q for any a and w < q, ws = floor(w * 2^32 / q); canonical.
+    __device__ __forceinline__ uint32_t mul_shoup(uint32_t a, uint32_t w, uint32_t ws) const {
+        const uint32_t r = a * w - __umulhi(a, ws) * q;  // in [0, 2q)
+        return r >= q ? r - q : r;
+    }
     __device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b) const {
         uint32_t s = a + b;
         return s >= q ? s - q : s;
@@ -92,6 +97,11 @@ struct M64 {
         uint64_t m = lo * qinv;
         uint64_t r = hi + (uint64_t)(((unsigned __int128)m * q) >> 64) + (lo != 0);
 #endif
+        return r >= q ? r - q : r;
+    }
+    // Shoup product a * w mod q for any a and w < q, ws = floor(w * 2^64 / q); canonical.
+    __device__ __forceinline__ uint64_t mul_shoup(uint64_t a, uint64_t w, uint64_t ws) const {
+        const uint64_t r = a * w - __umul64hi(a, ws) * q;  // in [0, 2q)
         return r >= q ? r - q : r;
     }
     __device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) const {

@@ -79,6 +79,18 @@ static void fill_powers(E* dst, uint64_t base, uint64_t start, uint64_t n, uint6
     }
 }
 
+// Shoup pairs of base^e, e < count: the plain power and floor(power * 2^bits / q).
+template <class E>
+static void fill_shoup(E* dst, uint64_t base, uint64_t count, uint64_t q) {
+    uint64_t x = 1 % q;
+    for (uint64_t e = 0; e < count; e++) {
+        dst[2 * e] = (E)x;
+        if constexpr (sizeof(E) == 4) dst[2 * e + 1] = (E)((x << 32) / q);
+        else dst[2 * e + 1] = (E)(((unsigned __int128)x << 64) / q);
+        x = h_mulmod(x, base, q);
+    }
+}
+
 template <class A, class PlanT, class ToMont>
 static int build_common(PlanT* p, uint32_t log_n, const uint64_t* moduli, uint32_t n_limbs, bool negacyclic,
                         uint64_t qmax, ToMont tm, std::string* why) {
@@ -94,8 +106,10 @@ static int build_common(PlanT* p, uint32_t log_n, const uint64_t* moduli, uint32
         if (moduli[l] >= qmax) { *why = "modulus " + std::to_string(moduli[l]) + " too large for this path"; return 1; }
         if (!make_limb_host(moduli[l], n, negacyclic, &p->limbs[l], why)) return 1;
     }
+    // omega^e, omega^-e (, psi^e, n^-1 psi^-e) in Montgomery form, then the
+    // Shoup pairs of omega^e and omega^-e for e < n / 2 (n words each)
     const uint32_t tables = negacyclic ? 4 : 2;
-    const size_t per_limb = (size_t)tables * n;
+    const size_t per_limb = (size_t)(tables + 2) * n;
     std::vector<E> host(per_limb * n_limbs);
     std::vector<LimbDev<A>> devs(n_limbs);
     E* d_tables = nullptr;
@@ -117,6 +131,10 @@ static int build_common(PlanT* p, uint32_t log_n, const uint64_t* moduli, uint32
             dv.psi = d + 2 * n;
             dv.psi_inv = d + 3 * n;
         }
+        fill_shoup(h + (size_t)tables * n, L.omega, n / 2, q);
+        fill_shoup(h + (size_t)(tables + 1) * n, L.omega_inv, n / 2, q);
+        dv.tw_sh = d + (size_t)tables * n;
+        dv.tw_inv_sh = d + (size_t)(tables + 1) * n;
         dv.ninv_m = (E)tm(L.n_inv, q);
         devs[l] = dv;
     }

@@ -20,6 +20,10 @@ struct LimbDev {
     const typename A::elem* tw_inv;    // omega^-e * R,  e < n
     const typename A::elem* psi;       // psi^e * R,     e < n (negacyclic only)
     const typename A::elem* psi_inv;   // n^-1 psi^-e R, e < n (negacyclic only)
+    // Shoup pairs for the radix-2 butterflies: [2e] = omega^e (plain form),
+    // [2e + 1] = floor(omega^e * 2^bits / q), e < n / 2 (bits = 32 or 64)
+    const typename A::elem* tw_sh;
+    const typename A::elem* tw_inv_sh;
 };
 
 // Host view of one modulus at one transform size.

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     const uint32_t stride = tile_stride<E>(L);
     constexpr uint32_t kPad = pad_shift<E>();
     E* t = reinterpret_cast<E*>(smem_raw);
-    E* tws = t + (size_t)V * stride;
+    E* tws = t + (((size_t)V * stride + 1) & ~(size_t)1);  // pair-aligned
 
     const uint32_t limb = blockIdx.y, poly = blockIdx.z;
     const uint32_t v0 = blockIdx.x * V;  // first vector of this tile
@@ -53,10 +53,17 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     const uint32_t total = V * L;
     const uint32_t flags = args.flags;
 
-    // powers of the length-L root: tws[k] = root_L^k, k < L/2
+    // Shoup pairs of the length-L root: tws[2k] = root_L^k (plain form),
+    // tws[2k + 1] its quotient, k < L/2; the butterflies multiply by them
+    // with one high and two low products (the Montgomery product takes two
+    // of each), giving the same canonical Montgomery-form results
     {
         const uint32_t step = args.n >> lgL;
-        for (uint32_t k = threadIdx.x; k < (L >> 1); k += blockDim.x) tws[k] = tw[(uint64_t)k * step];
+        const E* sh = args.inverse ? ld.tw_inv_sh : ld.tw_sh;
+        for (uint32_t k = threadIdx.x; k < (L >> 1); k += blockDim.x) {
+            tws[2 * k] = sh[2 * (uint64_t)k * step];
+            tws[2 * k + 1] = sh[2 * (uint64_t)k * step + 1];
+        }
     }
 
     constexpr bool kDIT = (MODE == MODE_COL || MODE == MODE_GATHER_T);
@@ -75,33 +82,49 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         psi_step = e < args.n ? ld.psi[e] : tw[0];  // tw[0] = 1 (Montgomery form)
     }
     // ---- load ----
-    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        uint32_t v, j;
-        uint64_t pos;
+    // Batches of kLoadBatch elements per thread: the global loads of a batch
+    // are issued together, then twisted and stored to shared memory in the
+    // same order (the twist chains advance per element).
+    auto load_pos = [&](uint32_t idx, uint32_t& v, uint32_t& j) -> uint64_t {
         if (kDIT) { v = idx & (V - 1); j = idx >> lgV; } else { v = idx >> lgL; j = idx & (L - 1); }
         const uint32_t vec = v0 + v;
-        if (MODE == MODE_COL) {
-            pos = (uint64_t)j * N2 + vec;
-        } else if (MODE == MODE_ROW_NAT) {
-            pos = (uint64_t)vec * N2 + j;
-        } else if (MODE == MODE_GATHER_T) {
+        if (MODE == MODE_COL) return (uint64_t)j * N2 + vec;
+        if (MODE == MODE_ROW_NAT) return (uint64_t)vec * N2 + j;
+        if (MODE == MODE_GATHER_T) {
             const uint64_t m = (uint64_t)vec * L + j;  // index into the transposed view
-            pos = (m & (N1 - 1)) * N2 + (m >> lgN1);
-        } else {
-            pos = (uint64_t)vec * L + j;
+            return (m & (N1 - 1)) * N2 + (m >> lgN1);
         }
-        E x = (E)src[pos];
-        if (flags & F_PRE_PSI) {
-            if (chain) {
-                x = ar.mul(x, psi_cur);
-                psi_cur = ar.mul(psi_cur, psi_step);
-            } else {
-                x = ar.mul(x, ld.psi[pos]);
+        return (uint64_t)vec * L + j;
+    };
+    constexpr uint32_t kLoadBatch = 8;
+    for (uint32_t idx0 = threadIdx.x; idx0 < total; idx0 += blockDim.x * kLoadBatch) {
+        S raw[kLoadBatch];
+#pragma unroll
+        for (uint32_t u = 0; u < kLoadBatch; u++) {
+            const uint32_t idx = idx0 + u * blockDim.x;
+            uint32_t v, j;
+            if (idx < total) raw[u] = src[load_pos(idx, v, j)];
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kLoadBatch; u++) {
+            const uint32_t idx = idx0 + u * blockDim.x;
+            if (idx >= total) break;
+            uint32_t v, j;
+            const uint64_t pos = load_pos(idx, v, j);
+            const uint32_t vec = v0 + v;
+            E x = (E)raw[u];
+            if (flags & F_PRE_PSI) {
+                if (chain) {
+                    x = ar.mul(x, psi_cur);
+                    psi_cur = ar.mul(psi_cur, psi_step);
+                } else {
+                    x = ar.mul(x, ld.psi[pos]);
+                }
             }
+            if (flags & F_PRE_TW) x = ar.mul(x, tw[((uint64_t)j * vec) & nmask]);
+            const uint32_t jj = kDIT ? bitrev(j, (int)lgL) : j;
+            t[(size_t)v * stride + jj + (jj >> kPad)] = x;
         }
-        if (flags & F_PRE_TW) x = ar.mul(x, tw[((uint64_t)j * vec) & nmask]);
-        const uint32_t jj = kDIT ? bitrev(j, (int)lgL) : j;
-        t[(size_t)v * stride + jj + (jj >> kPad)] = x;
     }
     __syncthreads();
 
@@ -133,8 +156,8 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
 #pragma unroll
                     for (uint32_t k = 0; k < kGN; k++) {
                         if ((k & half) || k + half >= nk) continue;
-                        const uint32_t p = low + ((k & (half - 1)) << s0);
-                        const E y = ar.mul(x[k + half], tws[p << (lgL - 1 - st)]);
+                        const uint32_t p = (low + ((k & (half - 1)) << s0)) << (lgL - 1 - st);
+                        const E y = ar.mul_shoup(x[k + half], tws[2 * p], tws[2 * p + 1]);
                         const E u0 = x[k];
                         x[k] = ar.add(u0, y);
                         x[k + half] = ar.sub(u0, y);
@@ -173,10 +196,10 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
 #pragma unroll
                     for (uint32_t k = 0; k < kGN; k++) {
                         if ((k & half) || k + half >= nk) continue;
-                        const uint32_t p = low + ((k & (half - 1)) << s_lo);
+                        const uint32_t p = (low + ((k & (half - 1)) << s_lo)) << (lgL - 1 - st);
                         const E u0 = x[k], y = x[k + half];
                         x[k] = ar.add(u0, y);
-                        x[k + half] = ar.mul(ar.sub(u0, y), tws[p << (lgL - 1 - st)]);
+                        x[k + half] = ar.mul_shoup(ar.sub(u0, y), tws[2 * p], tws[2 * p + 1]);
                     }
                 }
 #pragma unroll
@@ -232,7 +255,7 @@ template <class S, class A>
 int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t n_vectors,
                 uint32_t n_polys, cudaStream_t s) {
     using E = typename A::elem;
-    const size_t smem = ((size_t)a.vec_per_tile * tile_stride<E>(a.len) + (a.len >> 1) + 1) * sizeof(E);
+    const size_t smem = ((((size_t)a.vec_per_tile * tile_stride<E>(a.len) + 1) & ~(size_t)1) + a.len + 2) * sizeof(E);
     dim3 grid(n_vectors / a.vec_per_tile, a.n_limbs, n_polys);
     if (grid.x == 0 || n_polys > 65535 || a.n_limbs > 65535) return 1;
     void (*k)(PassArgs, const LimbDev<A>*) = nullptr;
@@ -250,14 +273,15 @@ int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
-inline uint32_t ilog2u(uint64_t x) { uint32_t l = 0; while ((1ull << l) < x) l++; return l; }
-
 // Vectors per tile: as many as the shared-memory tile holds, fewer while the
 // pass would have under ~1024 tiles (a single large polynomial otherwise
-// leaves most SMs idle).
+// leaves most SMs idle), but at least two: column passes read and write
+// `V` consecutive words per row, and one word per 32-byte sector cost more
+// than the extra tiles gain (one 2^20 polynomial mod the 60-bit prime:
+// 15.4 -> 17.9 G coefficient-transforms/s with the floor at two).
 inline uint32_t tile_vectors(uint32_t e_max, uint32_t len, uint32_t n_vectors, uint32_t units) {
     uint32_t v = e_max / len < n_vectors ? e_max / len : n_vectors;
-    while (v > 1 && (uint64_t)(n_vectors / v) * units < 1024) v >>= 1;
+    while (v > 2 && (uint64_t)(n_vectors / v) * units < 1024) v >>= 1;
     return v;
 }
 
