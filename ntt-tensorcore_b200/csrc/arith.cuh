@@ -58,6 +58,7 @@ inline uint64_t h_to_mont64(uint64_t x, uint64_t q) {
 // ---- device arithmetic ------------------------------------------------------
 struct M32 {
     using elem = uint32_t;
+    static constexpr bool kLazy = false;  // 4q does not fit 32 bits for 31-bit moduli
     uint32_t q, qinv;  // qinv = -q^-1 mod 2^32
 
     // Montgomery product: a * b * 2^-32 mod q, for a*b < q * 2^32; canonical.
@@ -84,6 +85,9 @@ struct M32 {
 
 struct M64 {
     using elem = uint64_t;
+    // q < 2^62: values in [0, 4q) fit a word, so butterflies may run lazily
+    // (D. Harvey, "Faster arithmetic for number-theoretic transforms", 2014)
+    static constexpr bool kLazy = true;
     uint64_t q, qinv;  // qinv = -q^-1 mod 2^64, q < 2^62
 
     __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) const {
@@ -101,8 +105,19 @@ struct M64 {
     }
     // Shoup product a * w mod q for any a and w < q, ws = floor(w * 2^64 / q); canonical.
     __device__ __forceinline__ uint64_t mul_shoup(uint64_t a, uint64_t w, uint64_t ws) const {
-        const uint64_t r = a * w - __umul64hi(a, ws) * q;  // in [0, 2q)
+        const uint64_t r = mul_shoup_lazy(a, w, ws);
         return r >= q ? r - q : r;
+    }
+    // The same product in [0, 2q).
+    __device__ __forceinline__ uint64_t mul_shoup_lazy(uint64_t a, uint64_t w, uint64_t ws) const {
+        return a * w - __umul64hi(a, ws) * q;
+    }
+    // x in [0, 4q) -> [0, 2q)
+    __device__ __forceinline__ uint64_t below2q(uint64_t x) const { return x >= 2 * q ? x - 2 * q : x; }
+    // x in [0, 4q) -> canonical
+    __device__ __forceinline__ uint64_t canon4(uint64_t x) const {
+        x = below2q(x);
+        return x >= q ? x - q : x;
     }
     __device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) const {
         uint64_t s = a + b;

@@ -157,10 +157,18 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
                     for (uint32_t k = 0; k < kGN; k++) {
                         if ((k & half) || k + half >= nk) continue;
                         const uint32_t p = (low + ((k & (half - 1)) << s0)) << (lgL - 1 - st);
-                        const E y = ar.mul_shoup(x[k + half], tws[2 * p], tws[2 * p + 1]);
-                        const E u0 = x[k];
-                        x[k] = ar.add(u0, y);
-                        x[k + half] = ar.sub(u0, y);
+                        if constexpr (A::kLazy) {
+                            // values in [0, 4q): u0 to [0, 2q), y = w x in [0, 2q)
+                            const E u0 = ar.below2q(x[k]);
+                            const E y = ar.mul_shoup_lazy(x[k + half], tws[2 * p], tws[2 * p + 1]);
+                            x[k] = u0 + y;
+                            x[k + half] = u0 - y + 2 * ar.q;
+                        } else {
+                            const E y = ar.mul_shoup(x[k + half], tws[2 * p], tws[2 * p + 1]);
+                            const E u0 = x[k];
+                            x[k] = ar.add(u0, y);
+                            x[k + half] = ar.sub(u0, y);
+                        }
                     }
                 }
 #pragma unroll
@@ -198,8 +206,14 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
                         if ((k & half) || k + half >= nk) continue;
                         const uint32_t p = (low + ((k & (half - 1)) << s_lo)) << (lgL - 1 - st);
                         const E u0 = x[k], y = x[k + half];
-                        x[k] = ar.add(u0, y);
-                        x[k + half] = ar.mul_shoup(ar.sub(u0, y), tws[2 * p], tws[2 * p + 1]);
+                        if constexpr (A::kLazy) {
+                            // values in [0, 2q)
+                            x[k] = ar.below2q(u0 + y);
+                            x[k + half] = ar.mul_shoup_lazy(u0 - y + 2 * ar.q, tws[2 * p], tws[2 * p + 1]);
+                        } else {
+                            x[k] = ar.add(u0, y);
+                            x[k + half] = ar.mul_shoup(ar.sub(u0, y), tws[2 * p], tws[2 * p + 1]);
+                        }
                     }
                 }
 #pragma unroll
@@ -226,6 +240,7 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
         const uint32_t vec = v0 + v;
         const uint32_t kk = kDIT ? k : bitrev(k, (int)lgL);
         E x = t[(size_t)v * stride + kk + (kk >> kPad)];
+        if constexpr (A::kLazy) x = ar.canon4(x);  // lazy butterflies leave [0, 4q)
         uint64_t pos;
         if (MODE == MODE_COL) {
             pos = (flags & F_STORE_T) ? (uint64_t)vec * N1 + k : (uint64_t)k * N2 + vec;
