@@ -79,15 +79,21 @@ static void fill_powers(E* dst, uint64_t base, uint64_t start, uint64_t n, uint6
     }
 }
 
-// Shoup pairs of base^e, e < count: the plain power and floor(power * 2^bits / q).
+// Shoup pairs of the roots of each length L = 2^l <= n, level by level:
+// pairs 2^(l-1) - 1 + k = (root_L^k, floor(root_L^k * 2^bits / q)), k < L/2,
+// root_L = root_n^(n/L); n - 1 pairs in all.
 template <class E>
-static void fill_shoup(E* dst, uint64_t base, uint64_t count, uint64_t q) {
-    uint64_t x = 1 % q;
-    for (uint64_t e = 0; e < count; e++) {
-        dst[2 * e] = (E)x;
-        if constexpr (sizeof(E) == 4) dst[2 * e + 1] = (E)((x << 32) / q);
-        else dst[2 * e + 1] = (E)(((unsigned __int128)x << 64) / q);
-        x = h_mulmod(x, base, q);
+static void fill_shoup_levels(E* dst, uint64_t root_n, uint32_t log_n, uint64_t q) {
+    for (uint32_t l = 1; l <= log_n; l++) {
+        const uint64_t step = h_powmod(root_n, 1ull << (log_n - l), q);
+        E* lvl = dst + 2 * ((1ull << (l - 1)) - 1);
+        uint64_t x = 1 % q;
+        for (uint64_t k = 0; k < (1ull << (l - 1)); k++) {
+            lvl[2 * k] = (E)x;
+            if constexpr (sizeof(E) == 4) lvl[2 * k + 1] = (E)((x << 32) / q);
+            else lvl[2 * k + 1] = (E)(((unsigned __int128)x << 64) / q);
+            x = h_mulmod(x, step, q);
+        }
     }
 }
 
@@ -107,9 +113,9 @@ static int build_common(PlanT* p, uint32_t log_n, const uint64_t* moduli, uint32
         if (!make_limb_host(moduli[l], n, negacyclic, &p->limbs[l], why)) return 1;
     }
     // omega^e, omega^-e (, psi^e, n^-1 psi^-e) in Montgomery form, then the
-    // Shoup pairs of omega^e and omega^-e for e < n / 2 (n words each)
+    // level-by-level Shoup pairs of the forward and inverse roots (2n words each)
     const uint32_t tables = negacyclic ? 4 : 2;
-    const size_t per_limb = (size_t)(tables + 2) * n;
+    const size_t per_limb = (size_t)(tables + 4) * n;
     std::vector<E> host(per_limb * n_limbs);
     std::vector<LimbDev<A>> devs(n_limbs);
     E* d_tables = nullptr;
@@ -131,10 +137,10 @@ static int build_common(PlanT* p, uint32_t log_n, const uint64_t* moduli, uint32
             dv.psi = d + 2 * n;
             dv.psi_inv = d + 3 * n;
         }
-        fill_shoup(h + (size_t)tables * n, L.omega, n / 2, q);
-        fill_shoup(h + (size_t)(tables + 1) * n, L.omega_inv, n / 2, q);
+        fill_shoup_levels(h + (size_t)tables * n, L.omega, log_n, q);
+        fill_shoup_levels(h + (size_t)(tables + 2) * n, L.omega_inv, log_n, q);
         dv.tw_sh = d + (size_t)tables * n;
-        dv.tw_inv_sh = d + (size_t)(tables + 1) * n;
+        dv.tw_inv_sh = d + (size_t)(tables + 2) * n;
         dv.ninv_m = (E)tm(L.n_inv, q);
         devs[l] = dv;
     }

@@ -20,8 +20,10 @@ struct LimbDev {
     const typename A::elem* tw_inv;    // omega^-e * R,  e < n
     const typename A::elem* psi;       // psi^e * R,     e < n (negacyclic only)
     const typename A::elem* psi_inv;   // n^-1 psi^-e R, e < n (negacyclic only)
-    // Shoup pairs for the radix-2 butterflies: [2e] = omega^e (plain form),
-    // [2e + 1] = floor(omega^e * 2^bits / q), e < n / 2 (bits = 32 or 64)
+    // Shoup pairs of the radix-2 butterflies, level by level: the roots of
+    // length L = 2^l sit at pairs 2^(l-1) - 1 .. 2^l - 2 (k < L/2), each pair
+    // root_L^k (plain form) and floor(root_L^k * 2^bits / q) (bits = 32 or 64),
+    // so a pass of length L reads one contiguous run
     const typename A::elem* tw_sh;
     const typename A::elem* tw_inv_sh;
 };

@@ -57,13 +57,9 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     // tws[2k + 1] its quotient, k < L/2; the butterflies multiply by them
     // with one high and two low products (the Montgomery product takes two
     // of each), giving the same canonical Montgomery-form results
-    {
-        const uint32_t step = args.n >> lgL;
-        const E* sh = args.inverse ? ld.tw_inv_sh : ld.tw_sh;
-        for (uint32_t k = threadIdx.x; k < (L >> 1); k += blockDim.x) {
-            tws[2 * k] = sh[2 * (uint64_t)k * step];
-            tws[2 * k + 1] = sh[2 * (uint64_t)k * step + 1];
-        }
+    if (L >= 2) {  // a pass of length 1 has no butterflies (and no level 0)
+        const E* sh = (args.inverse ? ld.tw_inv_sh : ld.tw_sh) + 2 * (size_t)((L >> 1) - 1);  // level lgL
+        for (uint32_t k = threadIdx.x; k < L; k += blockDim.x) tws[k] = sh[k];
     }
 
     constexpr bool kDIT = (MODE == MODE_COL || MODE == MODE_GATHER_T);

@@ -91,8 +91,9 @@ def test_wide_modulus_through_u64_plan(torch_cuda):
     assert (run_u64(torch_cuda, plan2, x) == O.ntt(x, 4293918721)).all()
 
 
-@pytest.mark.parametrize("n", [128, 4096, 8192, 16384, 1 << 16])
+@pytest.mark.parametrize("n", [64, 128, 4096, 8192, 16384, 1 << 16])
 def test_four_step_matches_reference_map(torch_cuda, n):
+    """n = 64 makes the second pass of length 1 (n1 = 64, n2 = 1)."""
     x = rand(n, BABYBEAR, n)
     plan = nb.Plan(n, BABYBEAR)
     d = to_dev(torch_cuda, x)
