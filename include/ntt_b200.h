@@ -108,6 +108,14 @@ NTTB_API int nttb_u64_four_step(const nttb_plan* plan, uint64_t* d_data, int inv
 /* Pre-transposed forward NTT for n == 4096, plain forward otherwise.
  * Replaces ntt_forward_rowmaj (src/ntt_optimized.cu:940-965). */
 NTTB_API int nttb_u64_rowmaj_forward(const nttb_plan* plan, uint64_t* d_data, void* stream);
+/* The RowMaj pre-transposed layout for every n and both directions: d_data
+ * holds pre[b*n1 + a] = x[a*n2 + b] (n2 = n / n1, the layout of
+ * rowmaj_to_pretransposed, src/ntt_optimized.cu:893-895, 922-934) and
+ * receives the transform in the same layout, in place.  n1 a power of two
+ * <= n; nttb_u64_rowmaj_forward is the case n = 4096, n1 = 64, forward.
+ * Runs as a TMA transpose, the transform, and the transpose back. */
+NTTB_API int nttb_u64_pretransposed_transform(const nttb_plan* plan, uint64_t* d_data, uint64_t n1, int inverse,
+                                              void* stream);
 /* d_dst[c*rows + r] = d_src[r*cols + c].  Replaces rowmaj_to_pretransposed
  * (rows=N1, cols=N2) and rowmaj_from_pretransposed (rows=N2, cols=N1),
  * src/ntt_optimized.cu:922-934.  d_dst may equal d_src only for a square matrix.

@@ -461,12 +461,19 @@ int nttb_u64_transpose(uint64_t* dst, const uint64_t* src, uint64_t rows, uint64
 int nttb_u64_rowmaj_forward(const nttb_plan* P, uint64_t* d, void* stream) {
     if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "rowmaj_forward: null argument");
     if (P->n != 4096) return nttb_u64_transform(P, d, 1, 0, NTTB_ENGINE_AUTO, stream);
-    // pre-transposed (64 x 64) in -> canonical -> forward -> pre-transposed out
-    int rc = nttb_u64_transpose(P->d_scratch, d, 64, 64, stream);
+    return nttb_u64_pretransposed_transform(P, d, 64, 0, stream);
+}
+
+int nttb_u64_pretransposed_transform(const nttb_plan* P, uint64_t* d, uint64_t n1, int inverse, void* stream) {
+    if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "pretransposed_transform: null argument");
+    if (!pow2(n1) || n1 > P->n) return fail(NTTB_ERR_INVALID_ARG, "pretransposed_transform: n1 must be a power of two <= n");
+    const uint64_t n2 = P->n / n1;
+    // pre[b * n1 + a] = canon[a * n2 + b]: canon is pre (n2 x n1) transposed
+    int rc = nttb_u64_transpose(P->d_scratch, d, n2, n1, stream);
     if (rc) return rc;
-    rc = nttb_u64_transform(P, P->d_scratch, 1, 0, NTTB_ENGINE_AUTO, stream);
+    rc = nttb_u64_transform(P, P->d_scratch, 1, inverse, NTTB_ENGINE_AUTO, stream);
     if (rc) return rc;
-    return nttb_u64_transpose(d, P->d_scratch, 64, 64, stream);
+    return nttb_u64_transpose(d, P->d_scratch, n1, n2, stream);
 }
 
 int nttb_u64_pointwise_mul(const nttb_plan* P, uint64_t* out, const uint64_t* a, const uint64_t* b, void* stream) {

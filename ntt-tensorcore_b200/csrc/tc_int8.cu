@@ -54,6 +54,7 @@
 // threads.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -706,10 +707,14 @@ void launch_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, uint32_t 
     cfg.numAttrs = 1;
 }
 
-// Clusters of 4 that fit on the device at once (one CTA per SM).
+// Clusters of 4 that fit on the current device at once (one CTA per SM).
+// The shared-memory attribute and the answer are per device.
 int max_clusters() {
-    static int cached = 0;
-    if (cached) return cached;
+    static std::atomic<int> cached[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::atomic<int>& slot = cached[dev & 63];
+    if (const int c = slot.load()) return c;
     cudaFuncSetAttribute(int8_cluster_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem);
     cudaLaunchConfig_t cfg;
     cudaLaunchAttribute attr[1];
@@ -717,13 +722,12 @@ int max_clusters() {
     int n = 0;
     if (cudaOccupancyMaxActiveClusters(&n, int8_cluster_n16, &cfg) != cudaSuccess || n < 1) {
         cudaGetLastError();
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
+        int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         n = sms / (int)kClCtas / 2 > 0 ? sms / (int)kClCtas / 2 : 1;
     }
-    cached = n;
-    return cached;
+    slot.store(n);
+    return n;
 }
 
 int launch_stages(Int8Cache* c, ClArgs& a, cudaStream_t s) {

@@ -105,6 +105,7 @@ def lib():
         "nttb_u64_transform": (_int, [_vp, _vp, _u64, _int, _int, _vp]),
         "nttb_u64_four_step": (_int, [_vp, _vp, _int, _vp]),
         "nttb_u64_rowmaj_forward": (_int, [_vp, _vp, _vp]),
+        "nttb_u64_pretransposed_transform": (_int, [_vp, _vp, _u64, _int, _vp]),
         "nttb_u64_transpose": (_int, [_vp, _vp, _u64, _u64, _vp]),
         "nttb_u64_pointwise_mul": (_int, [_vp, _vp, _vp, _vp, _vp]),
         "nttb_u64_bit_reverse": (_int, [_vp, _u64, _vp]),
@@ -453,6 +454,10 @@ class Plan:
 
     def rowmaj_forward(self, data, stream=None):
         _check(lib().nttb_u64_rowmaj_forward(self._h, _ptr(data), _stream(stream)))
+
+    def pretransposed_transform(self, data, n1, inverse=False, stream=None):
+        """Transform in the RowMaj pre-transposed layout pre[b*n1 + a] = x[a*n2 + b], in place."""
+        _check(lib().nttb_u64_pretransposed_transform(self._h, _ptr(data), n1, int(inverse), _stream(stream)))
 
     def pointwise_mul(self, out, a, b, stream=None):
         _check(lib().nttb_u64_pointwise_mul(self._h, _ptr(out), _ptr(a), _ptr(b), _stream(stream)))

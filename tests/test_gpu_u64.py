@@ -124,6 +124,39 @@ def test_rowmaj_forward(torch_cuda):
     assert (to_host(d2, np.uint64) == O.ntt(x2, BABYBEAR)).all()
 
 
+@pytest.mark.parametrize("lg,n1", [(10, 32), (12, 64), (12, 16), (16, 256), (16, 64), (20, 1024), (13, 8192),
+                                   (6, 1)])
+def test_pretransposed_transform_every_size(torch_cuda, lg, n1):
+    """The RowMaj pre-transposed layout pre[b*n1 + a] = x[a*n2 + b] for every
+    n: forward gives the pre-transposed forward transform, inverse returns the
+    input; n = 4096, n1 = 64 forward is ntt_forward_rowmaj."""
+    n = 1 << lg
+    n2 = n // n1
+    x = rand(n, BABYBEAR, lg * 31 + n1)
+    plan = nb.Plan(n, BABYBEAR)
+    d = to_dev(torch_cuda, O.to_pretransposed(x, n1, n2))
+    plan.pretransposed_transform(d, n1)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == O.to_pretransposed(O.ntt(x, BABYBEAR), n1, n2)).all()
+    plan.pretransposed_transform(d, n1, inverse=True)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == O.to_pretransposed(x, n1, n2)).all()
+    if n == 4096 and n1 == 64:
+        d2 = to_dev(torch_cuda, O.to_pretransposed(x, 64, 64))
+        plan.rowmaj_forward(d2)
+        torch_cuda.cuda.synchronize()
+        assert (to_host(d2, np.uint64) == O.rowmaj_forward(O.to_pretransposed(x, 64, 64), BABYBEAR)).all()
+
+
+def test_pretransposed_transform_rejects_bad_n1(torch_cuda):
+    plan = nb.Plan(1 << 10, BABYBEAR)
+    d = to_dev(torch_cuda, rand(1 << 10, BABYBEAR, 1))
+    for bad in (3, 1 << 11, 0):
+        with pytest.raises(nb.NTTError) as e:
+            plan.pretransposed_transform(d, bad)
+        assert "n1" in str(e.value)
+
+
 def test_transpose_helpers(torch_cuda):
     x = rand(64 * 128, BABYBEAR, 5)
     src = to_dev(torch_cuda, x)
