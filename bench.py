@@ -184,8 +184,9 @@ def reference_gpu_bar(qs, steps, warmup, device=0):
     import torch
     from oracle import oracle as O
     R = O.ref()
-    if R is None:
-        return {"unavailable": "reference library oracle/_ref/libntt_ref.so not built"}
+    if R is None or not hasattr(R, "ref_ntt_rns_optimized"):
+        return {"unavailable": "reference library oracle/_ref/libntt_ref.so not built (or built without "
+                               "ref_ntt_rns_optimized; rerun __graft_entry__.build())"}
     torch.cuda.set_device(device)
     dev = torch.device("cuda", device)
     stream = torch.cuda.Stream(device=dev)

@@ -86,8 +86,9 @@ def ref():
         R.ref_ntt_init.argtypes = [u64, u64]
         R.ref_ntt_cleanup.argtypes = [ctypes.c_void_p]
         R.ref_ntt_run.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
-        R.ref_ntt_rns_optimized.argtypes = [ctypes.POINTER(ctypes.c_void_p), u64, u64, ctypes.c_void_p, ctypes.c_int,
-                                            ctypes.c_void_p]
+        if hasattr(R, "ref_ntt_rns_optimized"):  # absent from libraries built before it existed
+            R.ref_ntt_rns_optimized.argtypes = [ctypes.POINTER(ctypes.c_void_p), u64, u64, ctypes.c_void_p,
+                                                ctypes.c_int, ctypes.c_void_p]
         R.ref_klimb_case.restype = ctypes.c_int
         R.ref_klimb_case.argtypes = [ctypes.c_int, ctypes.c_int, u64, _u32p, _u32p, _u32p, _u32p]
         R.ref_klimb_mont.restype = ctypes.c_int

@@ -302,7 +302,8 @@ def test_vs_reference_gpu_kernels(torch_cuda, n, op):
     assert (to_host(d, np.uint64) == to_host(d_ref, np.uint64)).all()
 
 
-@pytest.mark.skipif(O.ref() is None, reason="reference library not built")
+@pytest.mark.skipif(O.ref() is None or not hasattr(O.ref(), "ref_ntt_rns_optimized"),
+                    reason="reference library not built")
 def test_reference_optimized_on_rns_moduli(torch_cuda):
     """The reference's ntt_forward_optimized / ntt_inverse_optimized over the
     24 distinct 31-bit moduli of the RNS batch (one ntt_init per modulus,
