@@ -7,15 +7,17 @@
 //
 // One persistent kernel moves 32 x 32-word tiles (8 KB) through a ring of
 // shared-memory slots, one work item per slot:
-//   * TMA tiled loads bring a tile into its slot as two 128-byte-wide boxes
-//     with the 128-byte swizzle, completing on the slot's mbarrier;
-//   * the threads permute the tile inside the slot: lane i reads the 16-byte
-//     chunk (row i, words 2k, 2k+1) -- the swizzle spreads the 32 rows of one
-//     chunk over all banks -- into registers, and after a barrier writes the
-//     two words to rows 2k, 2k+1 (bit-reversed for the bit reversal) of the
-//     same swizzled layout, 16 lanes filling one 128-byte row segment;
-//   * TMA tiled stores write the slot back as two boxes, and the slot is
-//     reloaded only once those stores have read it, while a third of the
+//   * TMA tiled loads bring a tile into its slot with the 128-byte swizzle,
+//     completing on the slot's mbarrier: two 128-byte-wide boxes for the
+//     transposes, one box holding both halves of every 256-byte row segment
+//     for the bit reversal (tile_off);
+//   * the threads permute the tile inside the slot: whole 16-byte chunks
+//     are read into registers and, after a barrier, written back to their
+//     permuted places in the same swizzled layout, with lane assignments that
+//     keep both sides free of bank conflicts (permute_transpose,
+//     permute_bitrev);
+//   * TMA tiled stores write the slot back in the same boxes, and the slot
+//     is reloaded only once those stores have read it, while a third of the
 //     ring's slots may still be storing.
 // HBM sees only whole 256-byte row segments in both directions, and with no
 // separate output buffer every slot of shared memory carries loads in flight.
