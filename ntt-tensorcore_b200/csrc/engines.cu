@@ -16,15 +16,21 @@ static int env_engine() {
     return NTTB_ENGINE_AUTO;
 }
 
-int auto_engine32(const Plan32& p, bool src_u64) {
-    if (int8_serves(p, src_u64)) return NTTB_ENGINE_INT8;
+// The INT8 cluster kernel gives each (polynomial, limb) unit four SMs; the
+// uint64-word drop-in path takes it from kInt8MinUnits64 units on, below
+// which the CUDA-core engine, which spreads one polynomial over the whole
+// GPU, is faster.
+constexpr uint64_t kInt8MinUnits64 = 8;
+
+int auto_engine32(const Plan32& p, bool src_u64, uint64_t units) {
+    if (int8_serves(p, src_u64) && (!src_u64 || units >= kInt8MinUnits64)) return NTTB_ENGINE_INT8;
     return NTTB_ENGINE_SCALAR;
 }
 
 int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                     int engine, cudaStream_t s) {
     if (engine == NTTB_ENGINE_AUTO) engine = env_engine();
-    if (engine == NTTB_ENGINE_AUTO) engine = auto_engine32(p, src_u64);
+    if (engine == NTTB_ENGINE_AUTO) engine = auto_engine32(p, src_u64, (uint64_t)n_polys * p.n_limbs);
     switch (engine) {
         case NTTB_ENGINE_SCALAR:
             return scalar_transform32(p, src, dst, src_u64, n_polys, inverse, s);

@@ -15,7 +15,7 @@ int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_
                     int engine, cudaStream_t s);
 
 // Which engine AUTO resolves to for this plan (NTTB_ENGINE_*).
-int auto_engine32(const Plan32& p, bool src_u64);
+int auto_engine32(const Plan32& p, bool src_u64, uint64_t units);
 
 // Frees engine caches attached to a plan.
 void engines_release32(Plan32* p);

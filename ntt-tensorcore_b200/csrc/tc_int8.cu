@@ -126,11 +126,11 @@ struct ClStage {
 
 struct ClArgs {
     ClStage st[4];
-    const uint32_t* src;    // [units][2^16]
-    uint32_t* dst;          // [units][2^16], may equal src
+    const void* src;        // [units][2^16] words of 4 or 8 bytes (words64)
+    void* dst;              // the same layout, may equal src
     const uint8_t* consts;  // per limb: 2 DFT-16 images, 3 DFT-64 images
     uint64_t const_stride;
-    uint32_t n_stages, n_limbs, units, pad_;
+    uint32_t n_stages, n_limbs, units, words64;  // words64: uint64 words (residues < 2^31)
 };
 
 __device__ __forceinline__ void flag_error(uint32_t bit) { atomicOr(&g_tc_error, bit); }
@@ -203,12 +203,13 @@ __device__ __forceinline__ void copy_image(const Cl& c, const uint8_t* limb_blob
 
 // Stage A operand of tile w from HBM: row m = column b = 128(2c+w) + beta(m),
 // elements a (rows of x) -> buffer 0, K-major SW128.
-__device__ __forceinline__ void load_columns(const Cl& c, const uint32_t* x) {
+template <class W>
+__device__ __forceinline__ void load_columns(const Cl& c, const W* x) {
     const uint32_t m = c.wt & 127u, hh = c.wt >> 7;
-    const uint32_t* col = x + 128u * (2u * c.rank + c.w) + beta(m) + (32u * hh) * 1024u;
+    const W* col = x + 128u * (2u * c.rank + c.w) + beta(m) + (32u * hh) * 1024u;
     uint32_t v[32];
 #pragma unroll
-    for (uint32_t a = 0; a < 32; a++) v[a] = __ldcs(col + a * 1024u);
+    for (uint32_t a = 0; a < 32; a++) v[a] = (uint32_t)__ldcs(col + a * 1024u);
     uint8_t* t = c.base + kOffBuf0 + c.w * kTileBytes;
 #pragma unroll
     for (uint32_t k = 0; k < 8; k++)
@@ -311,7 +312,7 @@ __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qi
 // one word of the SW128 atom (g, K block c2 / 8), staged at piece slot
 // w' * 32 + P * 8 + 2 g + c2 / 8 (in KB).
 template <class Gate, class PartDone>
-__device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qinv, uint32_t* gout, Gate gate,
+__device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qinv, void* gout, bool words64, Gate gate,
                                             PartDone part_done) {
     const uint32_t base = c.taddr + c.w * 256u + ((c.quarter * 32u) << 16);
     const uint32_t r = c.lane & 7u, d = 8u * (2u * c.rank + c.w) + r;
@@ -333,9 +334,16 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
         }
         if (gout) {
             const uint32_t d2 = 16u * (c.lane >> 3) + 4u * t2 + c.quarter;
-            uint32_t* o = gout + d + 64u * d2;
+            const uint32_t o = d + 64u * d2;
+            if (words64) {
+                uint64_t* g = static_cast<uint64_t*>(gout) + o;
 #pragma unroll
-            for (uint32_t k = 0; k < 16; k++) __stcs(o + 4096u * k, canon(y[k], q));
+                for (uint32_t k = 0; k < 16; k++) __stcs(g + 4096u * k, (uint64_t)canon(y[k], q));
+            } else {
+                uint32_t* g = static_cast<uint32_t*>(gout) + o;
+#pragma unroll
+                for (uint32_t k = 0; k < 16; k++) __stcs(g + 4096u * k, canon(y[k], q));
+            }
         } else {
             if (part == 0) gate();
             const uint32_t g = 2u * (c.quarter & 1u) + c.w;
@@ -398,7 +406,8 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             tc::bulk_g2s(c.base + kOffImg16, limb_blob, kBlobImg, c.bar + kBarConst);
             copy_image(c, limb_blob, args.st[0].img, c.bar + kBarConst);
         }
-        load_columns(c, args.src + ((uint64_t)unit << 16));
+        if (args.words64) load_columns(c, static_cast<const uint64_t*>(args.src) + ((uint64_t)unit << 16));
+        else load_columns(c, static_cast<const uint32_t*>(args.src) + ((uint64_t)unit << 16));
     };
     if (c.tid < 32) tc::tmem_alloc(slot, 512);
     if (c.tid == 0) {
@@ -519,7 +528,11 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                 wait_parity(c.bar + kBarMma2 + c.w, ph_mma2);
                 tc::fence_after_sync();
                 // staging overwrites both tiles' level-2 operands
-                epilogue_b2(c, q, qinv, last ? args.dst + off : nullptr,
+                void* gout = nullptr;
+                if (last)
+                    gout = args.words64 ? (void*)(static_cast<uint64_t*>(args.dst) + off)
+                                        : (void*)(static_cast<uint32_t*>(args.dst) + off);
+                epilogue_b2(c, q, qinv, gout, args.words64 != 0,
                             [&]() { wait_parity(c.bar + kBarMma2 + (c.w ^ 1u), ph_mma2); }, part_done);
                 ph_mma2 ^= 1u;
             }
@@ -753,7 +766,12 @@ std::vector<uint64_t> tc_dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint6
     return dft_matrix(L, root, q, row_twist, col_twist, scale);
 }
 
-bool int8_serves(const Plan32& p, bool src_u64) { return !src_u64 && p.log_n == 16; }
+// N = 2^16, residues as uint32 or as uint64 words (the drop-in layout; read
+// and written in place of the uint32 ones).
+bool int8_serves(const Plan32& p, bool src_u64) {
+    (void)src_u64;
+    return p.log_n == 16;
+}
 
 int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                      cudaStream_t s) {
@@ -765,8 +783,9 @@ int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32
     a.st[0] = stage(c, inverse, 0);
     a.st[1] = stage(c, inverse, 1);
     a.n_stages = 2;
-    a.src = static_cast<const uint32_t*>(src);
-    a.dst = static_cast<uint32_t*>(dst);
+    a.src = src;
+    a.dst = dst;
+    a.words64 = src_u64 ? 1u : 0u;
     a.n_limbs = p.n_limbs;
     a.units = n_polys * p.n_limbs;
     return launch_stages(c, a, s);

@@ -39,6 +39,41 @@ def test_forward_inverse_vs_oracle(torch_cuda, engine, lg):
         assert (run_u64(torch_cuda, plan, x, True, engine) == O.ntt(x, BABYBEAR, True)).all()
 
 
+@pytest.mark.parametrize("batch", [1, 3, 8, 24])
+@pytest.mark.parametrize("q", [BABYBEAR, 2147352577])
+def test_int8_engine_on_uint64_words(torch_cuda, batch, q):
+    """The INT8 tensor-core engine serves the drop-in uint64-word layout at
+    N = 2^16 (read and written as 8-byte words, in place): forward and
+    inverse equal the oracle for every polynomial of the batch."""
+    n = 1 << 16
+    x = np.stack([rand(n, q, 700 + i) for i in range(batch)])
+    plan = nb.Plan(n, q)
+    y = run_u64(torch_cuda, plan, x.reshape(-1), False, "int8", batch).reshape(batch, n)
+    for i in range(batch):
+        assert (y[i] == O.ntt(x[i], q)).all(), "poly %d" % i
+    z = run_u64(torch_cuda, plan, y.reshape(-1), True, "int8", batch).reshape(batch, n)
+    assert (z == x).all()
+    assert nb.device_errors() == 0
+
+
+def test_auto_engine_for_uint64_batches(torch_cuda):
+    """AUTO takes the INT8 kernel for uint64 batches of 8 or more polynomials
+    at N = 2^16 and the CUDA-core engine for fewer; both bit-exact."""
+    n = 1 << 16
+    plan = nb.Plan(n, BABYBEAR)
+    for batch, kernel in ((8, "int8_cluster_n16_x2"), (2, "scalar_pass_col")):
+        x = np.stack([rand(n, BABYBEAR, 900 + i) for i in range(batch)])
+        d = to_dev(torch_cuda, x.reshape(-1))
+        nb.profile_start()
+        plan.transform(d, batch=batch)
+        torch_cuda.cuda.synchronize()
+        ran = nb.profile_stop()
+        assert kernel in ran, (batch, ran)
+        y = to_host(d, np.uint64).reshape(batch, n)
+        for i in range(batch):
+            assert (y[i] == O.ntt(x[i], BABYBEAR)).all()
+
+
 @pytest.mark.parametrize("n", [64, 256, 1024, 4096])
 def test_golden_seed42(torch_cuda, n):
     g = golden("babybear_seed42.npz")
