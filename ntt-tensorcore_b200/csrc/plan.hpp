@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -76,6 +77,7 @@ struct Plan32 {
     LimbDev<M32>* d_limbs = nullptr;  // device array, n_limbs entries
     std::vector<void*> allocations;   // device memory owned by the plan
     void* engine_data[4] = {nullptr, nullptr, nullptr, nullptr};  // per-engine host-side caches
+    std::mutex engine_mu;             // guards the lazy construction of engine_data
     void* ws = nullptr;               // workspace for in-place multi-pass transforms
     size_t ws_bytes = 0;
 };

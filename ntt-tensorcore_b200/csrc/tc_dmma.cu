@@ -304,14 +304,18 @@ bool dmma_serves(const Plan32& p, bool src_u64) { return !src_u64 && p.log_n == 
 int dmma_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                      cudaStream_t s) {
     if (!dmma_serves(p, src_u64) || n_polys > 65535 || p.n_limbs > 65535) return 1;
-    auto* c = reinterpret_cast<DmCache*>(p.engine_data[2]);
-    if (!c) {
-        c = new DmCache();
-        if (build_dm(p, c)) {
-            delete c;
-            return 2;
+    DmCache* c;
+    {
+        std::lock_guard<std::mutex> lock(p.engine_mu);
+        c = reinterpret_cast<DmCache*>(p.engine_data[2]);
+        if (!c) {
+            c = new DmCache();
+            if (build_dm(p, c)) {
+                delete c;
+                return 2;
+            }
+            p.engine_data[2] = c;
         }
-        p.engine_data[2] = c;
     }
     const uint32_t* in = static_cast<const uint32_t*>(src);
     uint32_t* out = static_cast<uint32_t*>(dst);

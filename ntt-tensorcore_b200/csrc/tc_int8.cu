@@ -681,6 +681,7 @@ int build_cache(Plan32& p, Int8Cache* c) {
 }
 
 Int8Cache* get_cache(Plan32& p) {
+    std::lock_guard<std::mutex> lock(p.engine_mu);
     auto* c = reinterpret_cast<Int8Cache*>(p.engine_data[1]);
     if (c) return c;
     c = new Int8Cache();
