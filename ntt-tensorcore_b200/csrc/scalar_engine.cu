@@ -304,6 +304,16 @@ inline uint32_t tile_vectors(uint32_t e_max, uint32_t len, uint32_t n_vectors, u
 //           the same positions of `dst` -- each tile reads and writes one set
 //           of positions, so pass B is safe in place.
 // Pass A cannot run in place; an in-place call stages it in `ws`.
+// Whether a transform runs as two passes: always above the tile size e_max;
+// from 2^12 on also when there are few (polynomial, limb) units, since a
+// single pass gives each unit one CTA and leaves the GPU idle (one
+// polynomial of 2^12 words: one CTA for all twelve stages).
+constexpr uint64_t kFewUnits = 8;
+inline bool two_pass(uint32_t log_n, uint32_t e_max, uint64_t units) {
+    const uint32_t n = 1u << log_n;
+    return n > e_max || (log_n >= 12 && units < kFewUnits);
+}
+
 template <class S, class A>
 int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const LimbDev<A>* d_limbs,
                       const void* src, void* dst, void* ws, uint32_t n_polys, bool inverse, uint32_t e_max,
@@ -317,7 +327,7 @@ int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const L
     a.inverse = inverse ? 1 : 0;
     uint32_t pre = (!inverse && negacyclic) ? F_PRE_PSI : 0u;
     uint32_t post = inverse ? (negacyclic ? F_POST_PSI_INV : F_POST_SCALE) : 0u;
-    if (n <= e_max) {
+    if (!two_pass(log_n, e_max, (uint64_t)n_limbs * n_polys)) {
         // single pass: one row of length n per (poly, limb)
         a.src = src;
         a.dst = dst;
@@ -362,7 +372,7 @@ int transform_generic(uint32_t log_n, uint32_t n_limbs, bool negacyclic, const L
 int scalar_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                        cudaStream_t s) {
     void* ws = nullptr;
-    if (src == dst && p.n > 8192) {
+    if (src == dst && two_pass(p.log_n, 8192, (uint64_t)n_polys * p.n_limbs)) {
         ws = plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * (src_u64 ? 8 : 4));
         if (!ws) return 2;
     }
@@ -381,7 +391,7 @@ int scalar_transform32_ws(const Plan32& p, uint32_t* data, void* ws, uint32_t n_
 
 int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s) {
     void* ws = nullptr;
-    if (src == dst && p.n > 4096) {
+    if (src == dst && two_pass(p.log_n, 4096, (uint64_t)n_polys * p.n_limbs)) {
         ws = plan_workspace(&p.ws, &p.ws_bytes, (size_t)n_polys * p.n_limbs * p.n * 8);
         if (!ws) return 2;
     }
