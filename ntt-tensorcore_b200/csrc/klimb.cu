@@ -52,16 +52,21 @@ __global__ void klimb_bitrev(uint32_t* data, uint32_t n, uint32_t log_n) {
 
 // Stages s0 .. s0 + r - 1 on tiles of 2^(r + logC) elements (shared memory,
 // limb-major: sm[k * E + e], e = j * C + c).
+// With `fused_bitrev` (one CTA holding the whole transform) the tile loads
+// element i from its bit-reversed position: every load precedes the first
+// store, so the permutation needs no pass of its own.
 template <int K>
 __global__ void __launch_bounds__(256) klimb_group(uint32_t* data, const uint32_t* tw, uint32_t log_n, uint32_t s0,
-                                                   uint32_t r, uint32_t logC, Limbs<K> p, uint32_t np) {
+                                                   uint32_t r, uint32_t logC, Limbs<K> p, uint32_t np,
+                                                   bool fused_bitrev) {
     extern __shared__ uint32_t sm[];
     const uint32_t E = 1u << (r + logC), C = 1u << logC;
     const uint32_t chunks = (1u << s0) >> logC;  // column chunks per group of 2^(s0 + r)
     const uint32_t G = blockIdx.x / chunks, low0 = (blockIdx.x % chunks) << logC;
     const size_t base = ((size_t)G << (s0 + r)) + low0;
     for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
-        const size_t i = base + ((size_t)(e >> logC) << s0) + (e & (C - 1));
+        size_t i = base + ((size_t)(e >> logC) << s0) + (e & (C - 1));
+        if (fused_bitrev) i = log_n ? (__brev((uint32_t)i) >> (32u - log_n)) : 0u;
         const uint32_t* src = data + i * K;
 #pragma unroll
         for (int k = 0; k < K; k++) sm[k * E + e] = src[k];
@@ -107,8 +112,20 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
     Limbs<K> p;
     for (int k = 0; k < K; k++) p.l[k] = prime[k];
     const uint32_t n = 1u << log_n;
-    // largest tile: 48 KB of shared memory
-    const uint32_t log_emax = K <= 3 ? 12u : 10u;
+    // largest tile: 48 KB of shared memory; smaller while a pass would have
+    // fewer than kTargetCtas tiles (small transforms are bound by the latency
+    // of their stage chains, so more, shorter tiles win), but at least 2^6
+    constexpr uint32_t kTargetCtas = 148;
+    uint32_t log_emax = K <= 3 ? 12u : 10u;
+    while (log_emax > 6 && (n >> log_emax) < kTargetCtas) log_emax--;
+    // Small transforms run as one tile in one launch, the bit reversal fused
+    // into its loads (measured: K = 2 up to 2^10, K = 11 up to 2^8).
+    if (log_n <= (K <= 3 ? 10u : 8u)) {
+        ProfScope prof("klimb_group", s);
+        const uint32_t threads = n / 2 < 256 ? (n / 2 > 0 ? n / 2 : 1) : 256;
+        klimb_group<K><<<1, threads, (size_t)n * K * 4, s>>>(d_data, d_tw, log_n, 0, log_n, 0, p, np, true);
+        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    }
     {
         ProfScope prof("klimb_bitrev", s);
         klimb_bitrev<K><<<(n + 255) / 256, 256, 0, s>>>(d_data, n, log_n);
@@ -121,12 +138,13 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
             if (r > log_emax) r = log_emax;
         } else {
             if (r > 8) r = 8;
+            if (r > log_emax) r = log_emax;
             logC = log_emax - r < s0 ? log_emax - r : s0;
         }
         const uint32_t E = 1u << (r + logC);
         const uint32_t threads = E / 2 < 256 ? E / 2 : 256;
         ProfScope prof("klimb_group", s);
-        klimb_group<K><<<n / E, threads, (size_t)E * K * 4, s>>>(d_data, d_tw, log_n, s0, r, logC, p, np);
+        klimb_group<K><<<n / E, threads, (size_t)E * K * 4, s>>>(d_data, d_tw, log_n, s0, r, logC, p, np, false);
         if (cudaGetLastError() != cudaSuccess) return 2;
         s0 += r;
     }

@@ -46,9 +46,12 @@ def test_klimb_vs_reference_fixture(torch_cuda, K):
     assert run_klimb(torch_cuda, K, xs, omega, p) == want
 
 
-@pytest.mark.parametrize("K,log_n", [(2, 12), (3, 13), (11, 9)])
+@pytest.mark.parametrize("K,log_n", [(2, 1), (2, 6), (2, 10), (2, 11), (2, 12), (3, 10), (3, 13), (11, 8),
+                                     (11, 9), (11, 12)])
 def test_klimb_vs_naive_network(torch_cuda, K, log_n):
-    """Sizes that take more than one shared-memory pass, against the network."""
+    """Against the network: one fused tile (K <= 3 up to 2^10, K = 11 up to
+    2^8) and the multi-pass sizes above, whose tiles shrink until a pass has
+    enough CTAs."""
     g = golden("klimb.npz")
     # the fixture's omega as the twiddle base: the network is defined for
     # any omega (a DFT only when omega has order 2^log_n)
