@@ -62,15 +62,38 @@ def parse():
 
 
 def dist_setup(args):
+    """One process per GPU (torchrun): NCCL on GPUs, gloo where none is visible
+    (the host-side logic of the multi-rank path runs on CPU that way)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def reduce_over_ranks(x, world, op="max"):
+    """max (times, latencies) or sum (replica throughput) of a per-rank number
+    over all ranks.  Every rank calls it, in the same order."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def rank_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
 
 
 def moduli():
@@ -286,12 +309,7 @@ def run_ours(args, world, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
         launches = nb.launch_count() - c0
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = reduce_over_ranks(e0.elapsed_time(e1), world)
         barrier()
         return ms, launches
 
@@ -370,12 +388,7 @@ def run_ours(args, world, rank, local):
     plan.stream_host(h_in, h_out, 1, e_steps, mode="forward_inverse", engine=engine, stream=stream)
     e1.record(stream)
     torch.cuda.synchronize()
-    e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
+    e_ms = reduce_over_ranks(e0.elapsed_time(e1), world)
     assert (h_out.numpy().view(np.uint32) == h_in.numpy().view(np.uint32)).all(), "e2e round trip mismatch"
     e2e = {"value": world * coeffs_per_step * e_steps / (e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": batch_bytes, "d2h_bytes_per_step": batch_bytes,
@@ -497,6 +510,7 @@ def run_uneven(args, world, rank, local):
     assert nb.device_errors() == 0
 
     def timed(fn, steps):
+        rank_barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         c0 = nb.launch_count()
@@ -505,7 +519,7 @@ def run_uneven(args, world, rank, local):
             fn(stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1), nb.launch_count() - c0
+        return reduce_over_ranks(e0.elapsed_time(e1), world), nb.launch_count() - c0
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -662,12 +676,26 @@ def run_serve(args, world, rank, local):
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "mean_ms": float(lat.mean())}
 
+    def over_ranks(r):
+        # replicas: rates add up, latencies are the worst rank's
+        if world <= 1:
+            return r
+        out = dict(r)
+        for k in ("requests", "achieved_rps", "coeffs_per_s"):
+            out[k] = reduce_over_ranks(r[k], world, "sum")
+        for k in ("p50_ms", "p99_ms", "mean_ms", "submit_s"):
+            out[k] = reduce_over_ranks(r[k], world, "max")
+        if r["offered_rps"] is not None:
+            out["offered_rps"] = reduce_over_ranks(r["offered_rps"], world, "sum")
+        return out
+
     phase(None, 1.0)  # warm-up
     sat = phase(None, args.serve_seconds)
-    peak = sat["achieved_rps"]
+    peak = sat["achieved_rps"]  # this rank's saturated rate sets its own load levels
     levels = {}
     for frac in (0.25, 0.5, 0.8, 1.0):
-        levels["%d%%" % int(frac * 100)] = phase(frac * peak, args.serve_seconds)
+        levels["%d%%" % int(frac * 100)] = over_ranks(phase(frac * peak, args.serve_seconds))
+    sat = over_ranks(sat)
     st = srv.stats()
     srv.close()
     cpu = cpu_sample([(lg, limbs, False, True, True) for _, _, lg, limbs, _ in pool], qs) if rank == 0 else None
@@ -708,6 +736,7 @@ def run_q60(args, world, rank, local):
     pool = torch.from_numpy(host.view(np.int64)).to(dev).repeat(pool_n, 1)
 
     def timed(fn, steps):
+        rank_barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         c0 = nb.launch_count()
@@ -716,7 +745,7 @@ def run_q60(args, world, rank, local):
             fn(i)
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1), nb.launch_count() - c0
+        return reduce_over_ranks(e0.elapsed_time(e1), world), nb.launch_count() - c0
 
     def one(i):
         buf = pool[i % pool_n]
@@ -797,8 +826,10 @@ def run_aux(args, world, rank, local):
     peak = peaks.get("hbm_gbs", 6650.0)
 
     def timed(fn, steps):
+        # seconds per launch on the slowest rank (the figures are per GPU)
         for _ in range(3):
             fn()
+        rank_barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -806,7 +837,7 @@ def run_aux(args, world, rank, local):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps / 1e3
+        return reduce_over_ranks(e0.elapsed_time(e1) / steps / 1e3, world)
 
     out = {}
     qs = nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
@@ -921,7 +952,10 @@ def main():
             dist.destroy_process_group()
         return
     if args.impl == "reference":
-        if rank != 0:
+        if rank != 0:  # rank 0 alone runs the reference; no collective is issued on this arm
+            if world > 1:
+                import torch.distributed as dist
+                dist.destroy_process_group()
             return
         qs = moduli()
         r = cpu_reference(qs, args.steps, args.warmup)
@@ -938,6 +972,9 @@ def main():
             # the reference's own GPU kernels on the same batch (reported beside the CPU arm)
             line["reference_gpu"] = reference_gpu_bar(qs, args.steps, args.warmup, local)
         print(json.dumps(line))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     result, qs = run_ours(args, world, rank, local)
     if rank == 0 and world == 1 and not args.quick:
