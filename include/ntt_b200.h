@@ -113,7 +113,9 @@ NTTB_API int nttb_u64_rowmaj_forward(const nttb_plan* plan, uint64_t* d_data, vo
  * rowmaj_to_pretransposed, src/ntt_optimized.cu:893-895, 922-934) and
  * receives the transform in the same layout, in place.  n1 a power of two
  * <= n; nttb_u64_rowmaj_forward is the case n = 4096, n1 = 64, forward.
- * Runs as a TMA transpose, the transform, and the transpose back. */
+ * Square shapes (n1 * n1 == n, q < 2^31) run as two passes that read and
+ * write the layout directly; others as a TMA transpose, the transform, and
+ * the transpose back. */
 NTTB_API int nttb_u64_pretransposed_transform(const nttb_plan* plan, uint64_t* d_data, uint64_t n1, int inverse,
                                               void* stream);
 /* d_dst[c*rows + r] = d_src[r*cols + c].  Replaces rowmaj_to_pretransposed

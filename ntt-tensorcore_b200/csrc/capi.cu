@@ -468,6 +468,15 @@ int nttb_u64_pretransposed_transform(const nttb_plan* P, uint64_t* d, uint64_t n
     if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "pretransposed_transform: null argument");
     if (!pow2(n1) || n1 > P->n) return fail(NTTB_ERR_INVALID_ARG, "pretransposed_transform: n1 must be a power of two <= n");
     const uint64_t n2 = P->n / n1;
+    if (!P->wide && n1 == n2) {
+        // square: two passes that read and write the layout directly
+        const int r = scalar_pretransposed32(P->p32, d, P->d_scratch, inverse != 0, (cudaStream_t)stream);
+        if (r == 0) return cuda_status("pretransposed_transform");
+        if (r != 1) {
+            const int st = cuda_status("pretransposed_transform");
+            return st ? st : fail(NTTB_ERR_CUDA, "pretransposed_transform: launch failed");
+        }
+    }
     // pre[b * n1 + a] = canon[a * n2 + b]: canon is pre (n2 x n1) transposed
     int rc = nttb_u64_transpose(P->d_scratch, d, n2, n1, stream);
     if (rc) return rc;

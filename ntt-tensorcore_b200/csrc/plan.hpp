@@ -51,7 +51,8 @@ enum : uint32_t {
 // Pass geometries of the scalar engine.
 enum PassMode : int {
     MODE_COL = 0,          // vectors = columns of [N1 x N2]; out in place (row k, col b)
-    MODE_ROW_NAT = 1,      // vectors = rows d; out X[d + N1*k] (natural order)
+    MODE_ROW_NAT = 1,      // vectors = rows d; out X[d + N1*k] (natural order), or with F_STORE_T
+                           // row by row at d*len + k (F_POST_TW: times root^(k*d))
     MODE_GATHER_T = 2,     // vectors = chunks of the N1 x N2 -> N2 x N1 transpose; out in place
     MODE_ROW_SCATTER_T = 3 // vectors = contiguous chunks; out through the transpose back
 };
@@ -140,5 +141,8 @@ int dmma_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32
                      cudaStream_t s);
 void dmma_release(Plan32* p);
 int scalar_four_step32(const Plan32& p, uint64_t* data, uint64_t* scratch, bool inverse, cudaStream_t s);
+// Transform of one uint64-word polynomial in the pre-transposed layout for
+// n = M^2 (in place, staged in `mid`, n words); 1 when the plan is not served.
+int scalar_pretransposed32(const Plan32& p, uint64_t* data, uint64_t* mid, bool inverse, cudaStream_t s);
 
 }  // namespace nttb

@@ -232,7 +232,14 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
     // ---- store ----
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
         uint32_t v, k;
-        if (MODE == MODE_GATHER_T) { v = idx >> lgL; k = idx & (L - 1); } else { v = idx & (V - 1); k = idx >> lgV; }
+        // row-contiguous outputs: consecutive threads take consecutive k
+        if (MODE == MODE_GATHER_T || (MODE == MODE_ROW_NAT && (flags & F_STORE_T))) {
+            v = idx >> lgL;
+            k = idx & (L - 1);
+        } else {
+            v = idx & (V - 1);
+            k = idx >> lgV;
+        }
         const uint32_t vec = v0 + v;
         const uint32_t kk = kDIT ? k : bitrev(k, (int)lgL);
         E x = t[(size_t)v * stride + kk + (kk >> kPad)];
@@ -249,7 +256,8 @@ __global__ void __launch_bounds__(kThreads) scalar_pass_kernel(PassArgs args, co
                 }
             }
         } else if (MODE == MODE_ROW_NAT) {
-            pos = (uint64_t)vec + (uint64_t)N1 * k;
+            pos = (flags & F_STORE_T) ? (uint64_t)vec * L + k : (uint64_t)vec + (uint64_t)N1 * k;
+            if (flags & F_POST_TW) x = ar.mul(x, tw[((uint64_t)k * vec) & nmask]);
         } else if (MODE == MODE_GATHER_T) {
             pos = (uint64_t)vec * L + k;
         } else {
@@ -397,6 +405,39 @@ int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, 
     }
     return transform_generic<uint64_t, M64>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, src, dst, ws, n_polys,
                                             inverse, 4096, s);
+}
+
+// The RowMaj pre-transposed layout pre[b*M + a] = x[a*M + b] for n = M^2
+// (the layout of rowmaj_to_pretransposed, src/ntt_optimized.cu:893-895), in
+// and out, in two passes and no transpose:
+//   pass A (rows of pre = columns of x): U[d][b] = DFT_M(x[.][b])[d] * root^(d*b),
+//           stored at b*M + d in `mid`;
+//   pass B (columns of mid): X[d + M*c] = DFT_M(U[d][.])[c], stored at d*M + c,
+//           which is where pre-transposed X keeps element d + M*c.
+int scalar_pretransposed32(const Plan32& p, uint64_t* data, uint64_t* mid, bool inverse, cudaStream_t s) {
+    if (p.n_limbs != 1 || p.negacyclic || (p.log_n & 1u) || p.log_n < 2) return 1;
+    const uint32_t lg = p.log_n / 2, M = 1u << lg, e_max = 8192;
+    if (M > e_max) return 1;
+    PassArgs a{};
+    a.poly_stride = p.n;
+    a.n = p.n;
+    a.log_n = p.log_n;
+    a.n_limbs = 1;
+    a.inverse = inverse ? 1 : 0;
+    a.n1 = M;
+    a.n2 = M;
+    a.len = M;
+    a.log_len = lg;
+    a.vec_per_tile = tile_vectors(e_max, M, M, 1);
+    a.src = data;
+    a.dst = mid;
+    a.flags = F_POST_TW | F_STORE_T;
+    int rc = launch_pass<uint64_t, M32>(MODE_ROW_NAT, a, p.d_limbs, M, 1, s);
+    if (rc) return rc;
+    a.src = mid;
+    a.dst = data;
+    a.flags = F_STORE_T | (inverse ? F_POST_SCALE : 0u);
+    return launch_pass<uint64_t, M32>(MODE_COL, a, p.d_limbs, M, 1, s);
 }
 
 // The reference's four-step map (src/ntt_four_step.cu:244-392), race-free:

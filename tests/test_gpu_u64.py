@@ -183,6 +183,22 @@ def test_pretransposed_transform_every_size(torch_cuda, lg, n1):
         assert (to_host(d2, np.uint64) == O.rowmaj_forward(O.to_pretransposed(x, 64, 64), BABYBEAR)).all()
 
 
+def test_pretransposed_square_runs_without_transposes(torch_cuda):
+    """n = M^2, n1 = M: two scalar passes read and write the layout directly
+    (no transpose kernel runs); the result is the pre-transposed transform."""
+    n, m = 1 << 16, 256
+    x = rand(n, BABYBEAR, 4242)
+    plan = nb.Plan(n, BABYBEAR)
+    d = to_dev(torch_cuda, O.to_pretransposed(x, m, m))
+    nb.profile_start()
+    plan.pretransposed_transform(d, m)
+    torch_cuda.cuda.synchronize()
+    ran = nb.profile_stop()
+    assert not any("transpose" in k for k in ran), ran
+    assert sum(v[0] for k, v in ran.items() if k.startswith("scalar_pass")) == 2, ran
+    assert (to_host(d, np.uint64) == O.to_pretransposed(O.ntt(x, BABYBEAR), m, m)).all()
+
+
 def test_pretransposed_transform_rejects_bad_n1(torch_cuda):
     plan = nb.Plan(1 << 10, BABYBEAR)
     d = to_dev(torch_cuda, rand(1 << 10, BABYBEAR, 1))
