@@ -268,14 +268,19 @@ NTTB_API int nttb_batch_test_stall(nttb_batch* batch, uint32_t unit);
 
 /* ------------------------------------------------------------- serving
  * No reference counterpart (the reference has no request loop).  A server
- * multiplies polynomials for callers in host memory: request = (a, b) with
- * n_limbs rows of 2^log_n residues (row l mod moduli[first_modulus + l]),
- * result out = a * b per limb (negacyclic unless config.negacyclic == 0).
- * Requests are admitted in arrival order while their device operands
- * (2 x n_limbs x 2^log_n words) fit in the HBM budget left after the resident
+ * multiplies and transforms polynomials for callers in host memory:
+ *   product request = (a, b) with n_limbs rows of 2^log_n residues (row l mod
+ *     moduli[first_modulus + l]), result out = a * b per limb (negacyclic
+ *     unless config.negacyclic == 0), device operands 2 x n_limbs x 2^log_n words;
+ *   NTT request = one such operand, result its forward or inverse transform
+ *     per limb (with the negacyclic twist unless config.negacyclic == 0),
+ *     device operand n_limbs x 2^log_n words.
+ * Requests of both kinds share one queue and are admitted in arrival order
+ * while their device operands fit in the HBM budget left after the resident
  * twiddle tables and queues, and are batched continuously: up to `slots`
  * batches are in flight on separate streams, each one persistent launch
- * (forward a, forward b, product, inverse) between its copies.  a, b and out
+ * (per product: forward a, forward b, product, inverse; per NTT: the
+ * transform) between its copies.  a, b and out
  * must stay valid until the request completes; pinned host memory lets the
  * copies overlap.  Latency = submit -> completion, host steady clock. */
 typedef struct nttb_server nttb_server;
@@ -300,6 +305,10 @@ NTTB_API int nttb_server_create(const uint64_t* moduli, uint32_t n_moduli, const
 /* Queues a request; NTTB_ERR_BUDGET if its operands alone exceed the request region. */
 NTTB_API int nttb_server_submit(nttb_server* server, const uint32_t* a, const uint32_t* b, uint32_t* out,
                                 uint32_t log_n, uint32_t n_limbs, uint32_t first_modulus, uint64_t* id);
+/* Queues an NTT request: out = the forward (inverse != 0: inverse) transform of
+ * `in` per limb; NTTB_ERR_BUDGET if its operand alone exceeds the request region. */
+NTTB_API int nttb_server_submit_ntt(nttb_server* server, const uint32_t* in, uint32_t* out, uint32_t log_n,
+                                    uint32_t n_limbs, uint32_t first_modulus, int inverse, uint64_t* id);
 /* Waits for one request (NTTB_ERR_TIMEOUT after timeout_s); its latency in seconds. */
 NTTB_API int nttb_server_wait(nttb_server* server, uint64_t id, double timeout_s, double* latency_s);
 NTTB_API int nttb_server_drain(nttb_server* server, double timeout_s);

@@ -1,11 +1,14 @@
-// serve.cu -- the serving loop: polynomial products (negacyclic by default) of
-// mixed sizes and limb counts, admitted against an HBM budget and batched
-// continuously.
+// serve.cu -- the serving loop: polynomial products and NTTs (negacyclic by
+// default) of mixed sizes and limb counts, admitted against an HBM budget and
+// batched continuously.
 //
-// A request is (a, b) in host memory: n_limbs rows of 2^log_n residues, row l
-// reduced mod moduli[first_modulus + l]; its result a * b (per limb) goes to
-// `out` in host memory.  Its device footprint is 2 x n_limbs x 2^log_n words
-// (a, with the result written over it, and b).
+// A product request is (a, b) in host memory: n_limbs rows of 2^log_n
+// residues, row l reduced mod moduli[first_modulus + l]; its result a * b
+// (per limb) goes to `out` in host memory.  Its device footprint is
+// 2 x n_limbs x 2^log_n words (a, with the result written over it, and b).
+// An NTT request is one such operand, transformed forward or inverse in
+// place on the device (footprint n_limbs x 2^log_n words); both kinds share
+// the queue and the batches.
 //
 // One worker thread owns the device side.  Device memory for requests is one
 // region of (budget - resident tables and queues) bytes, carved first-fit in
@@ -13,9 +16,9 @@
 // empty, the worker admits requests in arrival order while their operands fit
 // in the region (and the batch stays under max_batch_requests /
 // max_batch_residues), and issues the batch on the slot's stream: host ->
-// device copies of every operand, ONE persistent batch launch (forward a,
-// forward b, pointwise product, inverse, per limb), device -> host copies of
-// the results, and a host callback that stamps the completion time, returns
+// device copies of every operand, ONE persistent batch launch (per product
+// and limb: forward a, forward b, pointwise product, inverse; per NTT and
+// limb: the transform), device -> host copies of the results, and a host callback that stamps the completion time, returns
 // the memory to the region and frees the slot.  Several slots are in flight
 // at once, so a batch's copies and kernels overlap with its neighbours', and
 // requests that arrive while others run are admitted as soon as memory and a
@@ -95,13 +98,18 @@ class Arena {
     size_t size_ = 0, used_ = 0, peak_ = 0;
 };
 
+enum ReqKind : uint32_t { kProduct = 0, kForward = 1, kInverse = 2 };
+
 struct Req {
     const uint32_t* a = nullptr;
-    const uint32_t* b = nullptr;
+    const uint32_t* b = nullptr;  // products only
     uint32_t* out = nullptr;
+    uint32_t kind = kProduct;
     uint32_t log_n = 0, limbs = 0, first = 0;
     size_t words = 0;  // per operand
     size_t off = 0;    // device offset of a; b follows
+    size_t bytes() const { return (kind == kProduct ? 2 : 1) * words * 4; }
+    size_t residues() const { return (kind == kProduct ? 3 : 1) * words; }  // transform work
     double t_submit = 0, t_done = 0;
     int status = NTTB_OK;
     bool done = false;
@@ -157,7 +165,7 @@ void CUDART_CB batch_done(void* p) {
         Req& r = s->reqs[id];
         r.t_done = t;
         r.done = true;
-        s->arena.release(r.off, 2 * r.words * 4);
+        s->arena.release(r.off, r.bytes());
         s->latencies.push_back(t - r.t_submit);
         s->completed++;
     }
@@ -183,12 +191,12 @@ void worker_main(nttb_server* s) {
         size_t residues = 0;
         while (!s->queue.empty() && ids.size() < s->cfg.max_batch_requests) {
             Req& r = s->reqs[s->queue.front()];
-            if (!ids.empty() && residues + r.words * 3 > s->cfg.max_batch_residues) break;
+            if (!ids.empty() && residues + r.residues() > s->cfg.max_batch_residues) break;
             size_t off = 0;
-            if (!s->arena.alloc(2 * r.words * 4, &off)) break;
+            if (!s->arena.alloc(r.bytes(), &off)) break;
             r.off = off;
             ids.push_back(s->queue.front());
-            residues += r.words * 3;
+            residues += r.residues();
             s->queue.pop_front();
         }
         if (ids.empty()) {  // memory is full: wait for a batch to finish
@@ -205,11 +213,12 @@ void worker_main(nttb_server* s) {
             work.push_back(r);
             nttb_batch_job j{};
             j.data = reinterpret_cast<uint32_t*>(s->region + r.off);
-            j.pointwise = j.data + r.words;
+            j.pointwise = r.kind == kProduct ? j.data + r.words : nullptr;
             j.log_n = r.log_n;
             j.n_limbs = r.limbs;
             j.first_modulus = r.first;
-            j.flags = NTTB_BATCH_POLYMUL | (s->cfg.negacyclic ? NTTB_NEGACYCLIC : 0u);
+            j.flags = (r.kind == kProduct ? NTTB_BATCH_POLYMUL : r.kind == kInverse ? NTTB_BATCH_INVERSE : 0u) |
+                      (s->cfg.negacyclic ? NTTB_NEGACYCLIC : 0u);
             sl->jobs.push_back(j);
         }
         s->batches++;
@@ -220,8 +229,9 @@ void worker_main(nttb_server* s) {
         for (size_t i = 0; i < work.size() && ok; i++) {
             const size_t bytes = work[i].words * 4;
             ok = cudaMemcpyAsync(sl->jobs[i].data, work[i].a, bytes, cudaMemcpyHostToDevice, sl->stream) == cudaSuccess &&
-                 cudaMemcpyAsync(sl->jobs[i].pointwise, work[i].b, bytes, cudaMemcpyHostToDevice, sl->stream) ==
-                     cudaSuccess;
+                 (work[i].kind != kProduct ||
+                  cudaMemcpyAsync(sl->jobs[i].pointwise, work[i].b, bytes, cudaMemcpyHostToDevice, sl->stream) ==
+                      cudaSuccess);
         }
         ok = ok && runner_run(sl->runner, sl->jobs.data(), (uint32_t)sl->jobs.size(), sl->stream) == 0;
         for (size_t i = 0; i < work.size() && ok; i++)
@@ -315,32 +325,60 @@ NTTB_API int nttb_server_create(const uint64_t* moduli, uint32_t n_moduli, const
     return NTTB_OK;
 }
 
-NTTB_API int nttb_server_submit(nttb_server* s, const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t log_n,
-                                uint32_t n_limbs, uint32_t first_modulus, uint64_t* id) {
-    if (!s || !a || !b || !out || !id) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: null argument");
-    if (log_n < 1 || log_n > s->cfg.max_log_n)
-        return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: log_n %u outside [1, %u]", log_n, s->cfg.max_log_n);
-    if (n_limbs == 0 || (uint64_t)first_modulus + n_limbs > s->plan->p.limbs.size())
-        return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: limbs outside the server's moduli");
-    nttb::Req r;
-    r.a = a;
-    r.b = b;
-    r.out = out;
-    r.log_n = log_n;
-    r.limbs = n_limbs;
-    r.first = first_modulus;
-    r.words = (size_t)n_limbs << log_n;
+}  // extern "C"
+
+namespace nttb {
+namespace {
+
+int submit_request(nttb_server* s, Req r, const char* what, uint64_t* id) {
+    if (r.log_n < 1 || r.log_n > s->cfg.max_log_n)
+        return fail(NTTB_ERR_INVALID_ARG, "%s: log_n %u outside [1, %u]", what, r.log_n, s->cfg.max_log_n);
+    if (r.limbs == 0 || (uint64_t)r.first + r.limbs > s->plan->p.limbs.size())
+        return fail(NTTB_ERR_INVALID_ARG, "%s: limbs outside the server's moduli", what);
+    r.words = (size_t)r.limbs << r.log_n;
     std::lock_guard<std::mutex> lk(s->mu);
-    if (nttb::round_up(2 * r.words * 4) > s->arena.size())
-        return fail(NTTB_ERR_BUDGET, "nttb_server_submit: %zu bytes exceed the HBM budget's request region (%zu)",
-                    2 * r.words * 4, s->arena.size());
-    r.t_submit = nttb::now_s();
+    if (round_up(r.bytes()) > s->arena.size())
+        return fail(NTTB_ERR_BUDGET, "%s: %zu bytes exceed the HBM budget's request region (%zu)", what, r.bytes(),
+                    s->arena.size());
+    r.t_submit = now_s();
     *id = s->next_id++;
     s->reqs[*id] = r;
     s->queue.push_back(*id);
     s->submitted++;
     s->cv.notify_all();
     return NTTB_OK;
+}
+
+}  // namespace
+}  // namespace nttb
+
+extern "C" {
+
+NTTB_API int nttb_server_submit(nttb_server* s, const uint32_t* a, const uint32_t* b, uint32_t* out, uint32_t log_n,
+                                uint32_t n_limbs, uint32_t first_modulus, uint64_t* id) {
+    if (!s || !a || !b || !out || !id) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit: null argument");
+    nttb::Req r;
+    r.a = a;
+    r.b = b;
+    r.out = out;
+    r.kind = nttb::kProduct;
+    r.log_n = log_n;
+    r.limbs = n_limbs;
+    r.first = first_modulus;
+    return nttb::submit_request(s, r, "nttb_server_submit", id);
+}
+
+NTTB_API int nttb_server_submit_ntt(nttb_server* s, const uint32_t* in, uint32_t* out, uint32_t log_n,
+                                    uint32_t n_limbs, uint32_t first_modulus, int inverse, uint64_t* id) {
+    if (!s || !in || !out || !id) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_submit_ntt: null argument");
+    nttb::Req r;
+    r.a = in;
+    r.out = out;
+    r.kind = inverse ? nttb::kInverse : nttb::kForward;
+    r.log_n = log_n;
+    r.limbs = n_limbs;
+    r.first = first_modulus;
+    return nttb::submit_request(s, r, "nttb_server_submit_ntt", id);
 }
 
 NTTB_API int nttb_server_wait(nttb_server* s, uint64_t id, double timeout_s, double* latency_s) {

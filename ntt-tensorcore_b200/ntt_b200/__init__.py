@@ -123,6 +123,7 @@ def lib():
         "nttb_server_default_config": (_int, [ctypes.POINTER(ServerConfig)]),
         "nttb_server_create": (_int, [_vp, _u32, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
         "nttb_server_submit": (_int, [_vp, _vp, _vp, _vp, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
+        "nttb_server_submit_ntt": (_int, [_vp, _vp, _vp, _u32, _u32, _u32, _int, ctypes.POINTER(_u64)]),
         "nttb_server_wait": (_int, [_vp, _u64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
         "nttb_server_drain": (_int, [_vp, ctypes.c_double]),
         "nttb_server_stats": (_int, [_vp, ctypes.POINTER(ServerStats)]),
@@ -282,8 +283,8 @@ class Batch:
 
 # ---------------------------------------------------------------- serving
 class Server:
-    """Polynomial-product server (nttb_server_*): requests are host arrays
-    (numpy, or pinned torch CPU tensors) of n_limbs x 2^log_n residues."""
+    """Polynomial-product and NTT server (nttb_server_*): requests are host
+    arrays (numpy, or pinned torch CPU tensors) of n_limbs x 2^log_n residues."""
 
     def __init__(self, moduli, **config):
         import numpy as np
@@ -311,6 +312,14 @@ class Server:
         _check(lib().nttb_server_submit(self._h, self._addr(a), self._addr(b), self._addr(out), log_n, n_limbs,
                                         first_modulus, ctypes.byref(i)))
         self._keep[int(i.value)] = (a, b, out)
+        return int(i.value)
+
+    def submit_ntt(self, x, out, log_n, n_limbs, first_modulus=0, inverse=False):
+        """Queues the forward (or inverse) transform of x per limb; result in out."""
+        i = _u64()
+        _check(lib().nttb_server_submit_ntt(self._h, self._addr(x), self._addr(out), log_n, n_limbs, first_modulus,
+                                            int(inverse), ctypes.byref(i)))
+        self._keep[int(i.value)] = (x, out)
         return int(i.value)
 
     def wait(self, rid, timeout=60.0):

@@ -1,7 +1,7 @@
-"""GPU: the serving loop (nttb_server_*) -- polynomial products of mixed
-sizes admitted against an HBM budget and batched continuously.  Every result
-equals the oracle's product, and a request gives the same result alone and
-in a mix of concurrent requests."""
+"""GPU: the serving loop (nttb_server_*) -- polynomial products and NTTs of
+mixed sizes admitted against an HBM budget and batched continuously.  Every
+result equals the oracle's product or transform, and a request gives the
+same result alone and in a mix of concurrent requests."""
 import numpy as np
 import pytest
 
@@ -74,6 +74,48 @@ def test_server_same_result_alone_and_in_mix(torch_cuda):
     for r, o in zip(others, outs):
         assert (o == product(r[0], r[1], PRIMES[r[4]:r[4] + r[3]], True)).all()
     srv.close()
+
+
+def test_server_ntt_requests_in_the_mix(torch_cuda):
+    """Forward and inverse NTT requests share the queue and the batches with
+    products: each equals the oracle's negacyclic transform per limb, and an
+    NTT request gives the same result alone and in the mix."""
+    rng = np.random.default_rng(5)
+    srv = nb.Server(PRIMES, hbm_budget_bytes=96 << 20, max_log_n=16, slots=3, max_batch_requests=16)
+    x, _, lg, limbs, first = request(rng, (12, 12), (3, 3))
+    alone = np.zeros_like(x)
+    srv.wait(srv.submit_ntt(x, alone, lg, limbs, first))
+    mods = PRIMES[first:first + limbs]
+    assert (alone == O.rns(x[None].astype(np.uint64), mods, negacyclic=True)[0].astype(np.uint32)).all()
+    jobs = []
+    for k in range(36):
+        a, b, lgk, lk, fk = request(rng, (4, 16), (1, 5))
+        out = np.zeros_like(a)
+        if k % 3 == 0:
+            jobs.append(("product", a, b, lgk, lk, fk, out, srv.submit(a, b, out, lgk, lk, fk)))
+        else:
+            inv = k % 3 == 2
+            jobs.append(("inverse" if inv else "forward", a, None, lgk, lk, fk, out,
+                         srv.submit_ntt(a, out, lgk, lk, fk, inverse=inv)))
+        if k == 17:
+            mixed = np.zeros_like(x)
+            mine = srv.submit_ntt(x, mixed, lg, limbs, first)
+    srv.drain()
+    for j in jobs:
+        srv.wait(j[-1])
+    srv.wait(mine)
+    assert (mixed == alone).all()
+    for kind, a, b, lgk, lk, fk, out, _ in jobs:
+        m = PRIMES[fk:fk + lk]
+        if kind == "product":
+            want = product(a, b, m, True)
+        else:
+            want = O.rns(a[None].astype(np.uint64), m, negacyclic=True, inverse=kind == "inverse")[0].astype(np.uint32)
+        assert (out == want).all(), (kind, lgk, lk)
+    st = srv.stats()
+    assert st["completed"] == 38 and st["bytes_in_use"] == 0
+    srv.close()
+    assert nb.device_errors() == 0
 
 
 def test_server_admission_under_budget(torch_cuda):
