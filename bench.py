@@ -52,7 +52,7 @@ def parse():
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
                          "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
-    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60", "move"], default=None,
+    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60", "move", "klimb"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--quick", action="store_true",
@@ -873,9 +873,35 @@ def profile_case(name):
     directions) launched twice; batch_tc: the same with log2 N 17..20 on
     tensor-core tiles; q60: forward + inverse of one 2^20 polynomial mod the
     60-bit prime, four times; move: the TMA tile kernels on 4096 x 4096
-    words (transpose, in-place transpose, bit reversal), one launch each."""
+    words (transpose, in-place transpose, bit reversal), one launch each;
+    klimb: the K-limb forward NTT over the BN254 field (K = 11) at 2^14,
+    three times (its field from the committed fixture)."""
     import torch
     import ntt_b200 as nb
+    if name == "klimb":
+        # BN254 (K = 11 limbs of 24 bits), Montgomery form R = 2^264.  The
+        # twiddles are powers of the fixture's omega: the network does the same
+        # arithmetic for any base, and this case is timed, not checked.
+        K, lg = 11, 14
+        g = np.load(os.path.join(ROOT, "tests", "golden", "klimb.npz"))
+        to_int = lambda limbs: sum(int(v) << (24 * i) for i, v in enumerate(limbs))
+        to_limbs = lambda x: [(x >> (24 * i)) & 0xFFFFFF for i in range(K)]
+        p, w = to_int(g["prime_K11"]), to_int(g["omega_K11"])
+        R = 1 << (24 * K)
+        n = 1 << lg
+        tw, t = [], R % p
+        for _ in range(n):
+            tw.append(to_limbs(t))
+            t = t * w % p
+        rng = np.random.default_rng(11)
+        xs = [to_limbs(int(v) % p * R % p) for v in rng.integers(0, 2 ** 62, n, dtype=np.uint64)]
+        d = torch.from_numpy(np.array(xs, dtype=np.uint32).reshape(-1).view(np.int32)).cuda()
+        dt = torch.from_numpy(np.array(tw, dtype=np.uint32).reshape(-1).view(np.int32)).cuda()
+        limbs = to_limbs(p)
+        for _ in range(3):
+            nb.klimb_forward(K, d, dt, lg, limbs, nb.klimb_neg_inv24(limbs[0]))
+        torch.cuda.synchronize()
+        return
     if name == "move":
         # TMA tile kernels: 4096 x 4096 words (128 MB) transposed out of place,
         # then in place, then bit-reversed in place; checked against numpy

@@ -50,6 +50,39 @@ __global__ void klimb_bitrev(uint32_t* data, uint32_t n, uint32_t log_n) {
     }
 }
 
+// In-place bit reversal by tile pairs, log_n >= 8.  With the index split as
+// (a, b, c) -- a the high 4 bits, c the low 4, b the log_n - 8 middle bits --
+// element (a, b, c) moves to (rev4(c), rev(b), rev4(a)).  One block takes the
+// 16 x 16-element tiles of middle values b and rev(b) (b <= rev(b)): each tile
+// row is 16 K contiguous words, read and written as flat word runs, and the
+// permutation happens in shared memory.
+__device__ __forceinline__ uint32_t rev4(uint32_t v) { return __brev(v) >> 28; }
+
+template <int K>
+__global__ void __launch_bounds__(256) klimb_bitrev_tiled(uint32_t* data, uint32_t log_n) {
+    __shared__ uint32_t t0[256 * K], t1[256 * K];
+    const uint32_t M = log_n - 8u, row = 16u * K;
+    const uint32_t b = blockIdx.x, br = M ? (__brev(b) >> (32u - M)) : 0u;
+    if (br < b) return;
+    auto row_base = [&](uint32_t a, uint32_t mid) -> size_t {
+        return (((size_t)a << (M + 4)) + ((size_t)mid << 4)) * K;
+    };
+    for (uint32_t w = threadIdx.x; w < 256u * K; w += blockDim.x) {
+        const uint32_t a = w / row, off = w % row;
+        t0[w] = data[row_base(a, b) + off];
+        t1[w] = data[row_base(a, br) + off];
+    }
+    __syncthreads();
+    // output row a2 of the tile stored at mid, word off = c2 K + k: element
+    // (rev4(c2), rev4(a2)) of the tile loaded from the partner position
+    for (uint32_t w = threadIdx.x; w < 256u * K; w += blockDim.x) {
+        const uint32_t a2 = w / row, off = w % row, c2 = off / K, k = off % K;
+        const uint32_t src = (rev4(c2) * 16u + rev4(a2)) * K + k;
+        data[row_base(a2, br) + off] = t0[src];
+        data[row_base(a2, b) + off] = t1[src];
+    }
+}
+
 // Stages s0 .. s0 + r - 1 on tiles of 2^(r + logC) elements (shared memory,
 // limb-major: sm[k * E + e], e = j * C + c).
 // With `fused_bitrev` (one CTA holding the whole transform) the tile loads
@@ -128,7 +161,8 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
     }
     {
         ProfScope prof("klimb_bitrev", s);
-        klimb_bitrev<K><<<(n + 255) / 256, 256, 0, s>>>(d_data, n, log_n);
+        if (log_n >= 8) klimb_bitrev_tiled<K><<<n >> 8, 256, 0, s>>>(d_data, log_n);
+        else klimb_bitrev<K><<<(n + 255) / 256, 256, 0, s>>>(d_data, n, log_n);
         if (cudaGetLastError() != cudaSuccess) return 2;
     }
     uint32_t s0 = 0;
