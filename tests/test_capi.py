@@ -81,6 +81,16 @@ def test_invalid_arguments_rejected_without_device():
     assert L.nttb_rns_plan_create(30, None, 0, 0, ctypes.byref(h)) == 1  # no moduli
     assert L.nttb_u64_transform(None, None, 1, 0, 0, None) == 1
     assert L.nttb_rns_transform(None, None, None, 1, 0, 0, None) == 1
+    rid = ctypes.c_uint64()
+    assert L.nttb_u64_pretransposed_transform(None, None, 64, 0, None) == 1
+    assert L.nttb_server_submit_ntt(None, None, None, 10, 1, 0, 0, ctypes.byref(rid)) == 1
+    assert b"null" in L.nttb_last_error()
+    assert L.nttb_u64_transpose(None, None, 32, 32, None) == 1
+    assert L.nttb_u64_bit_reverse(None, 1024, None) == 1
+    p = (ctypes.c_uint32 * 5)(*([1] * 5))
+    buf = ctypes.c_void_p(16)  # never dereferenced: K = 5 is refused first
+    assert L.nttb_klimb_forward(5, buf, buf, 1 << 10, 10, p, 1, None) == 2  # K not served
+    assert b"K = 5" in L.nttb_last_error()
 
 
 def test_dropin_headers_compile_reference_test_programs():
