@@ -170,4 +170,11 @@ def test_server_cyclic_products(torch_cuda):
         srv.wait(i)
     for r, o in zip(reqs, outs):
         assert (o == product(r[0], r[1], PRIMES[r[4]:r[4] + r[3]], False)).all()
+    # cyclic NTT requests, the smallest size and the largest the server takes
+    for lg, inv in ((1, False), (13, False), (13, True), (7, True)):
+        x, _, lgx, limbs, first = request(rng, (lg, lg), (2, 2))
+        out = np.zeros_like(x)
+        srv.wait(srv.submit_ntt(x, out, lgx, limbs, first, inverse=inv))
+        want = O.rns(x[None].astype(np.uint64), PRIMES[first:first + limbs], negacyclic=False, inverse=inv)[0]
+        assert (out == want.astype(np.uint32)).all(), (lg, inv)
     srv.close()
