@@ -183,6 +183,35 @@ def test_pretransposed_transform_every_size(torch_cuda, lg, n1):
         assert (to_host(d2, np.uint64) == O.rowmaj_forward(O.to_pretransposed(x, 64, 64), BABYBEAR)).all()
 
 
+@pytest.mark.parametrize("n1", [64, 16])
+def test_pretransposed_transform_60bit_prime(torch_cuda, n1):
+    """The 64-bit Montgomery plan takes the transpose route for every shape."""
+    g = golden("q60.npz")
+    q = int(g["q"])
+    n = 1 << 12
+    x = rand(n, q, 60 + n1)
+    plan = nb.Plan(n, q)
+    d = to_dev(torch_cuda, O.to_pretransposed(x, n1, n // n1))
+    plan.pretransposed_transform(d, n1)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == O.to_pretransposed(O.ntt(x, q), n1, n // n1)).all()
+    plan.pretransposed_transform(d, n1, inverse=True)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(d, np.uint64) == O.to_pretransposed(x, n1, n // n1)).all()
+
+
+@pytest.mark.parametrize("rows,cols", [(32, 1 << 20), (1 << 20, 32), (64, 1 << 18)])
+def test_transpose_tall_and_wide(torch_cuda, rows, cols):
+    """One row or one column of TMA tiles across 2^20 words."""
+    x = np.random.default_rng(rows + cols).integers(0, 1 << 63, rows * cols, dtype=np.uint64)
+    src = to_dev(torch_cuda, x)
+    dst = torch_cuda.empty_like(src)
+    nb.transpose_u64(dst, src, rows, cols)
+    torch_cuda.cuda.synchronize()
+    assert (to_host(dst, np.uint64) == x.reshape(rows, cols).T.reshape(-1)).all()
+    assert nb.device_errors() == 0
+
+
 def test_pretransposed_square_runs_without_transposes(torch_cuda):
     """n = M^2, n1 = M: two scalar passes read and write the layout directly
     (no transpose kernel runs); the result is the pre-transposed transform."""
