@@ -99,7 +99,10 @@ NTTB_API int nttb_plan_get_info(const nttb_plan* plan, nttb_plan_info* out);
 /* Natural-order cyclic NTT over `batch` contiguous polynomials of n words,
  * in place.  Replaces ntt_forward/inverse_{basic,tlmop,optimized}
  * (src/ntt_basic.cu:268-334, src/ntt_optimized.cu:515-613) and
- * ntt_forward/inverse_batch (src/ntt_basic.cu:337-389). */
+ * ntt_forward/inverse_batch (src/ntt_basic.cu:337-389).  NTTB_ENGINE_AUTO
+ * runs the INT8 tensor-core kernel on the words directly for n = 2^16 and
+ * q < 2^31 from 8 polynomials on, the CUDA-core engine otherwise (residues
+ * must be below 2^32, as the reference's kernels assume them below q). */
 NTTB_API int nttb_u64_transform(const nttb_plan* plan, uint64_t* d_data, uint64_t batch, int inverse, int engine,
                        void* stream);
 /* The reference's four-step map, in place.  Replaces
