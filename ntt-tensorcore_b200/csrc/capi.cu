@@ -562,7 +562,7 @@ int nttb_rns_forward_inverse(const nttb_rns_plan* P, uint32_t* d, uint32_t n_pol
     if (((uintptr_t)d) & 15) return fail(NTTB_ERR_INVALID_ARG, "rns_forward_inverse: pointer must be 16-byte aligned");
     Plan32& p = const_cast<Plan32&>(P->p);
     cudaStream_t s = (cudaStream_t)stream;
-    int eng = engine == NTTB_ENGINE_AUTO ? auto_engine32(p, false, 0) : engine;
+    int eng = engine == NTTB_ENGINE_AUTO ? auto_engine32(p, false, (uint64_t)n_polys * p.n_limbs) : engine;
     int rc;
     if (eng == NTTB_ENGINE_INT8) {
         rc = int8_forward_inverse32(p, d, n_polys, s);
@@ -582,7 +582,7 @@ int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_ds
     Plan32& p = P->p;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t bw = (size_t)n_polys * p.n_limbs * p.n;
-    const int eng = engine == NTTB_ENGINE_AUTO ? auto_engine32(p, false, 0) : engine;
+    const int eng = engine == NTTB_ENGINE_AUTO ? auto_engine32(p, false, (uint64_t)n_polys * p.n_limbs) : engine;
     nttb::HostStream*& H = P->hs;
     if (!H || H->words < bw) {  // (re)build the buffers, streams and events
         nttb::host_stream_free(H);
