@@ -39,7 +39,9 @@ enum {
     NTTB_ERR_BUDGET = 6       /* serving admission refused: HBM budget exceeded */
 };
 
-/* Inner-DFT engines.  AUTO picks the fastest one that serves the request. */
+/* Inner-DFT engines.  AUTO picks the fastest one that serves the request:
+ * the INT8 tensor-core kernel at N = 2^16 from 8 (polynomial, limb) units
+ * on, the CUDA-core engine otherwise. */
 enum {
     NTTB_ENGINE_AUTO = 0,
     NTTB_ENGINE_SCALAR = 1, /* CUDA-core radix-2 in shared memory */
