@@ -93,6 +93,12 @@ __global__ void __launch_bounds__(256) klimb_group(uint32_t* data, const uint32_
                                                    uint32_t r, uint32_t logC, Limbs<K> p, uint32_t np,
                                                    bool fused_bitrev) {
     extern __shared__ uint32_t sm[];
+    // a one-warp tile (small transforms) needs only the warp's barrier
+    const bool one_warp = blockDim.x <= 32;
+    auto tile_sync = [&]() {
+        if (one_warp) __syncwarp();
+        else __syncthreads();
+    };
     const uint32_t E = 1u << (r + logC), C = 1u << logC;
     const uint32_t chunks = (1u << s0) >> logC;  // column chunks per group of 2^(s0 + r)
     const uint32_t G = blockIdx.x / chunks, low0 = (blockIdx.x % chunks) << logC;
@@ -104,7 +110,7 @@ __global__ void __launch_bounds__(256) klimb_group(uint32_t* data, const uint32_
 #pragma unroll
         for (int k = 0; k < K; k++) sm[k * E + e] = src[k];
     }
-    __syncthreads();
+    tile_sync();
     for (uint32_t t = 0; t < r; t++) {
         const uint32_t half = 1u << t, tshift = log_n - s0 - t - 1;
         for (uint32_t bf = threadIdx.x; bf < E / 2; bf += blockDim.x) {
@@ -129,7 +135,7 @@ __global__ void __launch_bounds__(256) klimb_group(uint32_t* data, const uint32_
                 sm[k * E + ehi] = u[k];
             }
         }
-        __syncthreads();
+        tile_sync();
     }
     for (uint32_t e = threadIdx.x; e < E; e += blockDim.x) {
         const size_t i = base + ((size_t)(e >> logC) << s0) + (e & (C - 1));
