@@ -70,3 +70,12 @@ def test_reference_timing_compare_runs():
     r = subprocess.run([path, "6", "8", "10", "12"], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, (r.stdout + r.stderr)[-3000:]
     assert "LEGEND" in r.stdout
+
+
+def test_icicle_harness_forward_matches_host():
+    """oracle/harness_compare.cu (the timing convention of the reference's
+    tests/icicle_compare.cu) on the drop-in: every timed size's forward equals
+    ntt_host on the same seeded input."""
+    rc, out = run("harness")
+    assert rc == 0, out[-2000:]
+    assert out.count("equal") == 7 and "DIFFERENT" not in out, out[-2000:]
