@@ -314,12 +314,15 @@ NTTB_API int nttb_server_submit(nttb_server* server, const uint32_t* a, const ui
  * `in` per limb; NTTB_ERR_BUDGET if its operand alone exceeds the request region. */
 NTTB_API int nttb_server_submit_ntt(nttb_server* server, const uint32_t* in, uint32_t* out, uint32_t log_n,
                                     uint32_t n_limbs, uint32_t first_modulus, int inverse, uint64_t* id);
-/* Waits for one request (NTTB_ERR_TIMEOUT after timeout_s); its latency in seconds. */
+/* Waits for one request (NTTB_ERR_TIMEOUT after timeout_s); its latency in seconds.
+ * A request's record (status, latency) is kept until a wait collects it, so
+ * every id should be waited for once; a second wait on it is refused. */
 NTTB_API int nttb_server_wait(nttb_server* server, uint64_t id, double timeout_s, double* latency_s);
 NTTB_API int nttb_server_drain(nttb_server* server, double timeout_s);
 NTTB_API int nttb_server_stats(nttb_server* server, nttb_server_stats_t* out);
 /* Latencies of completed requests in completion order (count = how many
- * there are; up to cap copied); reset != 0 forgets them. */
+ * there are; up to cap copied); reset != 0 forgets them.  They accumulate
+ * (8 bytes a request) until a reset. */
 NTTB_API int nttb_server_latencies(nttb_server* server, double* out, uint64_t cap, uint64_t* count, int reset);
 /* Drains, then releases the server. */
 NTTB_API int nttb_server_destroy(nttb_server* server);

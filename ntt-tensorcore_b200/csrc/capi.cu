@@ -378,8 +378,11 @@ int nttb_plan_create(uint64_t n, uint64_t q, nttb_plan** out) {
         nttb_plan_destroy(P);
         return fail(NTTB_ERR_NO_MEMORY, "plan_create: cudaMalloc failed");
     }
-    cudaMemcpy(P->d_twiddles, tw.data(), n * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(P->d_twiddles_inv, twi.data(), n * 8, cudaMemcpyHostToDevice);
+    if (cudaMemcpy(P->d_twiddles, tw.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(P->d_twiddles_inv, twi.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        nttb_plan_destroy(P);
+        return fail(NTTB_ERR_CUDA, "plan_create: twiddle upload: %s", cudaGetErrorString(cudaGetLastError()));
+    }
     P->ar64.q = q;
     P->ar64.qinv = h_neg_inv64(q);
     P->r2_64 = h_to_mont64(h_to_mont64(1, q), q);
@@ -530,7 +533,10 @@ int nttb_rns_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_limb
         nttb_rns_plan_destroy(P);
         return fail(NTTB_ERR_NO_MEMORY, "rns_plan_create: cudaMalloc failed");
     }
-    cudaMemcpy(P->d_r2, r2.data(), n_limbs * 4, cudaMemcpyHostToDevice);
+    if (cudaMemcpy(P->d_r2, r2.data(), n_limbs * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+        nttb_rns_plan_destroy(P);
+        return fail(NTTB_ERR_CUDA, "rns_plan_create: table upload: %s", cudaGetErrorString(cudaGetLastError()));
+    }
     *out = P;
     return cuda_status("rns_plan_create");
 }

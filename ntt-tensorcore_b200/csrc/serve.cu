@@ -386,10 +386,19 @@ NTTB_API int nttb_server_wait(nttb_server* s, uint64_t id, double timeout_s, dou
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return fail(NTTB_ERR_INVALID_ARG, "nttb_server_wait: unknown request %llu", (unsigned long long)id);
-    const bool done = s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return s->reqs[id].done; });
+    // find() rather than operator[]: a concurrent wait on the same id may
+    // collect (erase) the record while this one sleeps
+    const bool done = s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+        auto w = s->reqs.find(id);
+        return w == s->reqs.end() || w->second.done;
+    });
     if (!done) return fail(NTTB_ERR_TIMEOUT, "nttb_server_wait: request %llu not done", (unsigned long long)id);
-    const nttb::Req r = s->reqs[id];
-    s->reqs.erase(id);
+    it = s->reqs.find(id);
+    if (it == s->reqs.end())
+        return fail(NTTB_ERR_INVALID_ARG, "nttb_server_wait: request %llu collected by another wait",
+                    (unsigned long long)id);
+    const nttb::Req r = it->second;
+    s->reqs.erase(it);
     if (latency_s) *latency_s = r.t_done - r.t_submit;
     return r.status == NTTB_OK ? NTTB_OK : fail(r.status, "nttb_server_wait: request %llu failed", (unsigned long long)id);
 }

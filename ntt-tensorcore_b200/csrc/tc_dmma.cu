@@ -289,8 +289,12 @@ int build_dm(Plan32& p, DmCache* c) {
         cudaFree(d_tabs);
         return 4;
     }
-    cudaMemcpy(d_l, fwd.data(), nl * sizeof(DmLimb), cudaMemcpyHostToDevice);
-    cudaMemcpy(d_l + nl, inv.data(), nl * sizeof(DmLimb), cudaMemcpyHostToDevice);
+    if (cudaMemcpy(d_l, fwd.data(), nl * sizeof(DmLimb), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_l + nl, inv.data(), nl * sizeof(DmLimb), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d_l);
+        cudaFree(d_tabs);
+        return 3;
+    }
     c->d_fwd = d_l;
     c->d_inv = d_l + nl;
     c->d_tabs = d_tabs;
