@@ -1687,32 +1687,32 @@ NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jo
         for (uint32_t split = 0; split < 2; split++)
             for (uint32_t lag : lags)
                 for (uint32_t grp : groups) {
-                nttb_batch_config c = nttb::default_config();
-                c.tile_elems = sh[0];
-                c.threads = sh[1];
-                c.tensor = sh[2];
-                if (c.tensor && !plan->p.images) continue;
-                c.split = split;
-                c.lag = lag;
-                c.group = grp;
-                Batch* b = nullptr;
-                if (nttb::create_batch(&plan->p, sample.data(), (uint32_t)sample.size(), c, &b)) continue;
-                float t_min = 1e30f;
-                for (int it = 0; it < 4 && rc == 0; it++) {
-                    cudaEventRecord(e0, s);
-                    rc = nttb::launch_batch(b, s, false);
-                    cudaEventRecord(e1, s);
-                    cudaEventSynchronize(e1);
-                    float ms = 0;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    if (it > 0) t_min = std::min(t_min, ms);  // the first run warms up
-                }
-                nttb::free_batch(b);
-                if (rc) break;
-                if (t_min < best) {
-                    best = t_min;
-                    best_cfg = c;
-                }
+                    if (rc) continue;  // a failed launch ends the search
+                    nttb_batch_config c = nttb::default_config();
+                    c.tile_elems = sh[0];
+                    c.threads = sh[1];
+                    c.tensor = sh[2];
+                    if (c.tensor && !plan->p.images) continue;
+                    c.split = split;
+                    c.lag = lag;
+                    c.group = grp;
+                    Batch* b = nullptr;
+                    if (nttb::create_batch(&plan->p, sample.data(), (uint32_t)sample.size(), c, &b)) continue;
+                    float t_min = 1e30f;
+                    for (int it = 0; it < 4 && rc == 0; it++) {
+                        cudaEventRecord(e0, s);
+                        rc = nttb::launch_batch(b, s, false);
+                        cudaEventRecord(e1, s);
+                        cudaEventSynchronize(e1);
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (it > 0) t_min = std::min(t_min, ms);  // the first run warms up
+                    }
+                    nttb::free_batch(b);
+                    if (!rc && t_min < best) {
+                        best = t_min;
+                        best_cfg = c;
+                    }
                 }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
