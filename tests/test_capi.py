@@ -104,3 +104,14 @@ def test_dropin_headers_compile_reference_test_programs():
                         "-I" + os.path.join(ROOT, "include"), "-c", ref, "-o", out],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_harness_program_compiles_against_dropin_headers():
+    """oracle/harness_compare.cu needs only the drop-in's include/ntt.cuh."""
+    src = os.path.join(ROOT, "oracle", "harness_compare.cu")
+    out = os.path.join(ROOT, "_work", "harness_compile_check.o")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    r = subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I" + os.path.join(ROOT, "include"), "-c", src, "-o", out],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
