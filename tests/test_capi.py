@@ -93,24 +93,22 @@ def test_invalid_arguments_rejected_without_device():
     assert b"K = 5" in L.nttb_last_error()
 
 
-def test_dropin_headers_compile_reference_test_programs():
+def test_dropin_headers_compile_reference_test_programs(tmp_path):
     """The reference's own test sources compile against include/ntt.cuh (drop-in)."""
     ref = "/root/reference/tests/test_ntt.cu"
     if not os.path.exists(ref):
         pytest.skip("reference tree not present")
-    out = os.path.join(ROOT, "_work", "dropin_compile_check.o")
-    os.makedirs(os.path.dirname(out), exist_ok=True)
+    out = str(tmp_path / "dropin_compile_check.o")
     r = subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
                         "-I" + os.path.join(ROOT, "include"), "-c", ref, "-o", out],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
 
 
-def test_harness_program_compiles_against_dropin_headers():
+def test_harness_program_compiles_against_dropin_headers(tmp_path):
     """oracle/harness_compare.cu needs only the drop-in's include/ntt.cuh."""
     src = os.path.join(ROOT, "oracle", "harness_compare.cu")
-    out = os.path.join(ROOT, "_work", "harness_compile_check.o")
-    os.makedirs(os.path.dirname(out), exist_ok=True)
+    out = str(tmp_path / "harness_compile_check.o")
     r = subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
                         "-I" + os.path.join(ROOT, "include"), "-c", src, "-o", out],
                        capture_output=True, text=True)
