@@ -53,7 +53,7 @@ def test_psi_squares_to_omega():
         assert pow(psi, n, q) == q - 1
 
 
-@pytest.mark.parametrize("lg", [1, 2, 6, 10, 12])
+@pytest.mark.parametrize("lg", [0, 1, 2, 6, 10, 12])
 def test_host_ntt_matches_oracle(lg):
     rng = np.random.default_rng(lg)
     for q in (BABYBEAR, Q60):

@@ -84,6 +84,21 @@ def test_oracle_vs_reference_cpu_random():
 
 
 @pytest.mark.skipif(not HAVE_REF, reason="reference library not built")
+def test_oracle_vs_reference_cpu_smallest_sizes():
+    """n = 1, 2, 4: the reference's ntt_host (src/ntt_basic.cu:412-463) and the
+    restatement agree at the edge of the size range, including n = 1
+    (omega = 1, identity forward and inverse)."""
+    rng = np.random.default_rng(13)
+    for q in (BABYBEAR, Q60):
+        for lg in (0, 1, 2):
+            x = rng.integers(0, q, 1 << lg, dtype=np.uint64)
+            for inv in (False, True):
+                assert (O.ntt(x, q, inv) == O.ref_ntt_host(x, q, inv)).all()
+        x = rng.integers(0, q, 1, dtype=np.uint64)
+        assert (O.ntt(x, q, False) == x).all() and (O.ntt(x, q, True) == x).all()
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference library not built")
 def test_reference_batch_driver_negacyclic():
     rng = np.random.default_rng(12)
     from conftest import GOLDEN  # noqa: F401
