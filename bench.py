@@ -50,7 +50,8 @@ def parse():
                     help="rns: the 24-limb 2^16 negacyclic batch (headline); uneven: 512 polynomials of "
                          "2^12..2^20 residues, 1..32 limbs, mixed directions, one persistent launch; "
                          "serve: Poisson stream of negacyclic products under a 60 GB budget, p50/p99; "
-                         "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse")
+                         "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse; aux: the helper "
+                         "kernels (transposes, bit reversal, pointwise products) against the HBM roofline")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
     ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60", "move", "klimb"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
