@@ -113,3 +113,16 @@ def test_harness_program_compiles_against_dropin_headers(tmp_path):
                         "-I" + os.path.join(ROOT, "include"), "-c", src, "-o", out],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_device_paths_fail_loudly_without_a_gpu():
+    """With no usable CUDA device the product path raises: plans need device
+    memory and there is no host fallback for any transform."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    qs = nb.generate_primes(31, 17, 2)
+    with pytest.raises(nb.NTTError):
+        nb.RnsPlan(16, qs, negacyclic=True)
+    with pytest.raises(nb.NTTError):
+        nb.Plan(1 << 12, BABYBEAR)
