@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "../../include/ntt_b200.h"
+#include "arena.hpp"
 #include "batch.hpp"
 #include "engines.hpp"
 
@@ -46,57 +47,6 @@ namespace {
 double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
-
-constexpr size_t kGranule = 256;
-size_t round_up(size_t x) { return (x + kGranule - 1) / kGranule * kGranule; }
-
-// First-fit allocator over one device region, coalescing on release.
-class Arena {
-   public:
-    void init(size_t bytes) {
-        size_ = bytes / kGranule * kGranule;
-        free_.clear();
-        if (size_) free_[0] = size_;
-    }
-    bool alloc(size_t bytes, size_t* off) {
-        bytes = round_up(bytes);
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < bytes) continue;
-            const size_t o = it->first, rest = it->second - bytes;
-            free_.erase(it);
-            if (rest) free_[o + bytes] = rest;
-            *off = o;
-            used_ += bytes;
-            peak_ = std::max(peak_, used_);
-            return true;
-        }
-        return false;
-    }
-    void release(size_t off, size_t bytes) {
-        bytes = round_up(bytes);
-        used_ -= bytes;
-        auto it = free_.emplace(off, bytes).first;
-        auto nx = std::next(it);
-        if (nx != free_.end() && it->first + it->second == nx->first) {
-            it->second += nx->second;
-            free_.erase(nx);
-        }
-        if (it != free_.begin()) {
-            auto pv = std::prev(it);
-            if (pv->first + pv->second == it->first) {
-                pv->second += it->second;
-                free_.erase(it);
-            }
-        }
-    }
-    size_t size() const { return size_; }
-    size_t used() const { return used_; }
-    size_t peak() const { return peak_; }
-
-   private:
-    std::map<size_t, size_t> free_;
-    size_t size_ = 0, used_ = 0, peak_ = 0;
-};
 
 enum ReqKind : uint32_t { kProduct = 0, kForward = 1, kInverse = 2 };
 
