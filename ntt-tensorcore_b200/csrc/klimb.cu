@@ -24,6 +24,7 @@
 #include "../../include/ntt_b200.h"
 #include "../../include/ntt_limb_arith.cuh"
 #include "engines.hpp"
+#include "klimb_plan.hpp"
 #include "profiler.hpp"
 
 namespace nttb {
@@ -151,15 +152,8 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
     Limbs<K> p;
     for (int k = 0; k < K; k++) p.l[k] = prime[k];
     const uint32_t n = 1u << log_n;
-    // largest tile: 48 KB of shared memory; smaller while a pass would have
-    // fewer than kTargetCtas tiles (small transforms are bound by the latency
-    // of their stage chains, so more, shorter tiles win), but at least 2^6
-    constexpr uint32_t kTargetCtas = 148;
-    uint32_t log_emax = K <= 3 ? 12u : 10u;
-    while (log_emax > 6 && (n >> log_emax) < kTargetCtas) log_emax--;
-    // Small transforms run as one tile in one launch, the bit reversal fused
-    // into its loads (measured: K = 2 up to 2^10, K = 11 up to 2^8).
-    if (log_n <= (K <= 3 ? 10u : 8u)) {
+    const KlimbPlan P = klimb_plan(K, log_n);
+    if (P.single_tile) {
         ProfScope prof("klimb_group", s);
         const uint32_t threads = n / 2 < 256 ? (n / 2 > 0 ? n / 2 : 1) : 256;
         klimb_group<K><<<1, threads, (size_t)n * K * 4, s>>>(d_data, d_tw, log_n, 0, log_n, 0, p, np, true);
@@ -171,22 +165,14 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
         else klimb_bitrev<K><<<(n + 255) / 256, 256, 0, s>>>(d_data, n, log_n);
         if (cudaGetLastError() != cudaSuccess) return 2;
     }
-    uint32_t s0 = 0;
-    while (s0 < log_n) {
-        uint32_t r = log_n - s0, logC = 0;
-        if (s0 == 0) {
-            if (r > log_emax) r = log_emax;
-        } else {
-            if (r > 8) r = 8;
-            if (r > log_emax) r = log_emax;
-            logC = log_emax - r < s0 ? log_emax - r : s0;
-        }
-        const uint32_t E = 1u << (r + logC);
+    for (uint32_t i = 0; i < P.n_passes; i++) {
+        const KlimbPass& ps = P.pass[i];
+        const uint32_t E = 1u << (ps.r + ps.logC);
         const uint32_t threads = E / 2 < 256 ? E / 2 : 256;
         ProfScope prof("klimb_group", s);
-        klimb_group<K><<<n / E, threads, (size_t)E * K * 4, s>>>(d_data, d_tw, log_n, s0, r, logC, p, np, false);
+        klimb_group<K><<<n / E, threads, (size_t)E * K * 4, s>>>(d_data, d_tw, log_n, ps.s0, ps.r, ps.logC, p, np,
+                                                                  false);
         if (cudaGetLastError() != cudaSuccess) return 2;
-        s0 += r;
     }
     return 0;
 }

@@ -2,7 +2,7 @@
 // against a granule bitmap: every allocation lands at the lowest offset
 // whose free run holds it, allocations never overlap, the used and peak
 // counters follow, and releasing everything leaves one free run.
-// Built and run by tests/test_arena.py; prints "ok" and exits 0 on success.
+// Built and run by tests/test_host_cpp.py; prints "ok" and exits 0 on success.
 #include <cstdio>
 #include <cstdlib>
 #include <random>
