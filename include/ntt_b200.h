@@ -336,7 +336,7 @@ NTTB_API int nttb_server_destroy(nttb_server* server);
  * d_tw[k * n / 2^(s+1)] at stage s (d_tw: n Montgomery-form powers of omega,
  * as setup_ntt builds them).  `prime` is a HOST array of K limbs, np =
  * -prime^-1 mod 2^24.  Replaces run_forward_ct, run_forward_ct_tcu
- * (include/ntt_arbitrary.cuh:2556-2646) and run_forward_radix64_scalar
+ * (include/ntt_arbitrary.cuh:2547-2646) and run_forward_radix64_scalar
  * (include/ntt_arbitrary_radix64.cuh:345-389), which compute the same
  * network.  K in {2, 3, 11} (the reference's FieldConfig set), n = 2^log_n,
  * log_n <= 24. */
