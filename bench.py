@@ -97,9 +97,72 @@ def rank_barrier(world):
         dist.barrier()
 
 
+def _is_prime(n):
+    """Deterministic Miller-Rabin for n < 2^64 (the first twelve prime bases)."""
+    if n < 2:
+        return False
+    small = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+    for p in small:
+        if n % p == 0:
+            return n == p
+    d, r = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        r += 1
+    for a in small:
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(r - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def workload_primes(bits, two_adicity, count):
+    """The workload's moduli: the `count` largest primes q < 2^bits with
+    q == 1 mod 2^two_adicity, in descending order (the rule of the library's
+    nttb_generate_primes, restated here so that the reference arm computes its
+    moduli without loading the library)."""
+    step = 1 << two_adicity
+    out, k = [], ((1 << bits) - 1) // step
+    while k > 0 and len(out) < count:
+        q = k * step + 1
+        if q < (1 << bits) and _is_prime(q):
+            out.append(q)
+        k -= 1
+    if len(out) < count:
+        raise ValueError("only %d primes exist" % len(out))
+    return out
+
+
 def moduli():
-    import ntt_b200 as nb
-    return nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
+    return workload_primes(31, TWO_ADICITY, N_LIMBS)
+
+
+def headline_config(world):
+    """The workload description shared by both arms' JSON lines."""
+    batch_bytes = N_LIMBS * (1 << LOG_N) * 4
+    pool_n = max(8, int(np.ceil(2.4 * L2_BYTES / batch_bytes)))
+    return {"workload": WORKLOAD, "n": 1 << LOG_N, "limbs": N_LIMBS, "moduli": "31-bit, q == 1 mod 2^17",
+            "negacyclic": True, "transforms_per_step": 2,
+            "l2": "inputs rotate through %d batches (%d MB of uint32 residues) > 2x L2" % (pool_n, pool_n * batch_bytes >> 20),
+            "parallelism": "replicas x%d" % world}
+
+
+def load_peaks():
+    """(peaks dict, source) from MEASURED_PEAKS.json, else the fallback figures."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+        if "hbm_gbs" in peaks:
+            return peaks, "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError):
+        pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback (6650 GB/s: no MEASURED_PEAKS.json on this host)"
 
 
 def make_batch(qs, seed):
@@ -323,7 +386,7 @@ def run_ours(args, world, rank, local):
         ms, launches = timed(engine, args.steps)
         return {"metric": METRIC, "value": world * coeffs_per_step * args.steps / (ms / 1e3), "unit": UNIT,
                 "n_gpus": world, "steps": args.steps, "ms_per_step": ms / args.steps, "quick": True,
-                "config": {"workload": WORKLOAD, "engine": engine}, "gpu_launches": launches}, qs
+                "config": headline_config(world), "engine": engine, "gpu_launches": launches}, qs
     clocks = ClockSampler(local)
     clocks.start()
     t_end = time.time() + 1.0
@@ -349,7 +412,14 @@ def run_ours(args, world, rank, local):
     prof = nb.profile_stop()
     top = max(prof.items(), key=lambda kv: kv[1][1])
     k_name, (k_launches, k_ms) = top
-    k_avg_s = k_ms / k_launches / 1e3
+    # Events around each launch add their own overhead, so the per-launch
+    # sums run longer than the back-to-back timed loop.  The dominant
+    # kernel's time is its SHARE of the event sums applied to the timed loop's
+    # device time (with one kernel per step: exactly ms_per_step).
+    ev_total_ms = sum(v[1] for v in prof.values())
+    k_share = k_ms / ev_total_ms
+    # (the profiled loop runs the same steps as the timed one)
+    k_avg_s = ms * k_share / k_launches / 1e3
     # algorithmic bytes: 8 B per coefficient per transform (4 B read + 4 B
     # write of a uint32 residue).  The fused queue kernel runs two transforms
     # (x4 = forward + inverse, 4 stages) or one (x2); a single-pass kernel
@@ -357,13 +427,8 @@ def run_ours(args, world, rank, local):
     coeffs_per_launch = N_LIMBS * (1 << LOG_N)
     transforms = 2 if k_name.endswith("_x4") else 1
     alg_bytes = 8 * coeffs_per_launch * transforms
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peaks, peak_source = load_peaks()
+    peak = peaks["hbm_gbs"]
     achieved = alg_bytes / k_avg_s / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -416,13 +481,13 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded uniform residues",
-        "config": {"workload": WORKLOAD, "n": 1 << LOG_N, "limbs": N_LIMBS, "moduli": "31-bit, q == 1 mod 2^17",
-                   "negacyclic": True, "engine": engine, "l2": "rotating %d batches (%d MB) > 2x L2"
-                   % (pool_n, pool_n * batch_bytes >> 20), "parallelism": "replicas x%d" % world},
+        "config": headline_config(world), "engine": engine,
         "roofline": {"bound": "hbm", "kernel": k_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
-                     "kernel_avg_us": k_avg_s * 1e6, "alg_bytes_per_launch": alg_bytes},
+                     "peak_source": peak_source,
+                     "kernel_avg_us": k_avg_s * 1e6, "kernel_share": k_share,
+                     "kernel_timing": "share of per-launch event time x the timed loop's device time",
+                     "alg_bytes_per_launch": alg_bytes},
         "kernels": {k: {"launches": v[0], "total_ms": v[1]} for k, v in prof.items()},
         "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         "engines_coeffs_per_s": dict(compare, **{engine: value}),
@@ -477,6 +542,60 @@ def uneven_jobs(seed=4):
     return [(int(a), int(b), bool(c)) for a, b, c in zip(lg, limbs, inv)]
 
 
+def uneven_sample(shapes):
+    """(job index, limb) rows checked against the oracle: the first job of
+    every (log2 N, direction) class and of every limb-count bucket (1-8,
+    9-16, 17-24, 25-32), limbs first, middle and last of each."""
+    picked, seen = [], set()
+    for i, (lg, limbs, inv) in enumerate(shapes):
+        for key in (("class", lg, inv), ("bucket", (limbs - 1) // 8)):
+            if key not in seen:
+                seen.add(key)
+                if i not in picked:
+                    picked.append(i)
+    return [(i, l) for i in picked for l in sorted({0, shapes[i][1] // 2, shapes[i][1] - 1})]
+
+
+def uneven_check(torch, nb, plan, jobs, shapes, qs, buf, buf0, config, stream):
+    """Bit-exact check of the full-size batch: restore the inputs, launch the
+    batch once, compare the sampled rows with the oracle's transforms; then
+    launch the batch with every direction flipped and require the inputs
+    back, word for word."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    buf.copy_(buf0)
+    b = plan.batch(jobs, config)
+    b.launch(stream)
+    torch.cuda.synchronize()
+    errors = nb.device_errors()
+    rows = uneven_sample(shapes)
+
+    def one(row):
+        i, l = row
+        view = jobs[i][0]
+        got = view[l].cpu().numpy().view(np.uint32).astype(np.uint64)
+        x = buf0[view.storage_offset() - buf.storage_offset():][:view.numel()].view(view.shape)[l]
+        want = O.rns(x.cpu().numpy().view(np.uint32).astype(np.uint64)[None, None], [qs[l]],
+                     inverse=shapes[i][2])[0, 0]
+        return bool((got == want).all())
+
+    with ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1))) as ex:  # ctypes drops the GIL
+        ok = list(ex.map(one, rows))
+    b.close()
+    flipped = [(v, lg, limbs, first, not inv, nega) for v, lg, limbs, first, inv, nega in jobs]
+    b2 = plan.batch(flipped, config)
+    b2.launch(stream)
+    torch.cuda.synchronize()
+    errors |= nb.device_errors()
+    round_trip = bool(torch.equal(buf, buf0))
+    b2.close()
+    res = {"rows_checked": len(rows), "rows_exact": int(sum(ok)),
+           "jobs_sampled": len({i for i, _ in rows}), "round_trip_exact": round_trip,
+           "words_round_trip": int(buf.numel()), "device_errors": int(errors)}
+    assert all(ok) and round_trip and errors == 0, "uneven batch parity failed: %s" % res
+    return res
+
+
 def run_uneven(args, world, rank, local):
     import torch
     import ntt_b200 as nb
@@ -499,6 +618,7 @@ def run_uneven(args, world, rank, local):
         view.copy_((r % qt[:limbs, None]).to(torch.int32))
         jobs.append((view, lg, limbs, 0, inv, False))
         off += limbs * n
+    buf0 = buf.clone()  # the inputs, for the parity check after the timed steps
     torch.cuda.synchronize()
     coeffs = words  # one transform per residue per launch
     plan = nb.BatchPlan(qs, 20)
@@ -533,13 +653,8 @@ def run_uneven(args, world, rank, local):
     batch.graph_launch(stream)
     g_ms, _ = timed(batch.graph_launch, args.steps)
     value = world * coeffs * args.steps / (ms / 1e3)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peaks, peak_source = load_peaks()
+    peak = peaks["hbm_gbs"]
     avg_s = ms / args.steps / 1e3
     alg_bytes = 8 * coeffs
     # units of two passes move each residue twice (through the workspace ring)
@@ -570,10 +685,11 @@ def run_uneven(args, world, rank, local):
                      "traffic_source": traffic_src,
                      "model_bytes_per_launch": model_bytes, "model_frac": model_bytes / avg_s / 1e9 / peak,
                      "alg_bytes_per_launch": alg_bytes,
-                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"},
+                     "peak_source": peak_source},
         "gpu_launches": launches, "clocks": clk, "e2e": None,
     }
     batch.close()
+    result["parity"] = uneven_check(torch, nb, plan, jobs, shapes, qs, buf, buf0, tuned, stream)
     plan.close()
     if rank == 0 and world == 1:
         result["cpu_baseline"] = cpu_sample([(a, min(b, 8), c, False, False) for a, b, c in shapes], qs)
@@ -607,6 +723,38 @@ def run_serve(args, world, rank, local):
         b = torch.from_numpy((rng.integers(0, 1 << 62, (limbs, 1 << lg), dtype=np.uint64) % mods)
                              .astype(np.uint32).view(np.int32)).pin_memory()
         pool.append((a, b, lg, limbs, first))
+    # Results go to per-entry output buffers (the inputs stay unchanged).
+    # Every CHECK_EVERY-th pool entry is a check entry: each of its requests
+    # writes into a slot of its own ring, and the slot's limbs 0 and last are
+    # compared with the oracle's negacyclic product (forward a, forward b,
+    # pointwise, inverse) before the slot is reused and at the end of every
+    # phase.  That checks every CHECK_EVERY-th product of the stream.
+    CHECK_EVERY, RING = 8, 12
+    outs = [torch.empty_like(a).pin_memory() for a, _, _, _, _ in pool]
+    from oracle import oracle as O
+
+    def oracle_product(a, b, lg, limbs, first, l):
+        q = qs[first + l]
+        x = a.numpy().view(np.uint32).reshape(limbs, 1 << lg)[l].astype(np.uint64)
+        y = b.numpy().view(np.uint32).reshape(limbs, 1 << lg)[l].astype(np.uint64)
+        fa, fb = O.negacyclic(x, q), O.negacyclic(y, q)
+        return O.negacyclic(fa * fb % np.uint64(q), q, inverse=True).astype(np.uint32)
+
+    expect, rings = {}, {}
+    for e in range(0, pool_n, CHECK_EVERY):
+        a, b, lg, limbs, first = pool[e]
+        expect[e] = {l: oracle_product(a, b, lg, limbs, first, l) for l in sorted({0, limbs - 1})}
+        rings[e] = {"bufs": [torch.empty_like(a).pin_memory() for _ in range(RING)], "pending": [None] * RING,
+                    "next": 0}
+    checks = {"products_checked": 0, "mismatches": 0}
+
+    def verify(e, slot):
+        a, b, lg, limbs, first = pool[e]
+        got = rings[e]["bufs"][slot].numpy().view(np.uint32).reshape(limbs, 1 << lg)
+        checks["products_checked"] += 1
+        if not all((got[l] == want).all() for l, want in expect[e].items()):
+            checks["mismatches"] += 1
+        rings[e]["pending"][slot] = None
     # tile configuration tuned on this request mix
     tplan = nb.BatchPlan(qs, 17, negacyclic=True)
     sample = []
@@ -658,12 +806,26 @@ def run_serve(args, world, rank, local):
                 dt = nxt - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
-            a, b, lg, limbs, first = pool[i % pool_n]
-            rid = srv.submit(a, b, a, lg, limbs, first)  # result over a (the pool keeps residues < q)
-            work += coeffs[i % pool_n]
+            e = i % pool_n
+            a, b, lg, limbs, first = pool[e]
+            out = outs[e]
+            if e in rings:  # a check request: its own output slot
+                r = rings[e]
+                slot = r["next"]
+                r["next"] = (slot + 1) % RING
+                if r["pending"][slot] is not None:  # the slot's last request: done, then checked
+                    with lock:
+                        while done[0] <= r["pending"][slot]:
+                            lock.wait(0.01)
+                    verify(e, slot)
+                out = r["bufs"][slot]
+            rid = srv.submit(a, b, out, lg, limbs, first)
+            work += coeffs[e]
             with lock:
                 ids.append(rid)
                 lock.notify_all()
+            if e in rings:
+                rings[e]["pending"][slot] = len(ids) - 1
             i += 1
         t_sub = time.perf_counter() - t0
         with lock:
@@ -671,6 +833,10 @@ def run_serve(args, world, rank, local):
             lock.notify_all()
         th.join()
         t_all = time.perf_counter() - t0
+        for e, r in rings.items():  # every request has completed: check the slots left
+            for slot in range(RING):
+                if r["pending"][slot] is not None:
+                    verify(e, slot)
         lat = np.sort(srv.latencies(reset=True)) * 1e3
         return {"offered_rps": None if rate is None else rate, "requests": i,
                 "achieved_rps": i / t_all, "coeffs_per_s": work / t_all, "submit_s": t_sub,
@@ -699,6 +865,7 @@ def run_serve(args, world, rank, local):
     sat = over_ranks(sat)
     st = srv.stats()
     srv.close()
+    assert checks["mismatches"] == 0, "serving products differ from the oracle: %s" % checks
     cpu = cpu_sample([(lg, limbs, False, True, True) for _, _, lg, limbs, _ in pool], qs) if rank == 0 else None
     return {
         "metric": METRIC, "value": sat["coeffs_per_s"], "unit": UNIT, "n_gpus": world, "steps": sat["requests"],
@@ -707,6 +874,8 @@ def run_serve(args, world, rank, local):
         "config": {"workload": SERVE_WORKLOAD, "n": "2^12..2^17", "limbs": "4..48", "moduli": "48 x 31-bit",
                    "budget_bytes": budget, "slots": 3, "max_batch_requests": 64, "tuned": tuned,
                    "closed_loop_outstanding": outstanding, "parallelism": "replicas x%d" % world},
+        "parity": dict(checks, rule="every %d-th product of the stream (one pool entry in %d), limbs 0 and last, "
+                                    "vs the oracle's negacyclic product" % (CHECK_EVERY, CHECK_EVERY)),
         "serve": {"saturated": sat, "load_levels": levels, "batches": st["batches"],
                   "mean_batch_requests": st["batched_requests"] / max(1, st["batches"]),
                   "peak_region_bytes_in_use": st["peak_bytes_in_use"], "resident_bytes": st["resident_bytes"]},
@@ -771,25 +940,24 @@ def run_q60(args, world, rank, local):
     assert (got == host).all(), "q60 round trip failed"
     coeffs = 2 << lg
     value = world * coeffs * args.steps / (ms / 1e3)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peaks, peak_source = load_peaks()
+    peak = peaks["hbm_gbs"]
     achieved = 16 * coeffs / (ms / args.steps / 1e3) / 1e9  # 8 B read + 8 B write per residue per transform
     cpu = None
     try:
         from oracle import oracle as O
-        if O.ref() is not None:
-            x = host.copy()
+        if O.ref() is not None and rank == 0 and world == 1:
+            # the reference's ntt_host (__int128) on all host threads: one
+            # 2^20 polynomial per thread, forward then inverse
+            threads = max(1, os.cpu_count() or 1)
+            x = np.tile(host, (threads, 1)).reshape(threads, 1, 1 << lg).copy()
             t0 = time.perf_counter()
-            y = O.ref_ntt_host(x, Q60)
-            O.ref_ntt_host(y, Q60, inverse=True)
+            used = O.ref_host_batch(x, [Q60], inverse=False, threads=threads)
+            O.ref_host_batch(x, [Q60], inverse=True, threads=threads)
             dt = time.perf_counter() - t0
-            cpu = {"value": coeffs / dt, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": "1 x 2^20 forward + inverse (ntt_host, __int128)"}
+            assert (x[0, 0] == host).all(), "reference round trip failed"
+            cpu = {"value": threads * coeffs / dt, "unit": UNIT, "cores": used, "kind": "reference",
+                   "sample": "%d x 2^20 forward + inverse, one polynomial per thread (ntt_host, __int128)" % threads}
     except Exception as e:  # reference library missing on this host
         cpu = {"unavailable": str(e)[:200]}
     return {
@@ -818,13 +986,8 @@ def run_aux(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    peak = peaks.get("hbm_gbs", 6650.0)
+    peaks, peak_source = load_peaks()
+    peak = peaks["hbm_gbs"]
 
     def timed(fn, steps):
         # seconds per launch on the slowest rank (the figures are per GPU)
@@ -863,7 +1026,7 @@ def run_aux(args, world, rank, local):
     for v in out.values():
         v["frac"] = v["gbs"] / peak
     return {"metric": "HBM GB/s of the memory-bound helper passes", "unit": "GB/s", "peak": peak,
-            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
+            "peak_source": peak_source,
             "kernels": out, "n_gpus": world, "steps": args.steps}
 
 
@@ -987,10 +1150,11 @@ def main():
         qs = moduli()
         r = cpu_reference(qs, args.steps, args.warmup)
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3,
+                "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u64", "data": "synthetic: seeded uniform residues",
-                "config": {"workload": WORKLOAD, "n": 1 << LOG_N, "limbs": N_LIMBS, "negacyclic": True,
-                           "parallelism": "host threads"},
+                "config": headline_config(world),
+                "engine": "the reference's ntt_host (CPU), all host threads",
                 "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
                                  "sample": r["sample"]},
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -176,11 +176,16 @@ NTTB_API int nttb_rns_stream_host(nttb_rns_plan* plan, const uint32_t* h_src, ui
  * the allocator because cudaMalloc can synchronize the device, a fixed
  * up-front memory budget).  The first pass is staged in a static device
  * buffer of NTTB_NOALLOC_SCRATCH_BYTES that every GPU loading the library
- * holds until exit; batches needing more (n_polys * n_limbs * n * 4 bytes)
- * are rejected with NTTB_ERR_INVALID_ARG.  The first call on a device looks
- * up the buffer's address (cudaGetSymbolAddress): make it before any stream
- * capture.  Calls share the buffer: calls whose work overlaps on the GPU
- * race.  Runs the CUDA-core engine; same results as nttb_rns_transform. */
+ * holds until exit.  Shapes that run in two passes (n > 8192, or n >= 4096
+ * with fewer than 8 (polynomial, limb) units) stage n_polys * n_limbs * n * 4
+ * bytes there, and batches needing more are rejected with
+ * NTTB_ERR_INVALID_ARG; one-pass shapes stage nothing and are not limited.
+ * The plan's device must be the current device (else NTTB_ERR_INVALID_ARG).
+ * The first call on a device looks up the buffer's address
+ * (cudaGetSymbolAddress) and keeps it: make that call before any stream
+ * capture, and do not call again on a device after cudaDeviceReset.  Calls
+ * share the buffer: calls whose work overlaps on the GPU race.  Runs the
+ * CUDA-core engine; same results as nttb_rns_transform. */
 #define NTTB_NOALLOC_SCRATCH_BYTES (8u << 20)
 NTTB_API int nttb_rns_transform_noalloc(const nttb_rns_plan* plan, uint32_t* d_data, uint32_t n_polys, int inverse,
                                         void* stream);

@@ -38,6 +38,25 @@ int cuda_status(const char* what) {
     return NTTB_OK;
 }
 
+static thread_local cudaError_t g_launch_error = cudaSuccess;
+
+int launch_rc() {
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return 0;
+    g_launch_error = e;
+    return 2;
+}
+
+int engine_status(int rc, const char* what) {
+    if (rc == 0) return cuda_status(what);
+    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "%s: shape not served by the requested engine", what);
+    cudaError_t e = g_launch_error;
+    g_launch_error = cudaSuccess;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return fail(NTTB_ERR_CUDA, "%s: launch failed: %s", what,
+                e == cudaSuccess ? "no CUDA error recorded (engine set-up failed)" : cudaGetErrorString(e));
+}
+
 uint64_t reference_generator(uint64_t q);
 
 // ---- small elementwise kernels ---------------------------------------------
@@ -426,17 +445,14 @@ int nttb_u64_transform(const nttb_plan* P, uint64_t* d, uint64_t batch, int inve
     } else {
         rc = run_transform32(const_cast<Plan32&>(P->p32), d, d, true, (uint32_t)batch, inverse != 0, engine, s);
     }
-    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "u64_transform: size not served");
-    if (rc) return cuda_status("u64_transform");
-    return cuda_status("u64_transform");
+    return engine_status(rc, "u64_transform");
 }
 
 int nttb_u64_four_step(const nttb_plan* P, uint64_t* d, int inverse, void* stream) {
     if (!P || !d) return fail(NTTB_ERR_INVALID_ARG, "four_step: null argument");
     if (P->wide) return fail(NTTB_ERR_UNSUPPORTED, "four_step: q must be < 2^31");
     int rc = scalar_four_step32(P->p32, d, P->d_scratch, inverse != 0, (cudaStream_t)stream);
-    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "four_step: size not served");
-    return cuda_status("four_step");
+    return engine_status(rc, "four_step");
 }
 
 int nttb_u64_transpose(uint64_t* dst, const uint64_t* src, uint64_t rows, uint64_t cols, void* stream) {
@@ -558,8 +574,7 @@ int nttb_rns_transform(const nttb_rns_plan* P, uint32_t* dst, const uint32_t* sr
     if ((((uintptr_t)dst) | ((uintptr_t)src)) & 15) return fail(NTTB_ERR_INVALID_ARG, "rns_transform: pointers must be 16-byte aligned");
     int rc = run_transform32(const_cast<Plan32&>(P->p), src, dst, false, n_polys, inverse != 0, engine,
                              (cudaStream_t)stream);
-    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_transform: shape not served by the requested engine");
-    return cuda_status("rns_transform");
+    return engine_status(rc, "rns_transform");
 }
 
 int nttb_rns_forward_inverse(const nttb_rns_plan* P, uint32_t* d, uint32_t n_polys, int engine, void* stream) {
@@ -576,8 +591,7 @@ int nttb_rns_forward_inverse(const nttb_rns_plan* P, uint32_t* d, uint32_t n_pol
         rc = run_transform32(p, d, d, false, n_polys, false, eng, s);
         if (!rc) rc = run_transform32(p, d, d, false, n_polys, true, eng, s);
     }
-    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_forward_inverse: shape not served by the requested engine");
-    return cuda_status("rns_forward_inverse");
+    return engine_status(rc, "rns_forward_inverse");
 }
 
 int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_dst, uint32_t n_polys, uint32_t n_batches,
@@ -639,8 +653,7 @@ int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_ds
         } else {
             rc = run_transform32(p, H->dbuf[k], H->dbuf[k], false, n_polys, mode == 1, eng, s);
         }
-        if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_stream_host: shape not served by the requested engine");
-        if (rc) return fail(NTTB_ERR_CUDA, "rns_stream_host: launch failed");
+        if (rc) return engine_status(rc, "rns_stream_host");
         cudaEventRecord(H->ev_c[k], s);
         for (int c = 0; c < 2; c++) {
             const size_t off = c ? half : 0, len = c ? (bw > half ? bw - half : 0) : std::min(half, bw);
@@ -698,8 +711,7 @@ int nttb_wide_transform(const nttb_wide_plan* P, uint64_t* dst, const uint64_t* 
     if (!P || !dst || !src) return fail(NTTB_ERR_INVALID_ARG, "wide_transform: null argument");
     if (n_polys == 0) return NTTB_OK;
     int rc = scalar_transform64(const_cast<Plan64&>(P->p), src, dst, n_polys, inverse != 0, (cudaStream_t)stream);
-    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "wide_transform: shape not served");
-    return cuda_status("wide_transform");
+    return engine_status(rc, "wide_transform");
 }
 
 }  // extern "C"

@@ -157,13 +157,13 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
         ProfScope prof("klimb_group", s);
         const uint32_t threads = n / 2 < 256 ? (n / 2 > 0 ? n / 2 : 1) : 256;
         klimb_group<K><<<1, threads, (size_t)n * K * 4, s>>>(d_data, d_tw, log_n, 0, log_n, 0, p, np, true);
-        return cudaGetLastError() == cudaSuccess ? 0 : 2;
+        return launch_rc();
     }
     {
         ProfScope prof("klimb_bitrev", s);
         if (log_n >= 8) klimb_bitrev_tiled<K><<<n >> 8, 256, 0, s>>>(d_data, log_n);
         else klimb_bitrev<K><<<(n + 255) / 256, 256, 0, s>>>(d_data, n, log_n);
-        if (cudaGetLastError() != cudaSuccess) return 2;
+        if (launch_rc()) return 2;
     }
     for (uint32_t i = 0; i < P.n_passes; i++) {
         const KlimbPass& ps = P.pass[i];
@@ -172,7 +172,7 @@ int klimb_forward(uint32_t* d_data, const uint32_t* d_tw, uint32_t log_n, const 
         ProfScope prof("klimb_group", s);
         klimb_group<K><<<n / E, threads, (size_t)E * K * 4, s>>>(d_data, d_tw, log_n, ps.s0, ps.r, ps.logC, p, np,
                                                                   false);
-        if (cudaGetLastError() != cudaSuccess) return 2;
+        if (launch_rc()) return 2;
     }
     return 0;
 }

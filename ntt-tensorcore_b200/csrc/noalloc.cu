@@ -13,7 +13,9 @@
 // process exits.  Host code cannot use the array's name as a device address;
 // the first call on each device looks the address up with
 // cudaGetSymbolAddress (with that device current) and caches it.  Make that
-// first call before any stream capture.  All calls share the one buffer and
+// first call before any stream capture.  The cached address is not looked up
+// again: after cudaDeviceReset a process must not call this entry point
+// again on that device.  The plan's device must be the current device.  All calls share the one buffer and
 // it keeps the previous call's contents: the first pass writes every word
 // the second pass reads, so nothing needs clearing, but two calls whose work
 // overlaps on the GPU (different streams, no ordering) race on the buffer.
@@ -73,7 +75,12 @@ extern "C" int nttb_rns_transform_noalloc(const nttb_rns_plan* plan, uint32_t* d
     if (n_polys == 0) return NTTB_OK;
     if (n_polys > 65535) return fail(NTTB_ERR_INVALID_ARG, "rns_transform_noalloc: n_polys > 65535");
     if (((uintptr_t)d_data) & 15) return fail(NTTB_ERR_INVALID_ARG, "rns_transform_noalloc: pointer must be 16-byte aligned");
-    const size_t need = (size_t)n_polys * p->n_limbs * p->n * sizeof(uint32_t);
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != p->device)
+        return fail(NTTB_ERR_INVALID_ARG,
+                    "rns_transform_noalloc: the plan's device (%d) must be the current device (%d)", p->device, dev);
+    // shapes that run as one pass stage nothing and are not limited
+    const size_t need = scalar_transform32_ws_bytes(*p, n_polys);
     if (need > NTTB_NOALLOC_SCRATCH_BYTES)
         return fail(NTTB_ERR_INVALID_ARG,
                     "rns_transform_noalloc: batch needs %zu bytes of scratch; the static scratch holds %u bytes "
@@ -82,9 +89,6 @@ extern "C" int nttb_rns_transform_noalloc(const nttb_rns_plan* plan, uint32_t* d
     int status = NTTB_OK;
     uint32_t* ws = scratch_address(&status);
     if (!ws) return status;
-    int rc = scalar_transform32_ws(*p, d_data, ws, n_polys, inverse != 0, (cudaStream_t)stream);
-    if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "rns_transform_noalloc: size not served");
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(NTTB_ERR_CUDA, "rns_transform_noalloc: %s", cudaGetErrorString(e));
-    return NTTB_OK;
+    const int rc = scalar_transform32_ws(*p, d_data, ws, n_polys, inverse != 0, (cudaStream_t)stream);
+    return engine_status(rc, "rns_transform_noalloc");
 }

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -105,6 +106,9 @@ static int build_common(PlanT* p, uint32_t log_n, const uint64_t* moduli, uint32
     p->n = 1u << log_n;
     p->n_limbs = n_limbs;
     p->negacyclic = negacyclic;
+    if constexpr (std::is_same<PlanT, Plan32>::value) {
+        if (cudaGetDevice(&p->device) != cudaSuccess) p->device = -1;
+    }
     const uint64_t n = p->n;
     if (n_limbs == 0) { *why = "no moduli"; return 1; }
     p->limbs.resize(n_limbs);

@@ -81,6 +81,7 @@ struct Plan32 {
     std::mutex engine_mu;             // guards the lazy construction of engine_data
     void* ws = nullptr;               // workspace for in-place multi-pass transforms
     size_t ws_bytes = 0;
+    int device = -1;                  // the CUDA device holding d_limbs and the tables
 };
 
 // A u64-residue plan (q < 2^62).
@@ -93,6 +94,15 @@ struct Plan64 {
     void* ws = nullptr;
     size_t ws_bytes = 0;
 };
+
+// Status of the kernel launch just made: 0, or 2 after keeping its CUDA
+// error for the C-ABI's message (cudaGetLastError clears a launch error, so
+// the caller could not read it again).
+int launch_rc();
+// C-ABI status of an engine's return code: 0 -> cudaGetLastError's status,
+// 1 -> NTTB_ERR_UNSUPPORTED ("<what>: shape not served"), 2 or more ->
+// NTTB_ERR_CUDA with the error kept by launch_rc (or the current one).
+int engine_status(int rc, const char* what);
 
 // Returns a device workspace of at least `bytes`, growing the plan's buffer
 // (an in-place multi-pass transform stages its first pass there).  Calls
@@ -115,6 +125,9 @@ int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, 
 // `ws` (n_polys * n_limbs * n words); allocates nothing.
 int scalar_transform32_ws(const Plan32& p, uint32_t* data, void* ws, uint32_t n_polys, bool inverse,
                           cudaStream_t s);
+// Bytes of `ws` that scalar_transform32_ws stages in for n_polys polynomials
+// (0 when the shape runs as one pass and stages nothing).
+size_t scalar_transform32_ws_bytes(const Plan32& p, uint32_t n_polys);
 
 // INT8 tensor-core engine (tc_int8.cu).
 bool int8_serves(const Plan32& p, bool src_u64);

@@ -289,7 +289,7 @@ int launch_pass(int mode, const PassArgs& a, const LimbDev<A>* d_limbs, uint32_t
                                    "scalar_pass_scatter_t"};
     ProfScope prof(names[mode & 3], s);
     k<<<grid, kThreads, smem, s>>>(a, d_limbs);
-    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    return launch_rc();
 }
 
 // Vectors per tile: as many as the shared-memory tile holds, fewer while the
@@ -395,6 +395,11 @@ int scalar_transform32_ws(const Plan32& p, uint32_t* data, void* ws, uint32_t n_
                           cudaStream_t s) {
     return transform_generic<uint32_t, M32>(p.log_n, p.n_limbs, p.negacyclic, p.d_limbs, data, data, ws, n_polys,
                                             inverse, 8192, s);
+}
+
+size_t scalar_transform32_ws_bytes(const Plan32& p, uint32_t n_polys) {
+    if (!two_pass(p.log_n, 8192, (uint64_t)n_polys * p.n_limbs)) return 0;
+    return (size_t)n_polys * p.n_limbs * p.n * sizeof(uint32_t);
 }
 
 int scalar_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s) {

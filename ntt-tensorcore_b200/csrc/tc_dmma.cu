@@ -337,7 +337,7 @@ int dmma_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32
         ProfScope prof("dmma_pass_b_n16", s);
         dmma_pass_b_n16<<<dim3(8, p.n_limbs, n_polys), 128, 0, s>>>(mid, out, limbs, p.n_limbs);
     }
-    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    return launch_rc();
 }
 
 void dmma_release(Plan32* p) {

@@ -754,7 +754,7 @@ int launch_stages(Int8Cache* c, ClArgs& a, cudaStream_t s) {
     launch_config(cfg, attr, clusters, s);
     ProfScope prof(a.n_stages == 2 ? "int8_cluster_n16_x2" : "int8_cluster_n16_x4", s);
     if (cudaLaunchKernelEx(&cfg, int8_cluster_n16, a) != cudaSuccess) return 2;
-    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+    return launch_rc();
 }
 
 }  // namespace

@@ -35,12 +35,16 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+// Suspend-time hint of every wait (ns): a warp whose phase is not complete
+// sleeps until it completes (or this much time passes) instead of polling,
+// so waiting warps take no issue slots from the warps that compute.
+constexpr uint32_t kSuspendHintNs = 1000000u;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
@@ -72,15 +76,14 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 constexpr uint64_t kWaitBudgetNs = 2000000000ull;
 
 // Bounded wait for the phase with the given parity.  Returns false when the
-// time budget runs out.
+// time budget runs out.  Each try_wait sleeps up to kSuspendHintNs, so the
+// loop runs a few iterations per wait, not thousands.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (uint32_t i = 0; i < (1u << 26); i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) {
-            if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
-            __nanosleep(64);
-        }
+        if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
     }
     return false;
 }
@@ -122,22 +125,20 @@ __device__ __forceinline__ void arrive_cluster(uint32_t bar_cluster_addr) {
 __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
 // Bounded wait (acquire at cluster scope) for arrivals made by other CTAs.
 __device__ __forceinline__ bool mbar_wait_cluster_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait_cluster(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (uint32_t i = 0; i < (1u << 26); i++) {
         if (mbar_try_wait_cluster(bar, parity)) return true;
-        if (i > 64) {
-            if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
-            __nanosleep(64);
-        }
+        if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
     }
     return false;
 }

@@ -304,3 +304,63 @@ def test_batch_wait_timeout_is_reported_and_recoverable(torch_cuda):
     fresh = make_jobs(torch_cuda, rng, 6, (8, 16), (1, 2), 4)
     plan.batch(spec(fresh)).launch()
     check(torch_cuda, fresh)
+
+
+PRIMES32 = nb.generate_primes(31, 21, 32)
+
+
+@pytest.mark.parametrize("config", [None, TENSOR[0]])
+def test_batch_config4_shaped_mix_wraps_the_rings(torch_cuda, config):
+    """The uneven-batch workload's shape at reduced size: 128 polynomials,
+    log2 N uniform in 12..20, 1..32 limbs over 32 moduli, mixed directions
+    (1.8 GB).  The 2^17 .. 2^20 classes hold many more units than their
+    workspace rings have slots (217 units of 2^20 against 16 slots), so the
+    rings wrap many times and pass A tiles wait for their slot's previous
+    owner.  Checked job by job (limbs first, middle and last of every job
+    against the oracle) and as a whole (the batch with every direction
+    flipped returns the inputs word for word)."""
+    from concurrent.futures import ThreadPoolExecutor
+    torch = torch_cuda
+    rng = np.random.default_rng(8)
+    lgs, limbss = rng.integers(12, 21, 128), rng.integers(1, 33, 128)
+    invs = rng.integers(0, 2, 128).astype(bool)
+    words = int(sum(int(b) << int(a) for a, b in zip(lgs, limbss)))
+    buf = torch.empty(words, dtype=torch.int32, device="cuda")
+    qt = torch.tensor(PRIMES32, dtype=torch.int64, device="cuda")
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(8)
+    jobs, off = [], 0
+    for lg, limbs, inv in zip(lgs, limbss, invs):
+        lg, limbs = int(lg), int(limbs)
+        view = buf[off:off + (limbs << lg)].view(limbs, 1 << lg)
+        r = torch.randint(0, 1 << 31, (limbs, 1 << lg), generator=gen, device="cuda", dtype=torch.int64)
+        view.copy_((r % qt[:limbs, None]).to(torch.int32))
+        jobs.append((view, lg, limbs, 0, bool(inv), False))
+        off += limbs << lg
+    buf0 = buf.clone()
+    plan = nb.BatchPlan(PRIMES32, 20)
+    b = plan.batch(jobs, config)
+    assert b.info()["ws_bytes"] < 4 * words  # the rings are smaller than the batch: they wrap
+    b.launch()
+    torch.cuda.synchronize()
+    assert nb.device_errors() == 0
+    rows = [(i, l) for i, j in enumerate(jobs) for l in sorted({0, j[2] // 2, j[2] - 1})]
+
+    def one(row):
+        i, l = row
+        view, lg, limbs, _, inv, _ = jobs[i]
+        start = view.storage_offset() - buf.storage_offset() + (l << lg)
+        x = to_host(buf0[start:start + (1 << lg)], np.uint32).astype(np.uint64)
+        want = O.rns(x[None, None], [PRIMES32[l]], inverse=inv)[0, 0]
+        got = to_host(view[l], np.uint32).astype(np.uint64)
+        return int((got != want).sum())
+
+    with ThreadPoolExecutor(max_workers=16) as ex:  # the oracle's ctypes calls release the GIL
+        bad = list(ex.map(one, rows))
+    assert sum(bad) == 0, [(jobs[r[0]][1:5], r[1], n) for r, n in zip(rows, bad) if n][:8]
+    b.close()
+    flipped = [(v, lg, limbs, first, not inv, nega) for v, lg, limbs, first, inv, nega in jobs]
+    plan.batch(flipped, config).launch()
+    torch.cuda.synchronize()
+    assert nb.device_errors() == 0
+    assert torch.equal(buf, buf0)

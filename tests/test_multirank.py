@@ -74,3 +74,29 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["value"] > 0 and line["cpu_baseline"]["cores"] >= 1
     assert "reference_gpu" not in line  # no GPU visible
+    assert line["config"] == __import__("bench").headline_config(2)  # the same config as the measured arm
+    assert line["ms_per_step"] > 0
+
+
+def test_reference_arm_does_not_load_the_library():
+    """The reference arm computes its moduli in pure Python: running it loads
+    no libntt_b200.so (only the oracle's libraries)."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0'];"
+            "sys.path.insert(0, %r); import bench; bench.main();"
+            "maps = open('/proc/self/maps').read();"
+            "print(json.dumps({'dropin_loaded': 'libntt_b200' in maps}))" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    last = json.loads(r.stdout.strip().splitlines()[-1])
+    assert last == {"dropin_loaded": False}
+
+
+def test_workload_primes_match_the_library():
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "ntt-tensorcore_b200"))
+    import bench
+    import ntt_b200 as nb
+
+    for bits, adic, count in ((31, 17, 24), (31, 21, 32), (31, 18, 48), (62, 21, 3)):
+        assert bench.workload_primes(bits, adic, count) == nb.generate_primes(bits, adic, count)

@@ -87,3 +87,28 @@ def test_noalloc_rejects_oversized_batch(torch_cuda):
     assert b"static scratch holds" in nb.lib().nttb_last_error()
     before = to_host(d, np.uint32)
     assert (before == x.reshape(-1)).all()  # refused before touching the data
+
+
+def test_noalloc_wrapper_on_a_side_stream(torch_cuda):
+    # the Python wrapper (RnsPlan.transform_noalloc) on a non-default stream,
+    # two calls in a row, against the ordinary entry point
+    moduli = nb.generate_primes(31, 17, 4)
+    plan = nb.RnsPlan(16, moduli, negacyclic=True)
+    side = torch_cuda.cuda.Stream()
+    for seed in (6, 7):
+        x = batch(moduli, 1 << 16, 1, seed)
+        d = to_dev(torch_cuda, x.reshape(-1))
+        torch_cuda.cuda.synchronize()
+        plan.transform_noalloc(d, 1, inverse=False, stream=side)
+        side.synchronize()
+        assert (to_host(d, np.uint32).reshape(x.shape) == regular(torch_cuda, plan, x, False)).all()
+
+
+def test_noalloc_one_pass_shapes_are_not_limited(torch_cuda):
+    # 2^10 words x 24 limbs x 400 polynomials = 37.5 MiB: a one-pass shape
+    # stages nothing, so the scratch limit does not apply
+    moduli = nb.generate_primes(31, 17, 24)
+    plan = nb.RnsPlan(10, moduli, negacyclic=True)
+    x = batch(moduli, 1 << 10, 400, 8)
+    assert x.nbytes > SCRATCH_BYTES
+    assert (noalloc(torch_cuda, plan, x, False) == regular(torch_cuda, plan, x, False)).all()
