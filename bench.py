@@ -748,13 +748,25 @@ def run_serve(args, world, rank, local):
                     "next": 0}
     checks = {"products_checked": 0, "mismatches": 0}
 
+    # The same pool resident on the device, for requests whose operands and
+    # results stay in HBM (nttb_server_submit_device).
+    dpool = [(a.cuda(), b.cuda(), lg, limbs, first) for a, b, lg, limbs, first in pool]
+    douts = [torch.empty_like(d[0]) for d in dpool]
+    drings = {e: {"bufs": [torch.empty_like(dpool[e][0]) for _ in range(RING)], "pending": [None] * RING, "next": 0}
+              for e in rings}
+    modes = {"host": {"pool": pool, "outs": outs, "rings": rings},
+             "device": {"pool": dpool, "outs": douts, "rings": drings}}
+    cur = modes["host"]
+
     def verify(e, slot):
         a, b, lg, limbs, first = pool[e]
-        got = rings[e]["bufs"][slot].numpy().view(np.uint32).reshape(limbs, 1 << lg)
+        buf = cur["rings"][e]["bufs"][slot].view(limbs, 1 << lg)
         checks["products_checked"] += 1
-        if not all((got[l] == want).all() for l, want in expect[e].items()):
-            checks["mismatches"] += 1
-        rings[e]["pending"][slot] = None
+        for l, want in expect[e].items():
+            if not (buf[l].cpu().numpy().view(np.uint32) == want).all():
+                checks["mismatches"] += 1
+                break
+        cur["rings"][e]["pending"][slot] = None
     # tile configuration tuned on this request mix
     tplan = nb.BatchPlan(qs, 17, negacyclic=True)
     sample = []
@@ -807,10 +819,10 @@ def run_serve(args, world, rank, local):
                 if dt > 0:
                     time.sleep(dt)
             e = i % pool_n
-            a, b, lg, limbs, first = pool[e]
-            out = outs[e]
+            a, b, lg, limbs, first = cur["pool"][e]
+            out = cur["outs"][e]
             if e in rings:  # a check request: its own output slot
-                r = rings[e]
+                r = cur["rings"][e]
                 slot = r["next"]
                 r["next"] = (slot + 1) % RING
                 if r["pending"][slot] is not None:  # the slot's last request: done, then checked
@@ -819,13 +831,16 @@ def run_serve(args, world, rank, local):
                             lock.wait(0.01)
                     verify(e, slot)
                 out = r["bufs"][slot]
-            rid = srv.submit(a, b, out, lg, limbs, first)
+            if cur is modes["host"]:
+                rid = srv.submit(a, b, out, lg, limbs, first)
+            else:
+                rid = srv.submit_device("mul", a, b, out, lg, limbs, first)
             work += coeffs[e]
             with lock:
                 ids.append(rid)
                 lock.notify_all()
             if e in rings:
-                rings[e]["pending"][slot] = len(ids) - 1
+                cur["rings"][e]["pending"][slot] = len(ids) - 1
             i += 1
         t_sub = time.perf_counter() - t0
         with lock:
@@ -833,7 +848,7 @@ def run_serve(args, world, rank, local):
             lock.notify_all()
         th.join()
         t_all = time.perf_counter() - t0
-        for e, r in rings.items():  # every request has completed: check the slots left
+        for e, r in cur["rings"].items():  # every request has completed: check the slots left
             for slot in range(RING):
                 if r["pending"][slot] is not None:
                     verify(e, slot)
@@ -856,13 +871,18 @@ def run_serve(args, world, rank, local):
             out["offered_rps"] = reduce_over_ranks(r["offered_rps"], world, "sum")
         return out
 
-    phase(None, 1.0)  # warm-up
-    sat = phase(None, args.serve_seconds)
-    peak = sat["achieved_rps"]  # this rank's saturated rate sets its own load levels
-    levels = {}
-    for frac in (0.25, 0.5, 0.8, 1.0):
-        levels["%d%%" % int(frac * 100)] = over_ranks(phase(frac * peak, args.serve_seconds))
-    sat = over_ranks(sat)
+    def load_levels():
+        phase(None, 1.0)  # warm-up
+        sat = phase(None, args.serve_seconds)
+        peak = sat["achieved_rps"]  # this rank's saturated rate sets its own load levels
+        levels = {}
+        for frac in (0.25, 0.5, 0.8, 1.0):
+            levels["%d%%" % int(frac * 100)] = over_ranks(phase(frac * peak, args.serve_seconds))
+        return over_ranks(sat), levels
+
+    sat, levels = load_levels()  # operands and results in pinned host memory
+    cur = modes["device"]
+    dsat, dlevels = load_levels()  # operands and results resident in HBM
     st = srv.stats()
     srv.close()
     assert checks["mismatches"] == 0, "serving products differ from the oracle: %s" % checks
@@ -876,6 +896,8 @@ def run_serve(args, world, rank, local):
                    "closed_loop_outstanding": outstanding, "parallelism": "replicas x%d" % world},
         "parity": dict(checks, rule="every %d-th product of the stream (one pool entry in %d), limbs 0 and last, "
                                     "vs the oracle's negacyclic product" % (CHECK_EVERY, CHECK_EVERY)),
+        "serve_device_resident": {"saturated": dsat, "load_levels": dlevels,
+                                  "api": "nttb_server_submit_device (operands and results in device memory)"},
         "serve": {"saturated": sat, "load_levels": levels, "batches": st["batches"],
                   "mean_batch_requests": st["batched_requests"] / max(1, st["batches"]),
                   "peak_region_bytes_in_use": st["peak_bytes_in_use"], "resident_bytes": st["resident_bytes"]},
@@ -917,15 +939,17 @@ def run_q60(args, world, rank, local):
         torch.cuda.synchronize()
         return reduce_over_ranks(e0.elapsed_time(e1), world), nb.launch_count() - c0
 
-    def one(i):
+    engine = "auto" if args.engine == "auto" else ("int8" if args.engine == "int8" else "scalar")
+
+    def one(i, eng=None):
         buf = pool[i % pool_n]
-        plan.transform(buf, buf, 1, stream=stream)
-        plan.transform(buf, buf, 1, inverse=True, stream=stream)
+        plan.transform(buf, buf, 1, engine=eng or engine, stream=stream)
+        plan.transform(buf, buf, 1, inverse=True, engine=eng or engine, stream=stream)
 
     def sixteen(i):
         b = pool[(16 * i) % 32:(16 * i) % 32 + 16]
-        plan.transform(b, b, 16, stream=stream)
-        plan.transform(b, b, 16, inverse=True, stream=stream)
+        plan.transform(b, b, 16, engine=engine, stream=stream)
+        plan.transform(b, b, 16, inverse=True, engine=engine, stream=stream)
 
     for i in range(max(3, args.warmup)):
         one(i)
@@ -935,6 +959,16 @@ def run_q60(args, world, rank, local):
     time.sleep(0.5)
     ms, launches = timed(one, args.steps)
     ms16, _ = timed(sixteen, max(3, args.steps // 8))
+    # the CUDA-core Montgomery-64 engine on the same polynomial (comparison)
+    for i in range(3):
+        one(i, "scalar")
+    ms_sc, _ = timed(lambda i: one(i, "scalar"), max(10, args.steps // 4))
+    # per-kernel device time: each pass kernel's share of the event-timed launches
+    nb.profile_start()
+    for i in range(args.steps):
+        one(i)
+    torch.cuda.synchronize()
+    prof = nb.profile_stop()
     clk = clocks.stop()
     got = pool[0].cpu().numpy().view(np.uint64)
     assert (got == host).all(), "q60 round trip failed"
@@ -965,10 +999,16 @@ def run_q60(args, world, rank, local):
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic: seeded uniform residues",
         "config": {"workload": Q60_WORKLOAD, "n": 1 << lg, "q": Q60, "l2": "rotating 40 x 8 MB", "parallelism": "replicas x%d" % world},
+        "engine": engine,
         "batch16": {"value": world * 16 * coeffs * max(3, args.steps // 8) / (ms16 / 1e3),
                     "ms_per_step": ms16 / max(3, args.steps // 8)},
-        "roofline": {"bound": "hbm", "kernel": "scalar_pass (M64)", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "note": "one polynomial per step: launch-latency bound"},
+        "engines_coeffs_per_s": {engine: value,
+                                 "scalar": world * coeffs * max(10, args.steps // 4) / (ms_sc / 1e3)},
+        "kernels": {k: {"launches": v[0], "total_ms": v[1]} for k, v in prof.items()},
+        "roofline": {"bound": "hbm", "kernel": ", ".join(sorted(prof)), "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_source,
+                     "alg_bytes_per_step": 16 * coeffs,
+                     "note": "16 B per residue per transform over the step's device time"},
         "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk, "e2e": None,
     }
 

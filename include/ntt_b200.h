@@ -58,10 +58,23 @@ NTTB_API const char* nttb_last_error(void);
  * dependency wait did, bit 3: a batch tensor tile's wait on its MMA or image
  * copy did; the work item ran on regardless and its output is wrong; bit 4:
  * a TMA tile load of a transpose or bit reversal did not land, and that CTA
- * stopped storing).  Every
+ * stopped storing; bit 5: a wait of the 64-bit byte-plane engine did).  Every
  * such wait gives up after about 2 s of device time.  Reads after a device
  * synchronize; clear != 0 resets them. */
 NTTB_API int nttb_device_errors(uint32_t* flags, int clear);
+/* Range checks of the NTT_DEBUG_BOUNDS build (ntt_b200/libntt_b200_dbg.so,
+ * `python ntt-tensorcore_b200/build.py --debug-bounds`), the stand-in for a
+ * memory checker: bits 0-7 the INT8 cluster kernel, 8-15 the DMMA passes,
+ * 16-23 the uneven-batch queue kernels, 24-31 the 64-bit byte-plane engine
+ * (nttb_wide_transform_engine); within each byte the kind of check
+ * that failed (bit 0 global-memory index, 1 shared-memory offset, 2
+ * distributed-shared-memory piece copy, 3 queue ticket / unit / tile index,
+ * 4 workspace slot, 5 output residue not reduced).  A failed check skips
+ * the access it guards.  *enabled = 1 in that build; the release build
+ * compiles the checks away (enabled 0, flags 0).  Reads after a device
+ * synchronize; clear != 0 resets them.  No reference counterpart (the
+ * reference's debug build is nvcc -G -g, CMakeLists.txt:10). */
+NTTB_API int nttb_bounds_errors(uint32_t* flags, int* enabled, int clear);
 
 /* ------------------------------------------------ modular parameters (host)
  * Field-for-field the reference's ModularParams
@@ -203,6 +216,16 @@ NTTB_API int nttb_wide_plan_create(uint32_t log_n, const uint64_t* moduli, uint3
 NTTB_API int nttb_wide_plan_destroy(nttb_wide_plan* plan);
 NTTB_API int nttb_wide_transform(const nttb_wide_plan* plan, uint64_t* d_dst, const uint64_t* d_src, uint32_t n_polys,
                         int inverse, void* stream);
+/* The same with the engine named: NTTB_ENGINE_INT8 runs the tcgen05 kind::i8
+ * byte-plane engine (eight byte planes of each uint64 word, DFT-32 x DFT-32
+ * per pass of the four-step 1024 x 1024; served for n = 2^20, cyclic plans;
+ * NTTB_ERR_UNSUPPORTED otherwise), NTTB_ENGINE_SCALAR the CUDA-core
+ * Montgomery-64 engine, NTTB_ENGINE_AUTO (what nttb_wide_transform uses) the
+ * INT8 engine where it serves the plan.  Pointers 16-byte aligned; src may
+ * equal dst.  Replaces the reference's run_forward_ct_tcu<K> for primes near
+ * 2^60 (include/ntt_arbitrary.cuh:2599-2646, its limb products on FP64 MMA). */
+NTTB_API int nttb_wide_transform_engine(const nttb_wide_plan* plan, uint64_t* d_dst, const uint64_t* d_src,
+                                        uint32_t n_polys, int inverse, int engine, void* stream);
 
 /* ------------------------------------------------------- uneven batches
  * No single reference counterpart (the reference transforms one size and one
@@ -319,6 +342,23 @@ NTTB_API int nttb_server_submit(nttb_server* server, const uint32_t* a, const ui
  * `in` per limb; NTTB_ERR_BUDGET if its operand alone exceeds the request region. */
 NTTB_API int nttb_server_submit_ntt(nttb_server* server, const uint32_t* in, uint32_t* out, uint32_t log_n,
                                     uint32_t n_limbs, uint32_t first_modulus, int inverse, uint64_t* id);
+/* Device-resident operands: the same requests with a, b and out in device
+ * memory of the server's device, for callers that keep their residues in
+ * HBM between requests.  kind: NTTB_SERVER_PRODUCT (out = a * b per limb),
+ * NTTB_SERVER_FORWARD / NTTB_SERVER_INVERSE (out = the transform of a per
+ * limb; b ignored, may be NULL).  The operands are copied device-to-device
+ * into the server's region on the batch's stream and the result
+ * device-to-device into out, so nothing crosses the host link; a, b and out
+ * must stay valid (and a, b unchanged) until the request completes.  Host
+ * pointers, or memory of another device, are refused (NTTB_ERR_INVALID_ARG).
+ * The reference's device-pointer product is poly_multiply_ntt
+ * (src/ntt_basic.cu:391-409); it has no request loop. */
+#define NTTB_SERVER_PRODUCT 0
+#define NTTB_SERVER_FORWARD 1
+#define NTTB_SERVER_INVERSE 2
+NTTB_API int nttb_server_submit_device(nttb_server* server, int kind, const uint32_t* d_a, const uint32_t* d_b,
+                                       uint32_t* d_out, uint32_t log_n, uint32_t n_limbs, uint32_t first_modulus,
+                                       uint64_t* id);
 /* Waits for one request (NTTB_ERR_TIMEOUT after timeout_s); its latency in seconds.
  * A request's record (status, latency) is kept until a wait collects it, so
  * every id should be waited for once; a second wait on it is refused. */

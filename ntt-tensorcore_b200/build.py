@@ -1,9 +1,11 @@
 """Builds libntt_b200.so (in-tree) from csrc/*.cu and csrc/*.cpp with nvcc for sm_100a.
 
-Usage: python ntt-tensorcore_b200/build.py [--force]
+Usage: python ntt-tensorcore_b200/build.py [--force] [--debug-bounds]
 Objects go to ntt-tensorcore_b200/_build/, the library to
 ntt-tensorcore_b200/ntt_b200/libntt_b200.so.  Rebuilds only what changed
-(by modification time, headers included).
+(by modification time, headers included).  --debug-bounds builds the
+range-checked variant (-DNTT_DEBUG_BOUNDS, csrc/bounds.cuh) into _build_dbg/
+and ntt_b200/libntt_b200_dbg.so instead.
 """
 import concurrent.futures as cf
 import glob
@@ -16,6 +18,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "ntt_b200", "libntt_b200.so")
+BUILD_DBG = os.path.join(HERE, "_build_dbg")
+LIB_DBG = os.path.join(HERE, "ntt_b200", "libntt_b200_dbg.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -28,38 +32,40 @@ def _headers():
     return max((os.path.getmtime(h) for h in hs), default=0)
 
 
-def _compile(src, obj):
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+def _compile(src, obj, extra=()):
+    cmd = [NVCC] + ARCH + FLAGS + list(extra) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s%s" % (src, r.stdout, r.stderr))
     return obj
 
 
-def build(force=False, verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(force=False, verbose=False, debug_bounds=False):
+    build_dir, lib = (BUILD_DBG, LIB_DBG) if debug_bounds else (BUILD, LIB)
+    extra = ["-DNTT_DEBUG_BOUNDS"] if debug_bounds else []
+    os.makedirs(build_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     hdr_time = _headers()
     jobs = []
     objs = []
     for s in srcs:
-        o = os.path.join(BUILD, os.path.basename(s) + ".o")
+        o = os.path.join(build_dir, os.path.basename(s) + ".o")
         objs.append(o)
         if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hdr_time):
             jobs.append((s, o))
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
-            for f in [ex.submit(_compile, s, o) for s, o in jobs]:
+            for f in [ex.submit(_compile, s, o, extra) for s, o in jobs]:
                 f.result()
-    if jobs or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcuda"]
+    if jobs or not os.path.exists(lib):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart", "-lcuda"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))
     if verbose:
-        print("built", LIB, "(%d objects recompiled)" % len(jobs))
-    return LIB
+        print("built", lib, "(%d objects recompiled)" % len(jobs))
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    build(force="--force" in sys.argv, verbose=True, debug_bounds="--debug-bounds" in sys.argv)

@@ -54,6 +54,7 @@
 #include "../../include/ntt_b200.h"
 #include "arith.cuh"
 #include "batch.hpp"
+#include "bounds.cuh"
 #include "engines.hpp"
 #include "plan.hpp"
 #include "profiler.hpp"
@@ -65,6 +66,8 @@ namespace nttb {
 // bit 0: a queue dependency wait ran out of budget; bit 1: a tensor-core
 // tile's wait on its MMA or image copy did
 __device__ uint32_t g_batch_error;
+// NTT_DEBUG_BOUNDS build: failed range checks (bounds.cuh bits)
+__device__ uint32_t g_batch_bounds;
 
 namespace {
 
@@ -128,7 +131,24 @@ struct BArgs {
     uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u
     const uint8_t* images;  // per modulus: DFT-64 byte-plane images (forward, inverse, negacyclic forward)
     uint32_t n_tiles, max_log;
+    uint32_t n_units;       // units in the queue (range checks of the NTT_DEBUG_BOUNDS build)
+    const uint32_t* ws;     // the workspace rings, ws_words words
+    uint64_t ws_words;
 };
+
+// NTT_DEBUG_BOUNDS build: the tile's unit, its tile index and its workspace
+// slot are in range (else the tile is skipped; bounds.cuh bits).
+__device__ __forceinline__ bool tile_in_range(const BArgs& a, const BTile& tl) {
+    if (!NTTB_CHECK(g_batch_bounds, kBoundsQueue, tl.unit < a.n_units)) return false;
+    const BUnit& u = a.units[tl.unit];
+    const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
+    if (!NTTB_CHECK(g_batch_bounds, kBoundsQueue, tile < (pass ? u.tiles_b : u.tiles_a) && u.log_n <= a.max_log))
+        return false;
+    if (u.lg1 && !NTTB_CHECK(g_batch_bounds, kBoundsWorkspace,
+                             u.ws >= a.ws && (uint64_t)(u.ws - a.ws) + (1ull << u.log_n) <= a.ws_words))
+        return false;
+    return true;
+}
 
 __device__ __forceinline__ bool wait_ge(const uint32_t* p, uint32_t target) {
     const uint64_t t0 = tc::globaltimer_ns();
@@ -572,6 +592,15 @@ __device__ __forceinline__ void tc_images(const BArgs& a, const BUnit& u, const 
     }
 }
 
+// L2 lifetimes of a two-pass unit's traffic: every word of a tile's input is
+// read once (the unit's data, or its workspace slot in pass B), so it is
+// loaded evict-first; pass A's stores to the workspace are read back by
+// pass B a few hundred tiles later, so they are kept (evict-last) while the
+// batch's data streams past; pass B's results are stored evict-first.
+__device__ __forceinline__ void st_keep(uint32_t* p, uint32_t v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
+}
+
 // Operand A: row m = (b2, v) = b2 V + v holds column v0 + v's elements
 // j = r' a2 + b2 in K order a2; thread (m, hh) fills 16-byte chunks hh,
 // hh + 2, ..  A product's inverse multiplies by the pointwise operand on the way.
@@ -583,7 +612,7 @@ __device__ __forceinline__ void tc_operand(const BUnit& u, const TcGeo& g, const
 #pragma unroll
     for (uint32_t j = 0; j < 8; j++)
 #pragma unroll
-        for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcg(g.src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
+        for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcs(g.src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
     if (g.pre) {
 #pragma unroll
         for (uint32_t j = 0; j < 8; j++)
@@ -746,6 +775,7 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
     tc::fence_after_sync();
     // level-2 epilogue: thread (quarter, h) reads lane 32 quarter + lane of the
     // M-tiles h, h + 2, ..; 8 outputs k2 at a time (planes r' columns apart)
+    const uint64_t keep = tc::l2_policy_evict_last();
 #pragma unroll 1
     for (uint32_t t = h; t < n_mt; t += 2) {
         const uint32_t row = 128u * t + 32u * quarter + lane;
@@ -772,14 +802,14 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
                 for (uint32_t i = 0; i < 8; i++) {
                     const uint32_t k2 = 8u * gq + i;
                     const uint32_t y = tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
-                    o[64u * k2] = tca::canon(tca::mont_lazy(y, fac[v * rp + k2], q, qinv), q);
+                    st_keep(o + 64u * k2, tca::canon(tca::mont_lazy(y, fac[v * rp + k2], q, qinv), q), keep);
                 }
             } else {
                 uint32_t* o = u.data + (size_t)k1 * N1 + v0 + v;
 #pragma unroll
                 for (uint32_t i = 0; i < 8; i++) {
                     const uint32_t k2 = 8u * gq + i;
-                    o[(size_t)64u * k2 * N1] = tca::canon(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), q);
+                    __stcs(o + (size_t)64u * k2 * N1, tca::canon(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), q));
                 }
             }
         }
@@ -815,6 +845,12 @@ __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__
         const uint32_t ticket = s_ticket;
         if (ticket >= a.n_tiles) break;
         const BTile tl = a.tiles[ticket];
+#if NTTB_DEBUG_BOUNDS
+        if (!tile_in_range(a, tl)) {  // uniform over the CTA: every thread read the same tile
+            __syncthreads();          // s_ticket is read by every thread before it is rewritten
+            continue;
+        }
+#endif
         const BUnit u = a.units[tl.unit];
         const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
         if (threadIdx.x == 0 && !wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
@@ -847,6 +883,12 @@ __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T
         const uint32_t ticket = s_ticket;
         if (ticket >= a.n_tiles) break;
         const BTile tl = a.tiles[ticket];
+#if NTTB_DEBUG_BOUNDS
+        if (!tile_in_range(a, tl)) {  // uniform over the CTA: every thread read the same tile
+            __syncthreads();          // s_ticket is read by every thread before it is rewritten
+            continue;
+        }
+#endif
         const BUnit u = a.units[tl.unit];
         const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
         if (threadIdx.x == 0 && !wait_deps(a, u, tl.unit, pass)) atomicOr(&g_batch_error, 1u);
@@ -1259,6 +1301,9 @@ int launch_batch(Batch* b, cudaStream_t s, bool count) {
     a.n_tiles = b->n_tiles;
     a.max_log = b->plan->max_log;
     a.images = b->plan->images;
+    a.n_units = b->n_units;
+    a.ws = b->d_ws;
+    a.ws_words = b->ws_bytes / 4;
     if (cudaMemsetAsync(b->d_ctr, 0, (1 + 2 * (size_t)b->n_units) * 4, s) != cudaSuccess)
         return fail(NTTB_ERR_CUDA, "batch: counter reset failed");
     if (count) {
@@ -1374,6 +1419,9 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
     a.n_tiles = (uint32_t)r->tiles.size();
     a.max_log = r->plan->max_log;
     a.images = r->plan->images;
+    a.n_units = (uint32_t)r->units.size();
+    a.ws = r->d_ws;
+    a.ws_words = r->ws_bytes / 4;
     bool ok = cudaMemcpyAsync(r->d_units, r->h_units, r->units.size() * sizeof(BUnit), cudaMemcpyHostToDevice, s) ==
               cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->d_tiles, r->h_tiles, r->tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice, s) ==
@@ -1390,6 +1438,16 @@ size_t batch_plan_device_bytes(const BatchPlan* P) {
     const uint32_t lo = std::min<uint32_t>(kLoBits, P->max_log);
     return (size_t)P->limbs.size() * 4 * 4 * (((size_t)1 << (P->max_log - lo)) + ((size_t)1 << lo)) +
            P->limbs.size() * sizeof(BModulus) + (P->images ? P->limbs.size() * (size_t)kImgPerMod : 0);
+}
+
+uint32_t batch_bounds_errors(bool clear) {
+    uint32_t v = 0;
+    cudaMemcpyFromSymbol(&v, g_batch_bounds, sizeof v);
+    if (clear) {
+        uint32_t z = 0;
+        cudaMemcpyToSymbol(g_batch_bounds, &z, sizeof z);
+    }
+    return v;
 }
 
 uint32_t batch_device_errors(bool clear) {

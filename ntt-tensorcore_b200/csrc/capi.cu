@@ -47,6 +47,14 @@ int launch_rc() {
     return 2;
 }
 
+int launch_rc(cudaError_t e) {
+    const cudaError_t last = cudaGetLastError();  // clears the sticky copy
+    if (e == cudaSuccess) e = last;
+    if (e == cudaSuccess) return 0;
+    g_launch_error = e;
+    return 2;
+}
+
 int engine_status(int rc, const char* what) {
     if (rc == 0) return cuda_status(what);
     if (rc == 1) return fail(NTTB_ERR_UNSUPPORTED, "%s: shape not served by the requested engine", what);
@@ -263,8 +271,30 @@ const char* nttb_last_error(void) { return g_last_error.c_str(); }
 int nttb_device_errors(uint32_t* flags, int clear) {
     if (!flags) return fail(NTTB_ERR_INVALID_ARG, "device_errors: null argument");
     *flags = int8_device_errors(clear != 0) | (batch_device_errors(clear != 0) << 2) |
-             (tma_move_device_errors(clear != 0) << 4);
+             (tma_move_device_errors(clear != 0) << 4) | (wide_device_errors(clear != 0) << 5);
     return cuda_status("device_errors");
+}
+
+int nttb_bounds_errors(uint32_t* flags, int* enabled, int clear) {
+    if (!flags || !enabled) return fail(NTTB_ERR_INVALID_ARG, "bounds_errors: null argument");
+#ifdef NTT_DEBUG_BOUNDS
+    *enabled = 1;
+#else
+    *enabled = 0;
+#endif
+    *flags = int8_bounds_errors(clear != 0) | (dmma_bounds_errors(clear != 0) << 8) |
+             (batch_bounds_errors(clear != 0) << 16) | (wide_bounds_errors(clear != 0) << 24);
+    return cuda_status("bounds_errors");
+}
+
+// A wide (64-bit modulus) transform: AUTO takes the INT8 engine where it
+// serves the plan (n = 2^20, cyclic) and the CUDA-core Montgomery-64 engine
+// otherwise.
+static int wide_transform(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, int engine,
+                          cudaStream_t s) {
+    if (engine == NTTB_ENGINE_AUTO) engine = wide_tc_serves(p) ? NTTB_ENGINE_INT8 : NTTB_ENGINE_SCALAR;
+    if (engine == NTTB_ENGINE_INT8) return wide_tc_transform64(p, src, dst, n_polys, inverse, s);
+    return scalar_transform64(p, src, dst, n_polys, inverse, s);  // the 31-bit engines do not serve 64-bit moduli
 }
 
 static bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
@@ -412,6 +442,7 @@ int nttb_plan_create(uint64_t n, uint64_t q, nttb_plan** out) {
 int nttb_plan_destroy(nttb_plan* P) {
     if (!P) return NTTB_OK;
     engines_release32(&P->p32);
+    wide_tc_release(&P->p64);
     free_plan32(&P->p32);
     free_plan64(&P->p64);
     if (P->d_twiddles) cudaFree(P->d_twiddles);
@@ -441,7 +472,7 @@ int nttb_u64_transform(const nttb_plan* P, uint64_t* d, uint64_t batch, int inve
     cudaStream_t s = (cudaStream_t)stream;
     int rc;
     if (P->wide) {
-        rc = scalar_transform64(const_cast<Plan64&>(P->p64), d, d, (uint32_t)batch, inverse != 0, s);
+        rc = wide_transform(const_cast<Plan64&>(P->p64), d, d, (uint32_t)batch, inverse != 0, engine, s);
     } else {
         rc = run_transform32(const_cast<Plan32&>(P->p32), d, d, true, (uint32_t)batch, inverse != 0, engine, s);
     }
@@ -701,6 +732,7 @@ int nttb_wide_plan_create(uint32_t log_n, const uint64_t* moduli, uint32_t n_lim
 
 int nttb_wide_plan_destroy(nttb_wide_plan* P) {
     if (!P) return NTTB_OK;
+    wide_tc_release(&P->p);
     free_plan64(&P->p);
     delete P;
     return NTTB_OK;
@@ -708,9 +740,18 @@ int nttb_wide_plan_destroy(nttb_wide_plan* P) {
 
 int nttb_wide_transform(const nttb_wide_plan* P, uint64_t* dst, const uint64_t* src, uint32_t n_polys, int inverse,
                         void* stream) {
+    return nttb_wide_transform_engine(P, dst, src, n_polys, inverse, NTTB_ENGINE_AUTO, stream);
+}
+
+int nttb_wide_transform_engine(const nttb_wide_plan* P, uint64_t* dst, const uint64_t* src, uint32_t n_polys,
+                               int inverse, int engine, void* stream) {
     if (!P || !dst || !src) return fail(NTTB_ERR_INVALID_ARG, "wide_transform: null argument");
+    if (engine != NTTB_ENGINE_AUTO && engine != NTTB_ENGINE_SCALAR && engine != NTTB_ENGINE_INT8)
+        return fail(NTTB_ERR_INVALID_ARG, "wide_transform: engine must be AUTO, SCALAR or INT8");
+    if ((((uintptr_t)dst) | ((uintptr_t)src)) & 15) return fail(NTTB_ERR_INVALID_ARG, "wide_transform: pointers must be 16-byte aligned");
     if (n_polys == 0) return NTTB_OK;
-    int rc = scalar_transform64(const_cast<Plan64&>(P->p), src, dst, n_polys, inverse != 0, (cudaStream_t)stream);
+    const int rc = wide_transform(const_cast<Plan64&>(P->p), src, dst, n_polys, inverse != 0, engine,
+                                  (cudaStream_t)stream);
     return engine_status(rc, "wide_transform");
 }
 

@@ -93,12 +93,16 @@ struct Plan64 {
     std::vector<void*> allocations;
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    void* engine_data = nullptr;  // the INT8 wide engine's constants (tc_wide.cu)
+    std::mutex engine_mu;         // guards their lazy construction
 };
 
 // Status of the kernel launch just made: 0, or 2 after keeping its CUDA
 // error for the C-ABI's message (cudaGetLastError clears a launch error, so
 // the caller could not read it again).
 int launch_rc();
+// The same for a launch call that returned `e` itself (cudaLaunchKernelEx).
+int launch_rc(cudaError_t e);
 // C-ABI status of an engine's return code: 0 -> cudaGetLastError's status,
 // 1 -> NTTB_ERR_UNSUPPORTED ("<what>: shape not served"), 2 or more ->
 // NTTB_ERR_CUDA with the error kept by launch_rc (or the current one).
@@ -129,12 +133,26 @@ int scalar_transform32_ws(const Plan32& p, uint32_t* data, void* ws, uint32_t n_
 // (0 when the shape runs as one pass and stages nothing).
 size_t scalar_transform32_ws_bytes(const Plan32& p, uint32_t n_polys);
 
+// INT8 tensor-core engine for the wide plans (tc_wide.cu): n = 2^20, cyclic,
+// moduli below 2^62 on byte planes of uint64 words.  Returns 1 when the plan
+// is not served; src may equal dst (the plan workspace holds the first pass).
+bool wide_tc_serves(const Plan64& p);
+int wide_tc_transform64(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, cudaStream_t s);
+void wide_tc_release(Plan64* p);
+uint32_t wide_device_errors(bool clear);
+uint32_t wide_bounds_errors(bool clear);
+
 // INT8 tensor-core engine (tc_int8.cu).
 bool int8_serves(const Plan32& p, bool src_u64);
 int int8_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_t n_polys, bool inverse,
                      cudaStream_t s);
 void int8_release(Plan32* p);
 uint32_t int8_device_errors(bool clear);
+// Failed range checks of the NTT_DEBUG_BOUNDS build (bounds.cuh bits; 0 in the
+// release build), per kernel file.
+uint32_t int8_bounds_errors(bool clear);
+uint32_t dmma_bounds_errors(bool clear);
+uint32_t batch_bounds_errors(bool clear);
 // Forward then inverse, in place, in one persistent launch.
 int int8_forward_inverse32(Plan32& p, uint32_t* data, uint32_t n_polys, cudaStream_t s);
 

@@ -63,6 +63,7 @@ struct Req {
     double t_submit = 0, t_done = 0;
     int status = NTTB_OK;
     bool done = false;
+    bool device = false;  // a, b, out are device memory (copies stay in HBM)
 };
 
 }  // namespace
@@ -178,14 +179,15 @@ void worker_main(nttb_server* s) {
         bool ok = true;
         for (size_t i = 0; i < work.size() && ok; i++) {
             const size_t bytes = work[i].words * 4;
-            ok = cudaMemcpyAsync(sl->jobs[i].data, work[i].a, bytes, cudaMemcpyHostToDevice, sl->stream) == cudaSuccess &&
+            const cudaMemcpyKind in = work[i].device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+            ok = cudaMemcpyAsync(sl->jobs[i].data, work[i].a, bytes, in, sl->stream) == cudaSuccess &&
                  (work[i].kind != kProduct ||
-                  cudaMemcpyAsync(sl->jobs[i].pointwise, work[i].b, bytes, cudaMemcpyHostToDevice, sl->stream) ==
-                      cudaSuccess);
+                  cudaMemcpyAsync(sl->jobs[i].pointwise, work[i].b, bytes, in, sl->stream) == cudaSuccess);
         }
         ok = ok && runner_run(sl->runner, sl->jobs.data(), (uint32_t)sl->jobs.size(), sl->stream) == 0;
         for (size_t i = 0; i < work.size() && ok; i++)
-            ok = cudaMemcpyAsync(work[i].out, sl->jobs[i].data, work[i].words * 4, cudaMemcpyDeviceToHost,
+            ok = cudaMemcpyAsync(work[i].out, sl->jobs[i].data, work[i].words * 4,
+                                 work[i].device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                  sl->stream) == cudaSuccess;
         ok = ok && cudaLaunchHostFunc(sl->stream, batch_done, sl) == cudaSuccess;
         lk.lock();
@@ -329,6 +331,37 @@ NTTB_API int nttb_server_submit_ntt(nttb_server* s, const uint32_t* in, uint32_t
     r.limbs = n_limbs;
     r.first = first_modulus;
     return nttb::submit_request(s, r, "nttb_server_submit_ntt", id);
+}
+
+NTTB_API int nttb_server_submit_device(nttb_server* s, int kind, const uint32_t* d_a, const uint32_t* d_b,
+                                       uint32_t* d_out, uint32_t log_n, uint32_t n_limbs, uint32_t first_modulus,
+                                       uint64_t* id) {
+    static const char* what = "nttb_server_submit_device";
+    if (!s || !d_a || !d_out || !id) return fail(NTTB_ERR_INVALID_ARG, "%s: null argument", what);
+    if (kind < NTTB_SERVER_PRODUCT || kind > NTTB_SERVER_INVERSE)
+        return fail(NTTB_ERR_INVALID_ARG, "%s: kind must be NTTB_SERVER_PRODUCT, _FORWARD or _INVERSE", what);
+    if (kind == NTTB_SERVER_PRODUCT && !d_b) return fail(NTTB_ERR_INVALID_ARG, "%s: a product needs b", what);
+    const void* ptrs[3] = {d_a, kind == NTTB_SERVER_PRODUCT ? (const void*)d_b : (const void*)d_a, d_out};
+    for (const void* p : ptrs) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NTTB_ERR_INVALID_ARG, "%s: not a CUDA pointer", what);
+        }
+        if (at.type != cudaMemoryTypeDevice || at.device != s->device)
+            return fail(NTTB_ERR_INVALID_ARG, "%s: operands must be device memory of the server's device %d", what,
+                        s->device);
+    }
+    nttb::Req r;
+    r.a = d_a;
+    r.b = kind == NTTB_SERVER_PRODUCT ? d_b : nullptr;
+    r.out = d_out;
+    r.kind = kind == NTTB_SERVER_PRODUCT ? nttb::kProduct : kind == NTTB_SERVER_FORWARD ? nttb::kForward : nttb::kInverse;
+    r.log_n = log_n;
+    r.limbs = n_limbs;
+    r.first = first_modulus;
+    r.device = true;
+    return nttb::submit_request(s, r, what, id);
 }
 
 NTTB_API int nttb_server_wait(nttb_server* s, uint64_t id, double timeout_s, double* latency_s) {

@@ -20,10 +20,14 @@
 #include <vector>
 
 #include "../../include/ntt_b200.h"
+#include "bounds.cuh"
 #include "plan.hpp"
 #include "profiler.hpp"
 
 namespace nttb {
+
+// NTT_DEBUG_BOUNDS build: failed range checks (bounds.cuh bits)
+__device__ uint32_t g_dmma_bounds;
 
 namespace {
 
@@ -114,6 +118,7 @@ __global__ void __launch_bounds__(128) dmma_pass_a_n16(const uint32_t* __restric
     const uint64_t off = ((uint64_t)poly * n_limbs + limb) << 16;
     const uint32_t* x = src + off;
     uint32_t* out = dst + off;
+    if (!NTTB_CHECK(g_dmma_bounds, kBoundsGlobal, b0 + 127u < 1024u && limb < n_limbs)) return;
     {
         uint32_t v[64];
         const uint32_t* col = x + b0 + tid;
@@ -133,8 +138,12 @@ __global__ void __launch_bounds__(128) dmma_pass_a_n16(const uint32_t* __restric
         const uint32_t st = L.a_start[b];
         uint32_t t0 = mont(mont(L.a_pow[(b * k0) & 0xFFFFu], st, q, qinv), post0, q, qinv);
         uint32_t t1 = mont(mont(L.a_pow[(b * k1) & 0xFFFFu], st, q, qinv), post1, q, qinv);
-        out[(uint64_t)b * 64u + k0] = canon(mont(y[0], canon(t0, q), q, qinv), q);
-        out[(uint64_t)b * 64u + k1] = canon(mont(y[1], canon(t1, q), q, qinv), q);
+        const uint32_t o0 = canon(mont(y[0], canon(t0, q), q, qinv), q), o1 = canon(mont(y[1], canon(t1, q), q, qinv), q);
+        (void)NTTB_CHECK(g_dmma_bounds, kBoundsResidue, o0 < q && o1 < q);
+        if (NTTB_CHECK(g_dmma_bounds, kBoundsGlobal, b * 64u + k1 < 65536u && k0 < 64u)) {
+            out[(uint64_t)b * 64u + k0] = o0;
+            out[(uint64_t)b * 64u + k1] = o1;
+        }
     }
 }
 
@@ -149,6 +158,7 @@ __global__ void __launch_bounds__(128) dmma_pass_b_n16(const uint32_t* src, uint
     const uint32_t* u = src + off;
     uint32_t* out = dst + off;
     const uint32_t q = L.q, qinv = L.qinv;
+    if (!NTTB_CHECK(g_dmma_bounds, kBoundsGlobal, d0 + 7u < 64u && limb < n_limbs)) return;
     {
         const uint32_t r = tid & 7u, b2 = tid >> 3;
         const uint32_t* base = u + d0 + r;
@@ -203,7 +213,11 @@ __global__ void __launch_bounds__(128) dmma_pass_b_n16(const uint32_t* src, uint
         const uint32_t d2 = row >> 3, r = row & 7u;
         uint32_t* o = out + d0 + r + 64u * d2;
 #pragma unroll
-        for (uint32_t c = 0; c < 16; c++) o[4096u * c] = canon(mont(z[c], L.out16[c], q, qinv), q);
+        for (uint32_t c = 0; c < 16; c++) {
+            const uint32_t v = canon(mont(z[c], L.out16[c], q, qinv), q);
+            (void)NTTB_CHECK(g_dmma_bounds, kBoundsResidue, v < q);
+            o[4096u * c] = v;
+        }
     }
 }
 
@@ -302,6 +316,16 @@ int build_dm(Plan32& p, DmCache* c) {
 }
 
 }  // namespace
+
+uint32_t dmma_bounds_errors(bool clear) {
+    uint32_t v = 0;
+    cudaMemcpyFromSymbol(&v, g_dmma_bounds, sizeof v);
+    if (clear) {
+        uint32_t z = 0;
+        cudaMemcpyToSymbol(g_dmma_bounds, &z, sizeof z);
+    }
+    return v;
+}
 
 bool dmma_serves(const Plan32& p, bool src_u64) { return !src_u64 && p.log_n == 16; }
 

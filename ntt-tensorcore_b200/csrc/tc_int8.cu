@@ -47,8 +47,10 @@
 //   stage B level 2 (in place of level 1, SW64): row r + 8 (d2 / 16) + 32 (d2 % 16),
 //     K word b2.
 //
-// CTA layout: tile w = threadIdx.x / 256 of CTA rank c is tile 2c + w of a
-// stage (columns 128(2c+w).. in stage A, rows 8(2c+w).. in stage B).  Warp
+// CTA layout: threads 0..511 run the epilogues, thread 512 (the last warp)
+// issues the four DFT-64 MMAs of a stage and fetches the next stage's image,
+// so no epilogue warp stalls behind the MMA queue.  Tile w = threadIdx.x / 256
+// of CTA rank c is tile 2c + w of a stage (columns 128(2c+w).. in stage A, rows 8(2c+w).. in stage B).  Warp
 // v = (threadIdx.x / 32) % 8 of a tile reads TMEM lanes 32*(v%4).. (its TMEM
 // sub-partition) and output half v/4, so each vector is recombined by two
 // threads.
@@ -61,6 +63,7 @@
 #include <vector>
 
 #include "../../include/ntt_b200.h"
+#include "bounds.cuh"
 #include "engines.hpp"
 #include "plan.hpp"
 #include "profiler.hpp"
@@ -72,6 +75,8 @@ namespace nttb {
 // bit 0: an mbarrier wait on a local MMA or copy ran out of budget;
 // bit 1: a wait on another CTA of the cluster did
 __device__ uint32_t g_tc_error;
+// NTT_DEBUG_BOUNDS build: failed range checks (bounds.cuh bits)
+__device__ uint32_t g_tc_bounds;
 
 namespace {
 
@@ -81,29 +86,38 @@ constexpr uint32_t kMatBytes64 = 64 * 1024;  // DFT-64 byte-plane image (256 row
 constexpr uint32_t kMatBytes16 = 4 * 1024;   // DFT-16 byte-plane image (64 rows x 64 B)
 constexpr uint32_t kTileBytes = 32 * 1024;   // one 128-vector operand tile (SW128, 256 B rows)
 constexpr uint32_t kClCtas = 4;              // CTAs per cluster
-constexpr uint32_t kClThreads = 512;         // two tiles of 256 threads per CTA
+constexpr uint32_t kEpiThreads = 512;        // two tiles of 256 epilogue threads per CTA
+constexpr uint32_t kClThreads = kEpiThreads + 32;  // + the warp that issues the DFT-64 MMAs and image copies
 // shared memory map (offsets from a 1024-aligned base)
 constexpr uint32_t kOffBuf0 = 0;                        // operand buffer 0: 2 tiles
 constexpr uint32_t kOffBuf1 = 2 * kTileBytes;           // operand buffer 1: 2 tiles
 constexpr uint32_t kOffImg = 4 * kTileBytes;            // DFT-64 image
 constexpr uint32_t kOffImg16 = kOffImg + kMatBytes64;   // DFT-16 images: forward, inverse
-constexpr uint32_t kOffBar = kOffImg16 + 2 * kMatBytes16;
+constexpr uint32_t kOffTB1 = kOffImg16 + 2 * kMatBytes16;  // stage B level-1 twiddles: forward, inverse
+constexpr uint32_t kTB1Stride = 68;                         // words per b2 row (64 twiddles + padding)
+constexpr uint32_t kTB1Bytes = 16 * kTB1Stride * 4;         // one direction: 4352 B
+constexpr uint32_t kOffBar = kOffTB1 + 2 * kTB1Bytes;
 constexpr size_t kClSmem = kOffBar + 256 + 1024;
 constexpr uint32_t kPiece = 1024;            // DSMEM exchange granule
 constexpr uint32_t kBufBytes = 2 * kTileBytes;
 // per-limb device blob: DFT-16 images (8 KB), 3 DFT-64 images, twiddle tables
 constexpr uint32_t kImgSlots = 3;            // 0: stage A forward, 1: inverse (A and B), 2: stage B forward
 constexpr uint32_t kBlobImg = 2 * kMatBytes16;
-// twiddle table of one direction (words): a_st2[2048] a_ratio[1024] b_st2[32]
-// b_ratio[16] q qinv (pad to 16 bytes) a_step[2048] b_step[32]; the forward
-// table, then the inverse
-//   stage A:  t_A(b, d)   = a_st2[2b + h] * a_ratio[b]^(d - 32h),   d in [32h, 32h + 32)
-//   stage B1: t_B1(b2, d2) = b_st2[2 b2 + h] * b_ratio[b2]^(d2 - 32h)  (Montgomery form)
-// a_step / b_step: (ratio^2 mod q, floor(ratio^2 * 2^32 / q)) in plain form,
-// the Shoup operands of the twiddle chains' step (every second output).
-constexpr uint32_t kTabAst = 0, kTabArat = 2048, kTabBst = 3072, kTabBrat = 3104, kTabQ = 3120;
-constexpr uint32_t kTabAstep = 3124, kTabBstep = 5172;
-constexpr uint32_t kTabWords = 5204;
+// twiddle table of one direction (words): a_st2[2048] a_ratio[1024] q qinv
+// (pad to 16 bytes) a_step[2048] b1[16][68]; the forward table, then the
+// inverse
+//   stage A:  t_A(b, d) = a_st2[2b + h] * a_ratio[b]^(d - 32h),   d in [32h, 32h + 32)
+//             (Montgomery form); a_step = (ratio^2 mod q, floor(ratio^2 * 2^32 / q))
+//             in plain form, the Shoup operands of the twiddle chains' step
+//             (every second output);
+//   stage B1: b1[b2][d2] = t_B1(b2, d2) = b_ratio[b2]^d2 itself (Montgomery form,
+//             canonical), row b2 padded to 68 words so that 16-byte loads of
+//             neighbouring rows hit distinct banks; bulk-copied into shared
+//             memory with the unit's constants, so that epilogue reads its
+//             twiddles instead of walking chains.
+constexpr uint32_t kTabAst = 0, kTabArat = 2048, kTabQ = 3072, kTabAstep = 3076, kTabB1 = 5124;
+constexpr uint32_t kTabWords = kTabB1 + 16 * kTB1Stride;
+static_assert((kTabB1 * 4) % 16 == 0 && (kTabWords * 4) % 16 == 0, "bulk-copied table rows stay 16-byte aligned");
 constexpr uint32_t kBlobTab = kBlobImg + kImgSlots * kMatBytes64;
 constexpr uint32_t kBlobBytes = kBlobTab + 2 * kTabWords * 4;
 static_assert(kBlobBytes % 16 == 0, "per-limb blobs must stay 16-byte aligned");
@@ -113,6 +127,7 @@ struct Int8Cache {
     uint8_t* d_blob = nullptr;
     size_t per_limb = 0;
     bool negacyclic = false;
+    bool lazy = false;  // every modulus below 2^31 - 2^16: unreduced twiddle chains
 };
 
 // One stage of the on-chip stage list.
@@ -163,9 +178,12 @@ struct Cl {
     uint64_t* bar;
 };
 // Barriers (shared memory, after the images):
-//   [0, 1]  MMA of tile 0 / 1 (N = 256), issued in that order
+//   [0, 1]  MMA of tile 0 / 1 (N = 256), issued in that order (N = 128
+//           halves committed apart let half the threads start earlier, but
+//           the tensor pipe runs an N = 128 MMA in the time of an N = 256 one:
+//           slower overall)
 //   [4, 5]  level-2 MMA of tile 0 / 1
-//   [6]     per-unit constants (DFT-16 images + first DFT-64 image)
+//   [6]     per-unit constants (DFT-16 images, stage B level-1 twiddles, first DFT-64 image)
 //   [7]     DFT-64 image of the next stage
 //   [8, 9]  buffer 0 / 1 inbox: one arrival (the owner arming the 64 KB its
 //           four senders complete)
@@ -194,11 +212,15 @@ __device__ __forceinline__ void arrive_all(const Cl& c, uint32_t idx) {
 #pragma unroll
     for (uint32_t r = 0; r < kClCtas; r++) tc::arrive_cluster(tc::mapa(a, r));
 }
-// DFT-64 image `slot` of the unit's limb -> shared memory (thread 0), 4 x 16 KB.
+// DFT-64 image `slot` of the unit's limb -> shared memory (one thread), 4 x 16 KB.
+// The per-limb constants are re-read by every launch while the residues
+// stream through the L2 (loaded evict-first): they are loaded evict-last.
 __device__ __forceinline__ void copy_image(const Cl& c, const uint8_t* limb_blob, uint32_t slot, uint64_t* bar) {
     const uint8_t* src = limb_blob + kBlobImg + (size_t)slot * kMatBytes64;
+    const uint64_t pol = tc::l2_policy_evict_last();
 #pragma unroll
-    for (uint32_t k = 0; k < 4; k++) tc::bulk_g2s(c.base + kOffImg + k * 16384u, src + k * 16384u, 16384u, bar);
+    for (uint32_t k = 0; k < 4; k++)
+        tc::bulk_g2s_hint(c.base + kOffImg + k * 16384u, src + k * 16384u, 16384u, bar, pol);
 }
 
 // Stage A operand of tile w from HBM: row m = column b = 128(2c+w) + beta(m),
@@ -206,10 +228,12 @@ __device__ __forceinline__ void copy_image(const Cl& c, const uint8_t* limb_blob
 template <class W>
 __device__ __forceinline__ void load_columns(const Cl& c, const W* x) {
     const uint32_t m = c.wt & 127u, hh = c.wt >> 7;
-    const W* col = x + 128u * (2u * c.rank + c.w) + beta(m) + (32u * hh) * 1024u;
+    const uint32_t off0 = 128u * (2u * c.rank + c.w) + beta(m) + (32u * hh) * 1024u;
+    const W* col = x + off0;
     uint32_t v[32];
+    const bool ok = NTTB_CHECK(g_tc_bounds, kBoundsGlobal, c.rank < kClCtas && off0 + 31u * 1024u < 65536u);
 #pragma unroll
-    for (uint32_t a = 0; a < 32; a++) v[a] = (uint32_t)__ldcs(col + a * 1024u);
+    for (uint32_t a = 0; a < 32; a++) v[a] = ok ? (uint32_t)__ldcs(col + a * 1024u) : 0u;
     uint8_t* t = c.base + kOffBuf0 + c.w * kTileBytes;
 #pragma unroll
     for (uint32_t k = 0; k < 8; k++)
@@ -225,18 +249,29 @@ __device__ __forceinline__ uint32_t lane_cols(const Cl& c) {
 // The epilogues run in two parts of 16 outputs.  `gate` runs between the
 // first part's arithmetic and its stores: it waits until the shared memory
 // the stores overwrite is no longer read by the tensor core.
+//
+// Twiddle chains: each step is a Shoup product, in [0, 2q) for any input
+// below 2^32.  A REDC of the byte-plane sum (below 2^48) returns
+// y < q + 2^16, so with every modulus below 2^31 - 2^16 the product of y and
+// a twiddle in [0, 2q) stays below q * 2^32 and the Montgomery product is
+// exact: the chain need not be reduced to [0, q) (Lazy).  Other moduli
+// reduce every twiddle.
+template <bool Lazy>
+__device__ __forceinline__ uint32_t tw_norm(uint32_t t, uint32_t q) {
+    return Lazy ? t : canon(t, q);
+}
 
 // Stage A epilogue: y_d * t_A(b, d) in [0, 2q) for outputs d = 32h + i,
 // staged in buffer 0 for the A->B exchange.  Output d goes to CTA P = d / 16,
 // tile w' = (d / 8) % 2, level-1 row m' = (b % 16) + 16 (d % 8), K word b / 16
 // (K block = this CTA's rank): piece j = d % 8 of the receiver's K block
 // (rows 16 j..), staged at piece slot (j / 4, 4 (j % 4) + P) of tile w'.
-template <class Gate, class PartDone>
+template <bool Lazy, class Gate, class PartDone>
 __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qinv, uint32_t ratio, uint32_t start,
                                            uint2 step, Gate gate, PartDone part_done) {
     const uint32_t m = c.quarter * 32u + c.lane, b = 128u * (2u * c.rank + c.w) + beta(m);
     uint32_t tw_e = start;                                      // d = 32h
-    uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
+    uint32_t tw_o = tw_norm<Lazy>(mont_lazy(tw_e, ratio, q, qinv), q);  // d = 32h + 1
     const uint32_t col = lane_cols(c);
     const uint32_t bl = b & 15u, a2 = (b >> 4) & 15u;
     // SW64 offset of (row bl, K word a2) inside a 16-row piece
@@ -253,17 +288,19 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
                 y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
                 y[8 * sub + i + 1] =
                     mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
-                tw_e = canon(shoup_lazy(tw_e, step.x, step.y, q), q);
-                tw_o = canon(shoup_lazy(tw_o, step.x, step.y, q), q);
+                tw_e = tw_norm<Lazy>(shoup_lazy(tw_e, step.x, step.y, q), q);
+                tw_o = tw_norm<Lazy>(shoup_lazy(tw_o, step.x, step.y, q), q);
             }
         }
         if (part == 0) gate();
         // d = 32h + 16 part + i: P = 2h + part, w' = i / 8, j = i % 8
-        uint8_t* o = c.base + kOffBuf0 + inpiece + (2u * c.h + part) * kPiece;
+        const uint32_t o0 = inpiece + (2u * c.h + part) * kPiece;
+        uint8_t* o = c.base + kOffBuf0 + o0;
+        if (NTTB_CHECK(g_tc_bounds, kBoundsShared, o0 + kTileBytes + 16384u + 3u * kPiece + 4u <= kBufBytes))
 #pragma unroll
-        for (uint32_t i = 0; i < 16; i++)
-            *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u + 4u * (i & 3u) * kPiece) =
-                y[i];
+            for (uint32_t i = 0; i < 16; i++)
+                *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u +
+                                             4u * (i & 3u) * kPiece) = y[i];
         part_done(part);
     }
 }
@@ -272,11 +309,10 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
 // z * t_B1(b2, d2) in [0, 2q) -> level-2 operand of the same tile (over
 // level 1), SW64, row r + 8 (d2 / 16) + 32 (d2 % 16), K word b2.
 template <class Gate>
-__device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qinv, uint32_t ratio, uint32_t start,
-                                            uint2 step, Gate gate) {
+__device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qinv, uint32_t dir, Gate gate) {
     const uint32_t mv = c.quarter * 32u + c.lane, b2 = mv & 15u, r = mv >> 4;
-    uint32_t tw_e = start;
-    uint32_t tw_o = canon(mont_lazy(tw_e, ratio, q, qinv), q);
+    // t_B1(b2, 32h + 16 part + i) from the shared-memory table
+    const uint32_t* tb = reinterpret_cast<const uint32_t*>(c.base + kOffTB1 + dir * kTB1Bytes) + b2 * kTB1Stride + 32u * c.h;
     const uint32_t col = lane_cols(c);
     // sw64_offset(r + 8 (2h + part) + 32 i, 4 b2) = off + 512 (2h + part) + 2048 i
     const uint32_t off = r * 64u + (((b2 >> 2) ^ ((r >> 1) & 3u)) << 4) + 4u * (b2 & 3u);
@@ -288,18 +324,22 @@ __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qi
             uint32_t c0[8], c1[8], c2[8], c3[8];
             ld_planes8(col + 16u * part + 8u * sub, c0, c1, c2, c3);
 #pragma unroll
-            for (uint32_t i = 0; i < 8; i += 2) {
-                y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
-                y[8 * sub + i + 1] =
-                    mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), tw_o, q, qinv);
-                tw_e = canon(shoup_lazy(tw_e, step.x, step.y, q), q);
-                tw_o = canon(shoup_lazy(tw_o, step.x, step.y, q), q);
+            for (uint32_t g = 0; g < 2; g++) {  // four outputs per 16-byte twiddle load
+                const uint4 t = *reinterpret_cast<const uint4*>(tb + 16u * part + 8u * sub + 4u * g);
+                uint32_t* ys = y + 8 * sub + 4 * g;
+                const uint32_t i = 4 * g;
+                ys[0] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), t.x, q, qinv);
+                ys[1] = mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), t.y, q, qinv);
+                ys[2] = mont_lazy(combine_redc(c0[i + 2], c1[i + 2], c2[i + 2], c3[i + 2], q, qinv), t.z, q, qinv);
+                ys[3] = mont_lazy(combine_redc(c0[i + 3], c1[i + 3], c2[i + 3], c3[i + 3], q, qinv), t.w, q, qinv);
             }
         }
         if (part == 0) gate();
-        uint8_t* o = c.base + kOffBuf1 + c.w * kTileBytes + off + 512u * (2u * c.h + part);
+        const uint32_t o0 = off + 512u * (2u * c.h + part);
+        uint8_t* o = c.base + kOffBuf1 + c.w * kTileBytes + o0;
+        if (NTTB_CHECK(g_tc_bounds, kBoundsShared, o0 + 2048u * 15u + 4u <= kTileBytes))
 #pragma unroll
-        for (uint32_t i = 0; i < 16; i++) *reinterpret_cast<uint32_t*>(o + 2048u * i) = y[i];
+            for (uint32_t i = 0; i < 16; i++) *reinterpret_cast<uint32_t*>(o + 2048u * i) = y[i];
     }
 }
 
@@ -335,6 +375,10 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
         if (gout) {
             const uint32_t d2 = 16u * (c.lane >> 3) + 4u * t2 + c.quarter;
             const uint32_t o = d + 64u * d2;
+            if (!NTTB_CHECK(g_tc_bounds, kBoundsGlobal, o + 4096u * 15u < 65536u)) continue;
+#if NTTB_DEBUG_BOUNDS
+            for (uint32_t k = 0; k < 16; k++) NTTB_CHECK(g_tc_bounds, kBoundsResidue, canon(y[k], q) < q);
+#endif
             if (words64) {
                 uint64_t* g = static_cast<uint64_t*>(gout) + o;
 #pragma unroll
@@ -347,11 +391,13 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
         } else {
             if (part == 0) gate();
             const uint32_t g = 2u * (c.quarter & 1u) + c.w;
-            uint8_t* o = c.base + kOffBuf1 + (c.quarter >> 1) * kTileBytes + t2 * 8u * kPiece + 2u * g * kPiece +
-                         r * 128u + 4u * (c.lane >> 3);
+            const uint32_t o0 = (c.quarter >> 1) * kTileBytes + t2 * 8u * kPiece + 2u * g * kPiece + r * 128u +
+                                4u * (c.lane >> 3);
+            uint8_t* o = c.base + kOffBuf1 + o0;
+            if (NTTB_CHECK(g_tc_bounds, kBoundsShared, o0 + kPiece + (7u << 4) + 4u <= kBufBytes))
 #pragma unroll
-            for (uint32_t k = 0; k < 16; k++)
-                *reinterpret_cast<uint32_t*>(o + (k >> 3) * kPiece + (((k & 7u) ^ r) << 4)) = y[k];
+                for (uint32_t k = 0; k < 16; k++)
+                    *reinterpret_cast<uint32_t*>(o + (k >> 3) * kPiece + (((k & 7u) ^ r) << 4)) = y[k];
             part_done(part);
         }
     }
@@ -378,17 +424,21 @@ __device__ __forceinline__ void send_pieces(const Cl& c, uint32_t kind, uint32_t
         dst = kOffBuf0 + wp * kTileBytes + kb * 16384u + (4u * g + c.rank) * kPiece;
     }
     const uint32_t base = tc::smem_u32(c.base);
+    if (!NTTB_CHECK(g_tc_bounds, kBoundsCluster,
+                    P < kClCtas && src + kPiece <= kOffImg && dst + kPiece <= kOffImg && src % 16u == 0 && dst % 16u == 0))
+        return;
     tc::bulk_s2cluster(tc::mapa(base + dst, P), base + src, kPiece, tc::mapa(tc::smem_u32(c.bar + bar_idx), P));
 }
 
 // ---- the cluster kernel ----------------------------------------------------------------
+template <bool Lazy>
 __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_constant__ ClArgs args) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     Cl c;
     c.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     c.rank = tc::cluster_rank();
     c.tid = threadIdx.x;
-    c.w = threadIdx.x >> 8;
+    c.w = (threadIdx.x >> 8) & 1u;  // the issuing warp (threads 512..) maps to tile 0; it runs no epilogue
     c.wt = threadIdx.x & 255u;
     c.lane = threadIdx.x & 31u;
     c.quarter = (c.wt >> 5) & 3u;
@@ -399,16 +449,29 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
     const bool four = args.n_stages == 4;
     // the per-unit constants and operand: for the first unit, fetched before
     // the cluster start-up barrier
-    auto fetch_unit = [&](uint32_t unit) {
+    auto fetch_consts = [&](uint32_t unit) {
         const uint8_t* limb_blob = args.consts + (unit % args.n_limbs) * args.const_stride;
         if (c.tid == 0) {
-            tc::mbar_expect_tx(c.bar + kBarConst, kBlobImg + kMatBytes64);
-            tc::bulk_g2s(c.base + kOffImg16, limb_blob, kBlobImg, c.bar + kBarConst);
+            const uint64_t pol = tc::l2_policy_evict_last();
+            tc::mbar_expect_tx(c.bar + kBarConst, kBlobImg + kMatBytes64 + 2 * kTB1Bytes);
+            tc::bulk_g2s_hint(c.base + kOffImg16, limb_blob, kBlobImg, c.bar + kBarConst, pol);
+#pragma unroll
+            for (uint32_t dir = 0; dir < 2; dir++)
+                tc::bulk_g2s_hint(c.base + kOffTB1 + dir * kTB1Bytes, limb_blob + kBlobTab + (dir * kTabWords + kTabB1) * 4,
+                                  kTB1Bytes, c.bar + kBarConst, pol);
             copy_image(c, limb_blob, args.st[0].img, c.bar + kBarConst);
         }
+    };
+    const bool issuer = c.tid >= kEpiThreads;
+    auto fetch_data = [&](uint32_t unit) {
+        if (issuer) return;
         if (args.words64) load_columns(c, static_cast<const uint64_t*>(args.src) + ((uint64_t)unit << 16));
         else load_columns(c, static_cast<const uint32_t*>(args.src) + ((uint64_t)unit << 16));
     };
+    // Programmatic dependent launch: the next launch on the stream may be
+    // scheduled now (its CTAs set up on free SMs); nothing of it reads or
+    // writes residues before this grid has completed (griddepcontrol.wait).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (c.tid < 32) tc::tmem_alloc(slot, 512);
     if (c.tid == 0) {
         for (uint32_t i = 0; i <= kBarUnit; i++) tc::mbar_init(c.bar + i, i == kBarUnit ? kClCtas : 1);
@@ -416,7 +479,10 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
         tc::mbar_expect_tx(c.bar + kBarIn1, kBufBytes);
         if (four) tc::mbar_expect_tx(c.bar + kBarIn0, kBufBytes);
     }
-    if (tc::cluster_id() < args.units) fetch_unit(tc::cluster_id());
+    if (tc::cluster_id() < args.units) fetch_consts(tc::cluster_id());  // plan constants: no wait needed
+    // the previous grid on the stream has completed and its writes are visible
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (tc::cluster_id() < args.units) fetch_data(tc::cluster_id());
     tc::fence_before_sync();
     __syncthreads();
     tc::cluster_sync();  // every CTA's barriers exist and are armed before any remote traffic
@@ -432,13 +498,14 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             // the previous unit is finished everywhere: peers no longer read their
             // buffers and every copy out of this CTA's buffers has landed
             wait_cluster(c.bar + kBarUnit, ph_unit);
-            fetch_unit(unit);
+            fetch_consts(unit);
+            fetch_data(unit);
         }
         wait_local(c.bar + kBarConst, ph_ld);
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();
-        bool img_pending = false;  // thread 0: a next-stage image copy is in flight
+        bool img_pending = false;  // issuing thread: a next-stage image copy is in flight
         for (uint32_t s = 0; s < args.n_stages; s++) {
             const ClStage& S = args.st[s];
             const bool last = s + 1 == args.n_stages;
@@ -446,9 +513,9 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             const uint32_t in = buf_addr(c, s & 1u);
             // this thread's twiddle inputs, loaded now so the latency hides
             // behind the operand wait and the MMA
-            uint32_t q, qinv, ratio, start;
-            uint2 step;
-            {
+            uint32_t q = 0, qinv = 0, ratio = 0, start = 0;
+            uint2 step = make_uint2(0, 0);
+            if (!issuer) {
                 const uint32_t* T = reinterpret_cast<const uint32_t*>(limb_blob + kBlobTab) + S.dir * kTabWords;
                 q = __ldg(T + kTabQ);
                 qinv = __ldg(T + kTabQ + 1);
@@ -457,41 +524,49 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                     ratio = __ldg(T + kTabArat + b);
                     start = __ldg(T + kTabAst + 2 * b + c.h);
                     step = __ldg(reinterpret_cast<const uint2*>(T + kTabAstep) + b);
-                } else {
-                    const uint32_t b2 = c.lane & 15u;  // row m' = 32 quarter + lane: b2 = m' % 16
-                    ratio = __ldg(T + kTabBrat + b2);
-                    start = __ldg(T + kTabBst + 2 * b2 + c.h);
-                    step = __ldg(reinterpret_cast<const uint2*>(T + kTabBstep) + b2);
                 }
             }
-            if (s > 0) {  // this stage's 64 KB operand arrived from the four CTAs
-                if (s & 1u) wait_cluster(c.bar + kBarIn1, ph_in1);
-                else wait_cluster(c.bar + kBarIn0, ph_in0);
-                if (s == 1 && four && c.tid == 0) tc::mbar_expect_tx(c.bar + kBarIn1, kBufBytes);  // stage 3
-            }
-            if (c.tid == 0) {
-                if (img_pending) wait_local(c.bar + kBarImg, ph_img);
-                img_pending = false;
-                tc::fence_after_sync();
+            if (issuer) {
+                // the stage's operand (s > 0: 64 KB from the four CTAs) and
+                // image are in shared memory: issue the four MMAs, then, once
+                // they are done, fetch the next stage's image over this one
+                if (s > 0) {
+                    if (s & 1u) wait_cluster(c.bar + kBarIn1, ph_in1);
+                    else wait_cluster(c.bar + kBarIn0, ph_in0);
+                    if (s == 1 && four && c.lane == 0) tc::mbar_expect_tx(c.bar + kBarIn1, kBufBytes);  // stage 3
+                }
+                if (c.lane == 0) {
+                    if (img_pending) wait_local(c.bar + kBarImg, ph_img);
+                    img_pending = false;
+                    tc::fence_after_sync();
 #pragma unroll
-                for (uint32_t w = 0; w < 2; w++) {
-                    if (S.kind == 0) issue_k256(c.taddr + w * 256u, in + w * kTileBytes, 128, img_a, 256, 256);
-                    else issue_k256_a64(c.taddr + w * 256u, in + w * kTileBytes, 128, img_a, 256, 256);
-                    tc::commit(c.bar + kBarMma + w);
+                    for (uint32_t w = 0; w < 2; w++) {
+                        if (S.kind == 0) issue_k256(c.taddr + w * 256u, in + w * kTileBytes, 128, img_a, 256, 256);
+                        else issue_k256_a64(c.taddr + w * 256u, in + w * kTileBytes, 128, img_a, 256, 256);
+                        tc::commit(c.bar + kBarMma + w);
+                    }
                 }
-            }
-            __syncwarp();
-            wait_parity(c.bar + kBarMma + c.w, ph_mma);
-            tc::fence_after_sync();
-            // before the first stores: the MMAs reading the overwritten operand
-            // are done; thread 0 then fetches the next stage's image
-            auto mma_gate = [&]() {
-                if (S.kind == 0 || (c.tid == 0 && next_img)) wait_parity(c.bar + kBarMma + 1, ph_mma);
-                if (c.tid == 0 && next_img) {
+                __syncwarp();
+                wait_parity(c.bar + kBarMma + 1, ph_mma);  // the last commit: every MMA is done
+                ph_mma ^= 1u;
+                if (c.lane == 0 && next_img) {
                     tc::mbar_expect_tx(c.bar + kBarImg, kMatBytes64);
                     copy_image(c, limb_blob, args.st[s + 1].img, c.bar + kBarImg);
                     img_pending = true;
                 }
+                __syncwarp();
+                tc::fence_before_sync();
+                __syncthreads();
+                continue;
+            }
+            wait_parity(c.bar + kBarMma + c.w, ph_mma);
+            tc::fence_after_sync();
+            // before the first stores: the MMAs reading the overwritten operand
+            // are done (stage A stages into both tiles' operands: every MMA;
+            // stage B level 1 writes over its own tile's, whose MMA this
+            // thread has waited for)
+            auto mma_gate = [&]() {
+                if (S.kind == 0) wait_parity(c.bar + kBarMma + 1, ph_mma);
             };
             // after each part's stores: the 256 threads of output half h have
             // staged every piece for CTA 2h + part, and one warp sends them
@@ -503,10 +578,10 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                     send_pieces(c, S.kind, 2u * c.h + part, S.kind == 0 ? kBarIn1 : kBarIn0);
             };
             if (S.kind == 0) {
-                epilogue_a(c, q, qinv, ratio, start, step, mma_gate, part_done);
+                epilogue_a<Lazy>(c, q, qinv, ratio, start, step, mma_gate, part_done);
                 ph_mma ^= 1u;
             } else {
-                epilogue_b1(c, q, qinv, ratio, start, step, mma_gate);
+                epilogue_b1(c, q, qinv, S.dir, mma_gate);
                 ph_mma ^= 1u;
                 tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
@@ -597,7 +672,7 @@ std::vector<uint64_t> dft_matrix(uint32_t L, uint64_t root, uint64_t q, uint64_t
     return W;
 }
 
-// Twiddle table of one direction (layout at kTabAst..kTabQ).
+// Twiddle table of one direction (layout above kTabWords).
 void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_t* ratio_a, const uint64_t* ratio_b) {
     t[kTabQ] = (uint32_t)q;
     t[kTabQ + 1] = h_neg_inv32((uint32_t)q);
@@ -609,14 +684,8 @@ void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_
         t[kTabAstep + 2 * b] = (uint32_t)r2;
         t[kTabAstep + 2 * b + 1] = (uint32_t)((r2 << 32) / q);
     }
-    for (uint32_t b2 = 0; b2 < 16; b2++) {
-        t[kTabBst + 2 * b2] = h_to_mont32(1, q);
-        t[kTabBst + 2 * b2 + 1] = h_to_mont32(h_powmod(ratio_b[b2], 32, q), q);
-        t[kTabBrat + b2] = h_to_mont32(ratio_b[b2], q);
-        const uint64_t r2 = h_mulmod(ratio_b[b2], ratio_b[b2], q);
-        t[kTabBstep + 2 * b2] = (uint32_t)r2;
-        t[kTabBstep + 2 * b2 + 1] = (uint32_t)((r2 << 32) / q);
-    }
+    for (uint32_t b2 = 0; b2 < 16; b2++)
+        for (uint32_t d2 = 0; d2 < 64; d2++) t[kTabB1 + b2 * kTB1Stride + d2] = h_to_mont32(h_powmod(ratio_b[b2], d2, q), q);
 }
 
 // DFT-64 image slots: 0 stage A forward, 1 inverse (stage A and stage B
@@ -675,6 +744,8 @@ int build_cache(Plan32& p, Int8Cache* c) {
     }
     c->d_blob = d_blob;
     c->per_limb = per_limb;
+    c->lazy = true;
+    for (uint32_t l = 0; l < nl; l++) c->lazy = c->lazy && p.limbs[l].q < (1ull << 31) - (1ull << 16);
     c->negacyclic = p.negacyclic;
     c->log_n = p.log_n;
     return 0;
@@ -717,24 +788,27 @@ void launch_config(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* attr, uint32_t 
     attr[0].val.clusterDim.x = kClCtas;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
 }
 
 // Clusters of 4 that fit on the current device at once (one CTA per SM).
 // The shared-memory attribute and the answer are per device.
 int max_clusters() {
-    static std::atomic<int> cached[64];
+    static std::atomic<int> cached[64];  // the same for both kernel instances (same resources)
     int dev = 0;
     cudaGetDevice(&dev);
     std::atomic<int>& slot = cached[dev & 63];
     if (const int c = slot.load()) return c;
-    cudaFuncSetAttribute(int8_cluster_n16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem);
+    cudaFuncSetAttribute(int8_cluster_n16<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem);
+    cudaFuncSetAttribute(int8_cluster_n16<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClSmem);
     cudaLaunchConfig_t cfg;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     launch_config(cfg, attr, 1, 0);
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, int8_cluster_n16, &cfg) != cudaSuccess || n < 1) {
+    if (cudaOccupancyMaxActiveClusters(&n, int8_cluster_n16<true>, &cfg) != cudaSuccess || n < 1) {
         cudaGetLastError();
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -750,11 +824,12 @@ int launch_stages(Int8Cache* c, ClArgs& a, cudaStream_t s) {
     a.consts = c->d_blob;
     a.const_stride = c->per_limb;
     cudaLaunchConfig_t cfg;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     launch_config(cfg, attr, clusters, s);
     ProfScope prof(a.n_stages == 2 ? "int8_cluster_n16_x2" : "int8_cluster_n16_x4", s);
-    if (cudaLaunchKernelEx(&cfg, int8_cluster_n16, a) != cudaSuccess) return 2;
-    return launch_rc();
+    const cudaError_t e = c->lazy ? cudaLaunchKernelEx(&cfg, int8_cluster_n16<true>, a)
+                                  : cudaLaunchKernelEx(&cfg, int8_cluster_n16<false>, a);
+    return launch_rc(e);
 }
 
 }  // namespace
@@ -816,6 +891,16 @@ void int8_release(Plan32* p) {
     if (c->d_blob) cudaFree(c->d_blob);
     delete c;
     p->engine_data[1] = nullptr;
+}
+
+uint32_t int8_bounds_errors(bool clear) {
+    uint32_t v = 0;
+    cudaMemcpyFromSymbol(&v, g_tc_bounds, sizeof v);
+    if (clear) {
+        uint32_t z = 0;
+        cudaMemcpyToSymbol(g_tc_bounds, &z, sizeof z);
+    }
+    return v;
 }
 
 uint32_t int8_device_errors(bool clear) {

@@ -12,7 +12,8 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libntt_b200.so")
+# NTT_B200_LIB=dbg selects the NTT_DEBUG_BOUNDS build (range-checked kernels)
+LIB_PATH = os.path.join(HERE, "libntt_b200_dbg.so" if os.environ.get("NTT_B200_LIB") == "dbg" else "libntt_b200.so")
 HEADER = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "ntt_b200.h")
 
 OK = 0
@@ -119,11 +120,13 @@ def lib():
         "nttb_wide_plan_create": (_int, [_u32, _vp, _u32, _u32, ctypes.POINTER(_vp)]),
         "nttb_wide_plan_destroy": (_int, [_vp]),
         "nttb_wide_transform": (_int, [_vp, _vp, _vp, _u32, _int, _vp]),
+        "nttb_wide_transform_engine": (_int, [_vp, _vp, _vp, _u32, _int, _int, _vp]),
         "nttb_klimb_forward": (_int, [_u32, _vp, _vp, _u64, _u32, _vp, _u32, _vp]),
         "nttb_server_default_config": (_int, [ctypes.POINTER(ServerConfig)]),
         "nttb_server_create": (_int, [_vp, _u32, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
         "nttb_server_submit": (_int, [_vp, _vp, _vp, _vp, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
         "nttb_server_submit_ntt": (_int, [_vp, _vp, _vp, _u32, _u32, _u32, _int, ctypes.POINTER(_u64)]),
+        "nttb_server_submit_device": (_int, [_vp, _int, _vp, _vp, _vp, _u32, _u32, _u32, ctypes.POINTER(_u64)]),
         "nttb_server_wait": (_int, [_vp, _u64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
         "nttb_server_drain": (_int, [_vp, ctypes.c_double]),
         "nttb_server_stats": (_int, [_vp, ctypes.POINTER(ServerStats)]),
@@ -142,6 +145,7 @@ def lib():
         "nttb_batch_info": (_int, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64),
                                    ctypes.POINTER(BatchConfig)]),
         "nttb_device_errors": (_int, [ctypes.POINTER(_u32), _int]),
+        "nttb_bounds_errors": (_int, [ctypes.POINTER(_u32), ctypes.POINTER(_int), _int]),
         "nttb_launch_count": (_int, [ctypes.POINTER(_u64)]),
         "nttb_profile_start": (_int, []),
         "nttb_profile_stop": (_int, [ctypes.POINTER(_u32)]),
@@ -322,6 +326,17 @@ class Server:
         self._keep[int(i.value)] = (x, out)
         return int(i.value)
 
+    def submit_device(self, kind, a, b, out, log_n, n_limbs, first_modulus=0):
+        """Queues a request whose operands and result are CUDA tensors on the
+        server's device: kind "mul" (out = a * b), "forward" or "inverse"
+        (out = the transform of a; b unused)."""
+        k = {"mul": 0, "forward": 1, "inverse": 2}[kind]
+        i = _u64()
+        _check(lib().nttb_server_submit_device(self._h, k, a.data_ptr(), b.data_ptr() if b is not None else None,
+                                               out.data_ptr(), log_n, n_limbs, first_modulus, ctypes.byref(i)))
+        self._keep[int(i.value)] = (a, b, out)
+        return int(i.value)
+
     def wait(self, rid, timeout=60.0):
         lat = ctypes.c_double()
         try:
@@ -385,6 +400,14 @@ def device_errors(clear=True):
     f = _u32()
     _check(lib().nttb_device_errors(ctypes.byref(f), int(clear)))
     return int(f.value)
+
+
+def bounds_errors(clear=True):
+    """(enabled, flags) of the NTT_DEBUG_BOUNDS build's range checks
+    (nttb_bounds_errors); enabled is False in the release build."""
+    f, e = _u32(), _int()
+    _check(lib().nttb_bounds_errors(ctypes.byref(f), ctypes.byref(e), int(clear)))
+    return bool(e.value), int(f.value)
 
 
 def profile_start():
@@ -552,8 +575,11 @@ class WidePlan:
         self._h = h
         self.log_n, self.n, self.moduli = log_n, 1 << log_n, [int(x) for x in m]
 
-    def transform(self, dst, src, n_polys, inverse=False, stream=None):
-        _check(lib().nttb_wide_transform(self._h, _ptr(dst), _ptr(src), n_polys, int(inverse), _stream(stream)))
+    def transform(self, dst, src, n_polys, inverse=False, engine="auto", stream=None):
+        """engine "auto" (the INT8 byte-plane engine where it serves the plan),
+        "int8" or "scalar" (nttb_wide_transform_engine)."""
+        _check(lib().nttb_wide_transform_engine(self._h, _ptr(dst), _ptr(src), n_polys, int(inverse), _engine(engine),
+                                                _stream(stream)))
 
     def close(self):
         if getattr(self, "_h", None):

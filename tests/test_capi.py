@@ -20,6 +20,24 @@ def test_library_exports_every_header_symbol():
     assert not missing, missing
 
 
+def test_debug_bounds_library_exports_every_header_symbol():
+    """The NTT_DEBUG_BOUNDS build exports the same C ABI; the release build
+    reports its range checks as compiled away."""
+    dbg = os.path.join(os.path.dirname(nb.LIB_PATH), "libntt_b200_dbg.so")
+    assert os.path.exists(dbg), "run `python ntt-tensorcore_b200/build.py --debug-bounds`"
+    D = ctypes.CDLL(dbg)
+    missing = [s for s in nb.header_symbols() if not hasattr(D, s)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", dbg], capture_output=True, text=True).stdout
+    assert "g_tc_bounds" not in out  # device words stay internal
+    f, e = ctypes.c_uint32(7), ctypes.c_int(7)
+    assert nb.lib().nttb_bounds_errors(None, None, 0) == 1
+    import torch
+    if not torch.cuda.is_available():  # the symbol lookups need a device; the flag does not
+        return
+    assert nb.lib().nttb_bounds_errors(ctypes.byref(f), ctypes.byref(e), 0) == 0 and e.value == 0
+
+
 def test_library_exports_dropin_cpp_api():
     out = subprocess.run(["nm", "-DC", "--defined-only", nb.LIB_PATH], capture_output=True, text=True).stdout
     for name in ["ntt::ntt_init", "ntt::ntt_cleanup", "ntt::ntt_forward_basic", "ntt::ntt_inverse_basic",
@@ -84,6 +102,7 @@ def test_invalid_arguments_rejected_without_device():
     rid = ctypes.c_uint64()
     assert L.nttb_u64_pretransposed_transform(None, None, 64, 0, None) == 1
     assert L.nttb_server_submit_ntt(None, None, None, 10, 1, 0, 0, ctypes.byref(rid)) == 1
+    assert L.nttb_server_submit_device(None, 0, None, None, None, 10, 1, 0, ctypes.byref(rid)) == 1
     assert b"null" in L.nttb_last_error()
     assert L.nttb_u64_transpose(None, None, 32, 32, None) == 1
     assert L.nttb_u64_bit_reverse(None, 1024, None) == 1

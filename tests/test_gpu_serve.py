@@ -178,3 +178,52 @@ def test_server_cyclic_products(torch_cuda):
         want = O.rns(x[None].astype(np.uint64), PRIMES[first:first + limbs], negacyclic=False, inverse=inv)[0]
         assert (out == want.astype(np.uint32)).all(), (lg, inv)
     srv.close()
+
+
+def test_server_device_resident_requests(torch_cuda):
+    """Requests whose operands and result stay in device memory
+    (nttb_server_submit_device): products and forward / inverse NTTs equal
+    the oracle, a device product gives the same result alone and in a mix
+    with host-memory requests, and host pointers are refused."""
+    torch = torch_cuda
+    rng = np.random.default_rng(9)
+    srv = nb.Server(PRIMES, hbm_budget_bytes=96 << 20, max_log_n=16, slots=3, max_batch_requests=16)
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).cuda()
+    host = lambda t: t.cpu().numpy().view(np.uint32)
+    a, b, lg, limbs, first = request(rng, (14, 14), (3, 3))
+    da, db = dev(a), dev(b)
+    alone = torch.zeros_like(da)
+    srv.wait(srv.submit_device("mul", da, db, alone, lg, limbs, first))
+    want = product(a, b, PRIMES[first:first + limbs], True)
+    assert (host(alone).reshape(a.shape) == want).all()
+    jobs, mine = [], None
+    for k in range(30):
+        x, y, lgk, lk, fk = request(rng, (4, 16), (1, 5))
+        if k % 2:  # host-memory product
+            out = np.zeros_like(x)
+            jobs.append(("host", x, y, lgk, lk, fk, out, srv.submit(x, y, out, lgk, lk, fk)))
+        else:  # device-resident forward / inverse NTT
+            inv = k % 4 == 2
+            dx, dout = dev(x), torch.zeros(x.size, dtype=torch.int32, device="cuda")
+            jobs.append(("inverse" if inv else "forward", x, dx, lgk, lk, fk, dout,
+                         srv.submit_device("inverse" if inv else "forward", dx, None, dout, lgk, lk, fk)))
+        if k == 15:
+            mixed = torch.zeros_like(da)
+            mine = srv.submit_device("mul", da, db, mixed, lg, limbs, first)
+    srv.drain()
+    for j in jobs:
+        srv.wait(j[-1])
+    srv.wait(mine)
+    assert torch.equal(mixed, alone)
+    assert (host(da).reshape(a.shape) == a).all() and (host(db).reshape(b.shape) == b).all()  # inputs untouched
+    for kind, x, y, lgk, lk, fk, out, _ in jobs:
+        m = PRIMES[fk:fk + lk]
+        if kind == "host":
+            assert (out == product(x, y, m, True)).all()
+        else:
+            w = O.rns(x[None].astype(np.uint64), m, negacyclic=True, inverse=kind == "inverse")[0].astype(np.uint32)
+            assert (host(out).reshape(x.shape) == w).all(), (kind, lgk, lk)
+    with pytest.raises(nb.NTTError):  # host memory is not a device operand
+        srv.submit_device("forward", torch.from_numpy(a.view(np.int32)), None, da, lg, limbs, first)
+    srv.close()
+    assert nb.device_errors() == 0
