@@ -221,7 +221,9 @@ NTTB_API int nttb_wide_transform(const nttb_wide_plan* plan, uint64_t* d_dst, co
  * per pass of the four-step 1024 x 1024; served for n = 2^20, cyclic plans;
  * NTTB_ERR_UNSUPPORTED otherwise), NTTB_ENGINE_SCALAR the CUDA-core
  * Montgomery-64 engine, NTTB_ENGINE_AUTO (what nttb_wide_transform uses) the
- * INT8 engine where it serves the plan.  Pointers 16-byte aligned; src may
+ * INT8 engine where it serves the plan and the batch has fewer than 8
+ * (polynomial, limb) units (it has the shorter latency; the CUDA-core engine
+ * the higher throughput on larger batches).  Pointers 16-byte aligned; src may
  * equal dst.  Replaces the reference's run_forward_ct_tcu<K> for primes near
  * 2^60 (include/ntt_arbitrary.cuh:2599-2646, its limb products on FP64 MMA). */
 NTTB_API int nttb_wide_transform_engine(const nttb_wide_plan* plan, uint64_t* d_dst, const uint64_t* d_src,

@@ -128,7 +128,8 @@ struct BArgs {
     const BModulus* mods;
     const BUnit* units;
     const BTile* tiles;
-    uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u
+    uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u;
+                    // [1 + 2 n_units + u] pass B tiles of unit u that finished reading its slot
     const uint8_t* images;  // per modulus: DFT-64 byte-plane images (forward, inverse, negacyclic forward)
     uint32_t n_tiles, max_log;
     uint32_t n_units;       // units in the queue (range checks of the NTT_DEBUG_BOUNDS build)
@@ -375,6 +376,28 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
 // Thread 0 of a tile: waits until the tile's inputs are complete (pass B:
 // every pass A tile of its unit; pass A: the previous owner of its workspace
 // slot and the units it depends on).  False if a wait ran out of budget.
+// After a pass B tile of a two-pass unit: the last of the unit's pass B
+// tiles to finish invalidates the unit's workspace slot in the L2 without
+// writing it back (its words have all been read; the slot's next owner, which
+// waits for this tile's completion signal, rewrites it).  Without this the
+// dirty slot lines would reach DRAM on eviction: 4 bytes per residue that are
+// never read.  Called by every thread of the CTA after the tile's stores and
+// a CTA barrier, before the tile's completion signal.
+__device__ __forceinline__ void release_slot(const BArgs& a, const BUnit& u, uint32_t ui, uint32_t* s_last) {
+    if (threadIdx.x == 0) {
+        __threadfence();
+        *s_last = atomicAdd(a.ctr + 1 + 2 * a.n_units + ui, 1u) + 1u == u.tiles_b;
+    }
+    __syncthreads();
+    if (!*s_last) return;
+    const uint64_t lines = (4ull << u.log_n) / 128u;
+    const uint8_t* base = reinterpret_cast<const uint8_t*>(u.ws);
+    for (uint64_t i = threadIdx.x; i < lines; i += blockDim.x)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(base + 128u * i) : "memory");
+    __threadfence();
+    __syncthreads();
+}
+
 __device__ __forceinline__ bool wait_deps(const BArgs& a, const BUnit& u, uint32_t ui, uint32_t pass) {
     bool ok = true;
     if (pass == 1) {
@@ -821,7 +844,7 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
 template <uint32_t G>
 __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__ BArgs a) {
     extern __shared__ __align__(1024) uint8_t tc_raw[];
-    __shared__ uint32_t s_ticket, s_taddr;
+    __shared__ uint32_t s_ticket, s_taddr, s_last;
     __shared__ M32 s_ar[kMaxRows];
     TcState st;
     st.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
@@ -864,6 +887,7 @@ __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();
+        if (pass == 1 && u.lg1) release_slot(a, u, tl.unit, &s_last);
         if (threadIdx.x == 0) signal_done(a.ctr + 1 + 2 * tl.unit + pass);
     }
     tc::fence_before_sync();
@@ -875,7 +899,7 @@ template <uint32_t E, uint32_t T, uint32_t G>
 // more resident CTAs for the small register groups
 __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T) batch_queue(const __grid_constant__ BArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
-    __shared__ uint32_t s_ticket;
+    __shared__ uint32_t s_ticket, s_last;
     __shared__ M32 s_ar[kMaxRows];
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ctr, 1u);
@@ -895,6 +919,7 @@ __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T
         __syncthreads();
         run_tile<T, G>(a, u, pass, tile, sm, s_ar);
         __syncthreads();
+        if (pass == 1 && u.lg1) release_slot(a, u, tl.unit, &s_last);
         if (threadIdx.x == 0) signal_done(a.ctr + 1 + 2 * tl.unit + pass);
     }
 }
@@ -1271,7 +1296,7 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
     bool ok = true;
     ok = ok && cudaMalloc(&b->d_units, std::max<size_t>(1, units.size()) * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(BTile)) == cudaSuccess;
-    ok = ok && cudaMalloc(&b->d_ctr, (1 + 2 * (size_t)units.size()) * 4) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_ctr, (1 + 3 * (size_t)units.size()) * 4) == cudaSuccess;
     if (ok && b->ws_bytes) ok = cudaMalloc(&b->d_ws, b->ws_bytes) == cudaSuccess;
     if (!ok) {
         free_batch(b);
@@ -1304,7 +1329,7 @@ int launch_batch(Batch* b, cudaStream_t s, bool count) {
     a.n_units = b->n_units;
     a.ws = b->d_ws;
     a.ws_words = b->ws_bytes / 4;
-    if (cudaMemsetAsync(b->d_ctr, 0, (1 + 2 * (size_t)b->n_units) * 4, s) != cudaSuccess)
+    if (cudaMemsetAsync(b->d_ctr, 0, (1 + 3 * (size_t)b->n_units) * 4, s) != cudaSuccess)
         return fail(NTTB_ERR_CUDA, "batch: counter reset failed");
     if (count) {
         ProfScope prof("batch_queue", s);
@@ -1355,7 +1380,7 @@ int runner_reserve(BatchRunner* r, size_t units, size_t tiles) {
     runner_free_queue(r);
     bool ok = cudaMalloc(&r->d_units, cu * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMalloc(&r->d_tiles, ct * sizeof(BTile)) == cudaSuccess;
-    ok = ok && cudaMalloc(&r->d_ctr, (1 + 2 * cu) * 4) == cudaSuccess;
+    ok = ok && cudaMalloc(&r->d_ctr, (1 + 3 * cu) * 4) == cudaSuccess;
     ok = ok && cudaMallocHost(&r->h_units, cu * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMallocHost(&r->h_tiles, ct * sizeof(BTile)) == cudaSuccess;
     if (!ok) {
@@ -1426,7 +1451,7 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
               cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->d_tiles, r->h_tiles, r->tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice, s) ==
                    cudaSuccess;
-    ok = ok && cudaMemsetAsync(r->d_ctr, 0, (1 + 2 * r->units.size()) * 4, s) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->d_ctr, 0, (1 + 3 * r->units.size()) * 4, s) == cudaSuccess;
     if (!ok) return fail(NTTB_ERR_CUDA, "batch runner: queue upload failed");
     const int grid = (int)std::min<size_t>((size_t)r->grid, r->tiles.size());
     ProfScope prof("batch_queue", s);

@@ -288,11 +288,19 @@ int nttb_bounds_errors(uint32_t* flags, int* enabled, int clear) {
 }
 
 // A wide (64-bit modulus) transform: AUTO takes the INT8 engine where it
-// serves the plan (n = 2^20, cyclic) and the CUDA-core Montgomery-64 engine
-// otherwise.
+// serves the plan (n = 2^20, cyclic) for fewer than 8 (polynomial, limb)
+// units, the CUDA-core Montgomery-64 engine otherwise.  Both spend about the
+// same number of integer multiplies per residue (the 64-bit REDCs and twiddle
+// products of the byte-plane epilogues match the radix-2 butterflies'); the
+// INT8 engine's two passes have the shorter latency (one 2^20 polynomial:
+// 82 against 95 us forward + inverse), the CUDA-core engine the higher
+// throughput from 16 units on (1.01 against 1.07 ms for 16).
+constexpr uint64_t kWideTcMaxUnits = 8;
 static int wide_transform(Plan64& p, const void* src, void* dst, uint32_t n_polys, bool inverse, int engine,
                           cudaStream_t s) {
-    if (engine == NTTB_ENGINE_AUTO) engine = wide_tc_serves(p) ? NTTB_ENGINE_INT8 : NTTB_ENGINE_SCALAR;
+    if (engine == NTTB_ENGINE_AUTO)
+        engine = wide_tc_serves(p) && (uint64_t)n_polys * p.n_limbs < kWideTcMaxUnits ? NTTB_ENGINE_INT8
+                                                                                       : NTTB_ENGINE_SCALAR;
     if (engine == NTTB_ENGINE_INT8) return wide_tc_transform64(p, src, dst, n_polys, inverse, s);
     return scalar_transform64(p, src, dst, n_polys, inverse, s);  // the 31-bit engines do not serve 64-bit moduli
 }

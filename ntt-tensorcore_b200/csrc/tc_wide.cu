@@ -39,6 +39,7 @@
 // the image while the modulus and direction stay the same.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -361,14 +362,28 @@ int wide_grid() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63]) return cached[dev & 63];
+    // two CTAs per SM need the whole shared-memory carveout
     cudaFuncSetAttribute(wide_pass<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem);
     cudaFuncSetAttribute(wide_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem);
-    int per = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, wide_pass<0>, kWThreads, kWSmem) != cudaSuccess || per < 1)
-        per = 1;
-    cudaGetLastError();
+    cudaFuncSetAttribute(wide_pass<0>, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(wide_pass<1>, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    // The runtime's occupancy answer for a tcgen05 kernel is one CTA per SM;
+    // count from the resources instead: TMEM holds two 256-column
+    // allocations, and shared memory and registers are checked here.
+    cudaFuncAttributes fa{};
+    int sms = 0, smem_sm = 0, regs_sm = 0, reserved = 0;
+    cudaFuncGetAttributes(&fa, wide_pass<0>);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cached[dev & 63] = (per > 2 ? 2 : per) * (sms > 0 ? sms : 1);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaGetLastError();
+    const size_t per_smem = fa.sharedSizeBytes + kWSmem + (size_t)reserved;
+    const size_t per_regs = (size_t)((fa.numRegs * 32 + 255) / 256 * 256) * (kWThreads / 32);
+    int fit = 2;
+    if (per_smem) fit = std::min<int>(fit, (int)(smem_sm / per_smem));
+    if (per_regs) fit = std::min<int>(fit, (int)(regs_sm / per_regs));
+    cached[dev & 63] = (fit < 1 ? 1 : fit) * (sms > 0 ? sms : 1);
     return cached[dev & 63];
 }
 
