@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60", "move", "klimb"], default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the secondary workloads (q60, uneven, serve) that a single-GPU default run "
+                         "measures after the headline and reports under `secondary`")
     ap.add_argument("--quick", action="store_true",
                     help="warm-up + timed steps only (no clock soak, e2e, comparisons or CPU leg): "
                          "the short run used under ncu")
@@ -946,10 +949,10 @@ def run_q60(args, world, rank, local):
         plan.transform(buf, buf, 1, engine=eng or engine, stream=stream)
         plan.transform(buf, buf, 1, inverse=True, engine=eng or engine, stream=stream)
 
-    def sixteen(i):
+    def sixteen(i, eng=None):
         b = pool[(16 * i) % 32:(16 * i) % 32 + 16]
-        plan.transform(b, b, 16, engine=engine, stream=stream)
-        plan.transform(b, b, 16, inverse=True, engine=engine, stream=stream)
+        plan.transform(b, b, 16, engine=eng or engine, stream=stream)
+        plan.transform(b, b, 16, inverse=True, engine=eng or engine, stream=stream)
 
     for i in range(max(3, args.warmup)):
         one(i)
@@ -963,6 +966,10 @@ def run_q60(args, world, rank, local):
     for i in range(3):
         one(i, "scalar")
     ms_sc, _ = timed(lambda i: one(i, "scalar"), max(10, args.steps // 4))
+    b16 = {}
+    for eng in ("int8", "scalar"):  # 16 polynomials per launch on each engine
+        sixteen(0, eng)
+        b16[eng], _ = timed(lambda i: sixteen(i, eng), max(3, args.steps // 8))
     # per-kernel device time: each pass kernel's share of the event-timed launches
     nb.profile_start()
     for i in range(args.steps):
@@ -1000,8 +1007,9 @@ def run_q60(args, world, rank, local):
         "dtype": "u64", "data": "synthetic: seeded uniform residues",
         "config": {"workload": Q60_WORKLOAD, "n": 1 << lg, "q": Q60, "l2": "rotating 40 x 8 MB", "parallelism": "replicas x%d" % world},
         "engine": engine,
-        "batch16": {"value": world * 16 * coeffs * max(3, args.steps // 8) / (ms16 / 1e3),
-                    "ms_per_step": ms16 / max(3, args.steps // 8)},
+        "batch16": dict({"value": world * 16 * coeffs * max(3, args.steps // 8) / (ms16 / 1e3),
+                          "ms_per_step": ms16 / max(3, args.steps // 8)},
+                         **{eng + "_ms_per_step": m / max(3, args.steps // 8) for eng, m in b16.items()}),
         "engines_coeffs_per_s": {engine: value,
                                  "scalar": world * coeffs * max(10, args.steps // 4) / (ms_sc / 1e3)},
         "kernels": {k: {"launches": v[0], "total_ms": v[1]} for k, v in prof.items()},
@@ -1166,6 +1174,38 @@ def profile_case(name):
     print("profile case %s ok" % name)
 
 
+def secondary_workloads(args, world, rank, local):
+    """The other configurations, measured in the same single-GPU run after the
+    headline (each one's own checks run too: round trips, the uneven batch's
+    oracle rows and round trip, the serving stream's oracle products).  A
+    summary of each JSON line; a failure is recorded, not raised."""
+    import copy
+    out = {}
+    for name, fn, steps in (("q60", run_q60, 50), ("uneven", run_uneven, 5), ("serve", run_serve, 0)):
+        a = copy.copy(args)
+        a.steps, a.warmup, a.serve_seconds = (steps or args.steps), 3, 1.5
+        t0 = time.time()
+        try:
+            r = fn(a, world, rank, local)
+        except Exception as e:  # reported beside the headline, which stands on its own
+            out[name] = {"error": "%s: %s" % (type(e).__name__, str(e)[:300])}
+            continue
+        keep = {k: r[k] for k in ("workload", "value", "unit", "ms_per_step", "steps", "engine", "batch16",
+                                  "engines_coeffs_per_s", "parity", "roofline", "graph_replay") if k in r}
+        keep["config"] = r.get("config", {}).get("workload")
+        if "serve" in r:
+            keep["serve"] = {"saturated_rps": r["serve"]["saturated"]["achieved_rps"],
+                             "p50_p99_ms": {k: [v["p50_ms"], v["p99_ms"]] for k, v in r["serve"]["load_levels"].items()}}
+            d = r["serve_device_resident"]
+            keep["serve_device_resident"] = {"saturated_rps": d["saturated"]["achieved_rps"],
+                                             "p50_p99_ms": {k: [v["p50_ms"], v["p99_ms"]] for k, v in d["load_levels"].items()}}
+        if r.get("cpu_baseline"):
+            keep["cpu_baseline"] = r["cpu_baseline"]
+        keep["wall_s"] = round(time.time() - t0, 1)
+        out[name] = keep
+    return out
+
+
 def main():
     args = parse()
     if args.profile_case:
@@ -1210,6 +1250,8 @@ def main():
     result, qs = run_ours(args, world, rank, local)
     if rank == 0 and world == 1 and not args.quick:
         result["cpu_baseline"] = bounded_cpu_baseline(qs)
+        if not args.no_secondary:
+            result["secondary"] = secondary_workloads(args, world, rank, local)
     if rank == 0:
         print(json.dumps(result))
     if world > 1:

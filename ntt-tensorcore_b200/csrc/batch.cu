@@ -115,9 +115,23 @@ struct BUnit {
     // ctr[after_ctr[d]] >= need[1 + d] (the last pass of unit after[d])
     uint32_t need[3];
     uint32_t after_ctr[2];
-    uint32_t pad_;
+    uint32_t dis;      // tensor-tile two-pass units: first of the unit's discard-group counters
+                       // (after the 1 + 2 n_units queue counters), else kNoDiscard
 };
 static_assert(sizeof(BUnit) % 16 == 0, "unit records are copied in 16-byte pieces");
+
+// Workspace lines of a two-pass unit's slot are dropped from the L2 without a
+// write-back once its pass B has read them (the slot's next owner rewrites
+// them; otherwise the dirty lines reach DRAM on eviction: 4 bytes per residue
+// never read).  A pass B tile reads columns v0 .. v0 + V of every row of the
+// slot; with V < 32 words a 128-byte line holds the columns of g = 32 / V
+// consecutive tiles, so the lines are dropped by the last of each group of g
+// tiles to finish reading (a counter per group), one line per row.
+constexpr uint32_t kNoDiscard = 0xFFFFFFFFu;
+__host__ __device__ inline uint32_t discard_group(uint32_t log_n, uint32_t lg1) {
+    const uint32_t V = 128u >> (log_n - lg1 - 6u);  // pass B vectors per tile row
+    return V >= 32u ? 1u : 32u / V;
+}
 
 struct BTile {
     uint32_t unit;
@@ -128,13 +142,13 @@ struct BArgs {
     const BModulus* mods;
     const BUnit* units;
     const BTile* tiles;
-    uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u;
-                    // [1 + 2 n_units + u] pass B tiles of unit u that finished reading its slot
+    uint32_t* ctr;  // [0] ticket; [1 + 2u] pass A tiles done, [2 + 2u] pass B tiles done of unit u
     const uint8_t* images;  // per modulus: DFT-64 byte-plane images (forward, inverse, negacyclic forward)
     uint32_t n_tiles, max_log;
     uint32_t n_units;       // units in the queue (range checks of the NTT_DEBUG_BOUNDS build)
     const uint32_t* ws;     // the workspace rings, ws_words words
     uint64_t ws_words;
+    uint32_t n_dis;         // discard-group counters after the queue counters
 };
 
 // NTT_DEBUG_BOUNDS build: the tile's unit, its tile index and its workspace
@@ -142,6 +156,10 @@ struct BArgs {
 __device__ __forceinline__ bool tile_in_range(const BArgs& a, const BTile& tl) {
     if (!NTTB_CHECK(g_batch_bounds, kBoundsQueue, tl.unit < a.n_units)) return false;
     const BUnit& u = a.units[tl.unit];
+    if (u.dis != kNoDiscard && (tl.pass_tile >> 31) && u.lg1 && discard_group(u.log_n, u.lg1) > 1 &&
+        !NTTB_CHECK(g_batch_bounds, kBoundsQueue,
+                    u.dis + (tl.pass_tile & 0x7fffffffu) / discard_group(u.log_n, u.lg1) < a.n_dis))
+        return false;
     const uint32_t pass = tl.pass_tile >> 31, tile = tl.pass_tile & 0x7fffffffu;
     if (!NTTB_CHECK(g_batch_bounds, kBoundsQueue, tile < (pass ? u.tiles_b : u.tiles_a) && u.log_n <= a.max_log))
         return false;
@@ -376,28 +394,6 @@ __device__ __forceinline__ void run_tile(const BArgs& a, const BUnit& u, uint32_
 // Thread 0 of a tile: waits until the tile's inputs are complete (pass B:
 // every pass A tile of its unit; pass A: the previous owner of its workspace
 // slot and the units it depends on).  False if a wait ran out of budget.
-// After a pass B tile of a two-pass unit: the last of the unit's pass B
-// tiles to finish invalidates the unit's workspace slot in the L2 without
-// writing it back (its words have all been read; the slot's next owner, which
-// waits for this tile's completion signal, rewrites it).  Without this the
-// dirty slot lines would reach DRAM on eviction: 4 bytes per residue that are
-// never read.  Called by every thread of the CTA after the tile's stores and
-// a CTA barrier, before the tile's completion signal.
-__device__ __forceinline__ void release_slot(const BArgs& a, const BUnit& u, uint32_t ui, uint32_t* s_last) {
-    if (threadIdx.x == 0) {
-        __threadfence();
-        *s_last = atomicAdd(a.ctr + 1 + 2 * a.n_units + ui, 1u) + 1u == u.tiles_b;
-    }
-    __syncthreads();
-    if (!*s_last) return;
-    const uint64_t lines = (4ull << u.log_n) / 128u;
-    const uint8_t* base = reinterpret_cast<const uint8_t*>(u.ws);
-    for (uint64_t i = threadIdx.x; i < lines; i += blockDim.x)
-        asm volatile("discard.global.L2 [%0], 128;" ::"l"(base + 128u * i) : "memory");
-    __threadfence();
-    __syncthreads();
-}
-
 __device__ __forceinline__ bool wait_deps(const BArgs& a, const BUnit& u, uint32_t ui, uint32_t pass) {
     bool ok = true;
     if (pass == 1) {
@@ -656,6 +652,30 @@ __device__ __forceinline__ void signal_done(uint32_t* counter) {
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
 }
 
+// Pass B, warp 0, after the CTA barrier that follows the tile's workspace
+// loads: counts the tile into its line group; the group's last tile drops the
+// group's lines (one 128-byte line per row of the slot: columns 32 gi ..
+// 32 gi + 32; with V >= 32 the tile's own V / 32 lines per row).  The slot's
+// next owner waits for every pass B tile of this unit before writing it.
+__device__ __forceinline__ void discard_read_lines(const BArgs& a, const BUnit& u, const TcGeo& g, uint32_t tile) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t grp = g.V >= 32u ? 1u : 32u / g.V, gi = tile / grp;
+    uint32_t last = 1;
+    if (grp > 1) {
+        // relaxed: the members' loads have returned (their values are in
+        // shared memory, behind the CTA barrier) before they count in
+        if (lane == 0)
+            last = atomicAdd(a.ctr + 1 + 2 * a.n_units + u.dis + gi, 1u) + 1u == min(grp, u.tiles_b - gi * grp);
+        last = __shfl_sync(~0u, last, 0);
+    }
+    if (!last) return;
+    const uint32_t per_row = grp > 1 ? 1u : g.V >> 5, lines = (8192u / g.V) * per_row;
+    const uint32_t* first = g.src + (grp > 1 ? 32u * gi : g.v0);
+    for (uint32_t i = lane; i < lines; i += 32u)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(first + (size_t)(i / per_row) * g.C + 32u * (i % per_row))
+                     : "memory");
+}
+
 __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile, TcState& st) {
     const uint32_t tid = threadIdx.x;
     const TcGeo g = tc_geo(a, u, pass, tile);
@@ -695,6 +715,7 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
         tca::issue_k256(st.taddr, tc::smem_u32(base + kTcA), 128, tc::smem_u32(base + kTcImg), 256, 256);
         tc::commit(bar);
     }
+    if (pass == 1 && u.dis != kNoDiscard && tid < 32) discard_read_lines(a, u, g, tile);  // during the MMA
     if (st.pend_img) {
         st.ph_img ^= 1u;
         st.pend_img = 0;
@@ -844,7 +865,7 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
 template <uint32_t G>
 __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__ BArgs a) {
     extern __shared__ __align__(1024) uint8_t tc_raw[];
-    __shared__ uint32_t s_ticket, s_taddr, s_last;
+    __shared__ uint32_t s_ticket, s_taddr;
     __shared__ M32 s_ar[kMaxRows];
     TcState st;
     st.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
@@ -887,7 +908,6 @@ __global__ void __launch_bounds__(256, 2) batch_queue_tc(const __grid_constant__
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
         __syncthreads();
-        if (pass == 1 && u.lg1) release_slot(a, u, tl.unit, &s_last);
         if (threadIdx.x == 0) signal_done(a.ctr + 1 + 2 * tl.unit + pass);
     }
     tc::fence_before_sync();
@@ -899,7 +919,7 @@ template <uint32_t E, uint32_t T, uint32_t G>
 // more resident CTAs for the small register groups
 __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T) batch_queue(const __grid_constant__ BArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
-    __shared__ uint32_t s_ticket, s_last;
+    __shared__ uint32_t s_ticket;
     __shared__ M32 s_ar[kMaxRows];
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ctr, 1u);
@@ -919,7 +939,6 @@ __global__ void __launch_bounds__(T, (G == 1 ? 1536u : G == 3 ? 768u : 512u) / T
         __syncthreads();
         run_tile<T, G>(a, u, pass, tile, sm, s_ar);
         __syncthreads();
-        if (pass == 1 && u.lg1) release_slot(a, u, tl.unit, &s_last);
         if (threadIdx.x == 0) signal_done(a.ctr + 1 + 2 * tl.unit + pass);
     }
 }
@@ -1020,7 +1039,7 @@ struct Batch {
     BTile* d_tiles = nullptr;
     uint32_t* d_ctr = nullptr;
     uint32_t* d_ws = nullptr;
-    uint32_t n_units = 0, n_tiles = 0;
+    uint32_t n_units = 0, n_tiles = 0, n_dis = 0;
     size_t ws_bytes = 0;
     int grid = 0;
     cudaGraphExec_t gexec = nullptr;
@@ -1226,6 +1245,7 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
     std::vector<std::vector<int32_t>> slot_owner(25);
     for (uint32_t L = 1; L < 25; L++) slot_owner[L].assign(lay.slots[L], -1);
     uint32_t next_slot[25] = {};
+    uint32_t n_dis = 0;
     std::deque<uint32_t> pend_b;
     uint32_t phase = 0;
     auto emit_b = [&](uint32_t ui) {
@@ -1252,6 +1272,12 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
                 u.need[1 + d] = W.lg1 ? W.tiles_b : W.tiles_a;
             }
         }
+        u.dis = kNoDiscard;
+        if (u.lg1 && (u.flags & UF_TC)) {  // pass B rows span >= 64 words: lines never straddle two rows
+            u.dis = n_dis;
+            const uint32_t g = discard_group(u.log_n, u.lg1);
+            if (g > 1) n_dis += (u.tiles_b + g - 1) / g;
+        }
         if (u.lg1) {
             const uint32_t L = u.log_n, slot = next_slot[L]++ % lay.slots[L];
             // word offset, rebased on the workspace allocation later
@@ -1275,6 +1301,17 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
     return 0;
 }
 
+// Discard-group counters the planned units use (after the 1 + 2 units queue counters).
+uint32_t discard_counters(const std::vector<BUnit>& units) {
+    uint32_t n = 0;
+    for (const BUnit& u : units)
+        if (u.dis != kNoDiscard) {
+            const uint32_t g = discard_group(u.log_n, u.lg1);
+            if (g > 1) n = std::max(n, u.dis + (u.tiles_b + g - 1) / g);
+        }
+    return n;
+}
+
 int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, const nttb_batch_config& cfg, Batch** out) {
     if (int rc = check_config(cfg)) return rc;
     std::vector<BUnit> units;
@@ -1292,11 +1329,12 @@ int create_batch(BatchPlan* P, const nttb_batch_job* jobs, uint32_t n_jobs, cons
     b->var = find_variant(cfg.tile_elems, cfg.threads, cfg.group, cfg.tensor && any_tc ? 1u : 0u);
     b->n_units = (uint32_t)units.size();
     b->n_tiles = (uint32_t)tiles.size();
+    b->n_dis = discard_counters(units);
     b->ws_bytes = (size_t)lay.words * 4;
     bool ok = true;
     ok = ok && cudaMalloc(&b->d_units, std::max<size_t>(1, units.size()) * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMalloc(&b->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(BTile)) == cudaSuccess;
-    ok = ok && cudaMalloc(&b->d_ctr, (1 + 3 * (size_t)units.size()) * 4) == cudaSuccess;
+    ok = ok && cudaMalloc(&b->d_ctr, (1 + 2 * (size_t)units.size() + b->n_dis) * 4) == cudaSuccess;
     if (ok && b->ws_bytes) ok = cudaMalloc(&b->d_ws, b->ws_bytes) == cudaSuccess;
     if (!ok) {
         free_batch(b);
@@ -1329,7 +1367,8 @@ int launch_batch(Batch* b, cudaStream_t s, bool count) {
     a.n_units = b->n_units;
     a.ws = b->d_ws;
     a.ws_words = b->ws_bytes / 4;
-    if (cudaMemsetAsync(b->d_ctr, 0, (1 + 3 * (size_t)b->n_units) * 4, s) != cudaSuccess)
+    a.n_dis = b->n_dis;
+    if (cudaMemsetAsync(b->d_ctr, 0, (1 + 2 * (size_t)b->n_units + b->n_dis) * 4, s) != cudaSuccess)
         return fail(NTTB_ERR_CUDA, "batch: counter reset failed");
     if (count) {
         ProfScope prof("batch_queue", s);
@@ -1380,7 +1419,7 @@ int runner_reserve(BatchRunner* r, size_t units, size_t tiles) {
     runner_free_queue(r);
     bool ok = cudaMalloc(&r->d_units, cu * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMalloc(&r->d_tiles, ct * sizeof(BTile)) == cudaSuccess;
-    ok = ok && cudaMalloc(&r->d_ctr, (1 + 3 * cu) * 4) == cudaSuccess;
+    ok = ok && cudaMalloc(&r->d_ctr, (1 + 2 * cu + ct) * 4) == cudaSuccess;  // discard groups <= tiles
     ok = ok && cudaMallocHost(&r->h_units, cu * sizeof(BUnit)) == cudaSuccess;
     ok = ok && cudaMallocHost(&r->h_tiles, ct * sizeof(BTile)) == cudaSuccess;
     if (!ok) {
@@ -1418,7 +1457,7 @@ void runner_destroy(BatchRunner* r) {
 }
 
 size_t runner_device_bytes(const BatchRunner* r) {
-    return r->ws_bytes + r->cap_units * (sizeof(BUnit) + 8) + r->cap_tiles * sizeof(BTile);
+    return r->ws_bytes + r->cap_units * (sizeof(BUnit) + 8) + r->cap_tiles * (sizeof(BTile) + 4);
 }
 
 // Plans the jobs, uploads the queue from pinned staging and launches, all on
@@ -1447,11 +1486,12 @@ int runner_run(BatchRunner* r, const nttb_batch_job* jobs, uint32_t n_jobs, cuda
     a.n_units = (uint32_t)r->units.size();
     a.ws = r->d_ws;
     a.ws_words = r->ws_bytes / 4;
+    a.n_dis = discard_counters(r->units);
     bool ok = cudaMemcpyAsync(r->d_units, r->h_units, r->units.size() * sizeof(BUnit), cudaMemcpyHostToDevice, s) ==
               cudaSuccess;
     ok = ok && cudaMemcpyAsync(r->d_tiles, r->h_tiles, r->tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice, s) ==
                    cudaSuccess;
-    ok = ok && cudaMemsetAsync(r->d_ctr, 0, (1 + 3 * r->units.size()) * 4, s) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(r->d_ctr, 0, (1 + 2 * r->units.size() + a.n_dis) * 4, s) == cudaSuccess;
     if (!ok) return fail(NTTB_ERR_CUDA, "batch runner: queue upload failed");
     const int grid = (int)std::min<size_t>((size_t)r->grid, r->tiles.size());
     ProfScope prof("batch_queue", s);
