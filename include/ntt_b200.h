@@ -41,12 +41,16 @@ enum {
 
 /* Inner-DFT engines.  AUTO picks the fastest one that serves the request:
  * the INT8 tensor-core kernel at N = 2^16 from 8 (polynomial, limb) units
- * on, the CUDA-core engine otherwise. */
+ * on; the batch queue's tensor tiles at N = 2^17 .. 2^20 once a call holds
+ * 2^20 residues; the CUDA-core engine otherwise.  The tiles engine keeps up
+ * to four prepared queues per plan (one per source, destination, count,
+ * direction), each with its own workspace ring of up to 16 x N words. */
 enum {
     NTTB_ENGINE_AUTO = 0,
     NTTB_ENGINE_SCALAR = 1, /* CUDA-core radix-2 in shared memory */
     NTTB_ENGINE_DMMA = 2,   /* FP64 mma.sync m8n8k4 radix-8 contractions (the plain drop-in form) */
-    NTTB_ENGINE_INT8 = 3    /* tcgen05 kind::i8, byte-plane radix-64 contractions, INT32 in TMEM */
+    NTTB_ENGINE_INT8 = 3,   /* tcgen05 kind::i8, byte-plane radix-64 contractions, INT32 in TMEM */
+    NTTB_ENGINE_TILES = 4   /* the batch queue's tcgen05 tensor tiles (two-pass four-step, 2^13 .. 2^20) */
 };
 
 NTTB_API const char* nttb_version(void);
@@ -115,9 +119,11 @@ NTTB_API int nttb_plan_get_info(const nttb_plan* plan, nttb_plan_info* out);
  * in place.  Replaces ntt_forward/inverse_{basic,tlmop,optimized}
  * (src/ntt_basic.cu:268-334, src/ntt_optimized.cu:515-613) and
  * ntt_forward/inverse_batch (src/ntt_basic.cu:337-389).  NTTB_ENGINE_AUTO
- * runs the INT8 tensor-core kernel on the words directly for n = 2^16 and
- * q < 2^31 from 8 polynomials on, the CUDA-core engine otherwise (residues
- * must be below 2^32, as the reference's kernels assume them below q). */
+ * runs, for q < 2^31, the INT8 tensor-core kernel on the words directly for
+ * n = 2^16 from 8 polynomials on, the batch queue's tensor tiles for
+ * n = 2^17 .. 2^20 from 2^20 words per call, the CUDA-core engine otherwise
+ * (residues must be below 2^32, as the reference's kernels assume them below
+ * q). */
 NTTB_API int nttb_u64_transform(const nttb_plan* plan, uint64_t* d_data, uint64_t batch, int inverse, int engine,
                        void* stream);
 /* The reference's four-step map, in place.  Replaces

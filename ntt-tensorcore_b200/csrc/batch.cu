@@ -73,7 +73,9 @@ namespace {
 
 constexpr uint32_t BF_INV = 1, BF_PRE_PSI = 2, BF_POST_TW = 4, BF_STORE_T = 8, BF_POST_SCALE = 16, BF_POST_PSI = 32,
                    BF_PRE_MUL = 64;
-constexpr uint32_t UF_INV = 1, UF_NEGA = 2, UF_TC = 4;  // UF_TC: tensor-core tiles
+// UF_TC: tensor-core tiles; UF_W64: the unit's data (and its source) are
+// uint64 words holding residues (tensor-tile two-pass units only)
+constexpr uint32_t UF_INV = 1, UF_NEGA = 2, UF_TC = 4, UF_W64 = 8;
 constexpr uint32_t kMaxRows = 32;
 
 // Power tables: x^e R for e < 2^max_log as hi[e >> kLoBits] * lo[e & lo_mask]
@@ -99,7 +101,8 @@ __device__ __forceinline__ uint32_t pw(const BModulus& M, const M32& ar, uint32_
 }
 
 struct BUnit {
-    uint32_t* data;    // row 0 of the unit; row r (limb) at data + r n
+    uint32_t* data;    // row 0 of the unit; row r (limb) at data + r n (uint64 words with UF_W64)
+    const void* in;    // pass A reads here instead of data (same layout), or null
     uint32_t* ws;      // workspace slot (two-pass units)
     const uint32_t* pre_mul;  // inverse of a product: the input is data . pre_mul (same layout), else null
     uint32_t mod0;     // modulus index of row 0; row r uses mod0 + r
@@ -117,6 +120,7 @@ struct BUnit {
     uint32_t after_ctr[2];
     uint32_t dis;      // tensor-tile two-pass units: first of the unit's discard-group counters
                        // (after the 1 + 2 n_units queue counters), else kNoDiscard
+    uint32_t pad_[2];
 };
 static_assert(sizeof(BUnit) % 16 == 0, "unit records are copied in 16-byte pieces");
 
@@ -128,6 +132,12 @@ static_assert(sizeof(BUnit) % 16 == 0, "unit records are copied in 16-byte piece
 // consecutive tiles, so the lines are dropped by the last of each group of g
 // tiles to finish reading (a counter per group), one line per row.
 constexpr uint32_t kNoDiscard = 0xFFFFFFFFu;
+
+// Job flags of the plan-transform route (tiles_transform32), which the C ABI
+// refuses: kJobW64 -- data and source are uint64 words; kJobSrc -- pass A
+// reads `pointwise` (the source, same layout), pass B writes data.
+constexpr uint32_t kJobW64 = 1u << 30, kJobSrc = 1u << 29;
+constexpr uint32_t kPublicJobFlags = NTTB_BATCH_INVERSE | NTTB_NEGACYCLIC | NTTB_BATCH_POLYMUL;
 __host__ __device__ inline uint32_t discard_group(uint32_t log_n, uint32_t lg1) {
     const uint32_t V = 128u >> (log_n - lg1 - 6u);  // pass B vectors per tile row
     return V >= 32u ? 1u : 32u / V;
@@ -508,6 +518,10 @@ __device__ __forceinline__ void tc_level2(const BUnit& u, uint32_t pass, uint32_
             uint32_t* o = u.ws + (size_t)(v0 + v) * N1 + k1;
 #pragma unroll
             for (uint32_t k2 = 0; k2 < R; k2++) o[64u * k2] = use_fac ? ar.mul(x[k2], fac[v * R + k2]) : x[k2];
+        } else if (u.flags & UF_W64) {
+            uint64_t* o = reinterpret_cast<uint64_t*>(u.data) + (size_t)k1 * N1 + v0 + v;
+#pragma unroll
+            for (uint32_t k2 = 0; k2 < R; k2++) o[(size_t)64u * k2 * N1] = use_fac ? ar.mul(x[k2], fac[k2]) : x[k2];
         } else {
             uint32_t* o = u.data + (size_t)k1 * N1 + v0 + v;
 #pragma unroll
@@ -553,8 +567,9 @@ __device__ __forceinline__ void l2_store8(uint8_t* A2, const uint32_t (&y)[8], u
 // Geometry of a tensor tile.
 struct TcGeo {
     uint32_t L, n, shift, N1, lg, rl, rp, lgV, V, C, v0;
-    const uint32_t* src;
+    const uint32_t* src;  // uint64 words when w64
     bool pre, mma2, inv, nega;
+    bool w64;             // pass A source / pass B destination are uint64 words
     uint32_t variant, variant2, key, key2;
 };
 __device__ __forceinline__ TcGeo tc_geo(const BArgs& a, const BUnit& u, uint32_t pass, uint32_t tile) {
@@ -572,7 +587,8 @@ __device__ __forceinline__ TcGeo tc_geo(const BArgs& a, const BUnit& u, uint32_t
     g.V = 1u << g.lgV;
     g.C = pass == 0 ? g.n >> u.lg1 : g.N1;   // columns of the pass's matrix
     g.v0 = tile << g.lgV;
-    g.src = pass == 0 ? u.data : u.ws;
+    g.src = pass == 0 ? static_cast<const uint32_t*>(u.in ? u.in : u.data) : u.ws;
+    g.w64 = u.flags & UF_W64;
     g.pre = pass == 0 && u.pre_mul;
     g.mma2 = g.rl >= 3;  // level 2 on the tensor cores
     g.variant = g.inv ? 1u : (pass == 0 && g.nega ? 2u : 0u);
@@ -623,15 +639,25 @@ __device__ __forceinline__ void st_keep(uint32_t* p, uint32_t v, uint64_t pol) {
 // Operand A: row m = (b2, v) = b2 V + v holds column v0 + v's elements
 // j = r' a2 + b2 in K order a2; thread (m, hh) fills 16-byte chunks hh,
 // hh + 2, ..  A product's inverse multiplies by the pointwise operand on the way.
-__device__ __forceinline__ void tc_operand(const BUnit& u, const TcGeo& g, const M32& ar, uint8_t* A) {
+// `w64`: the source rows are uint64 words (pass A of a UF_W64 unit).
+__device__ __forceinline__ void tc_operand(const BUnit& u, const TcGeo& g, const M32& ar, uint8_t* A, bool w64) {
     const uint32_t mm = threadIdx.x & 127u, hh = threadIdx.x >> 7;
     const size_t off0 = (size_t)(mm >> g.lgV) * g.C + g.v0 + (mm & (g.V - 1u));
     const size_t step = (size_t)g.rp * g.C;  // between consecutive a2
     uint32_t xs[32];
+    if (w64) {  // the low words (residues < q)
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(g.src);
 #pragma unroll
-    for (uint32_t j = 0; j < 8; j++)
+        for (uint32_t j = 0; j < 8; j++)
 #pragma unroll
-        for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcs(g.src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
+            for (uint32_t t = 0; t < 4; t++)
+                xs[4 * j + t] = (uint32_t)__ldcs(src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
+    } else {
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++)
+#pragma unroll
+            for (uint32_t t = 0; t < 4; t++) xs[4 * j + t] = __ldcs(g.src + off0 + (size_t)(8u * j + 4u * hh + t) * step);
+    }
     if (g.pre) {
 #pragma unroll
         for (uint32_t j = 0; j < 8; j++)
@@ -706,7 +732,7 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
     }
     if (!mma2 && tid >= 128 && tid < 128 + rp / 2)
         fac[tid] = pw(M, ar, wb, (((n >> rl) * (tid - 128)) & (n - 1u)) << shift);
-    tc_operand(u, g, ar, base + kTcA);
+    tc_operand(u, g, ar, base + kTcA, pass == 0 && g.w64);
     tc::fence_proxy_async_smem();
     __syncthreads();
     if (tid == 0) {
@@ -847,6 +873,14 @@ __device__ __forceinline__ void run_tc_tile(const BArgs& a, const BUnit& u, uint
                     const uint32_t k2 = 8u * gq + i;
                     const uint32_t y = tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv);
                     st_keep(o + 64u * k2, tca::canon(tca::mont_lazy(y, fac[v * rp + k2], q, qinv), q), keep);
+                }
+            } else if (g.w64) {
+                uint64_t* o = reinterpret_cast<uint64_t*>(u.data) + (size_t)k1 * N1 + v0 + v;
+#pragma unroll
+                for (uint32_t i = 0; i < 8; i++) {
+                    const uint32_t k2 = 8u * gq + i;
+                    __stcs(o + (size_t)64u * k2 * N1,
+                           (uint64_t)tca::canon(tca::combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), q));
                 }
             } else {
                 uint32_t* o = u.data + (size_t)k1 * N1 + v0 + v;
@@ -1163,8 +1197,8 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
     };
     std::vector<Pending> list;
     // Units of one transform over rows [l0, l0 + rows) of `data`.
-    auto add_units = [&](uint32_t j, uint32_t* data, const uint32_t* pre_mul, uint32_t L, uint32_t first,
-                         uint32_t n_limbs, uint32_t uf, uint32_t phase, std::vector<uint32_t>* ids,
+    auto add_units = [&](uint32_t j, uint32_t* data, const void* in, const uint32_t* pre_mul, uint32_t L,
+                         uint32_t first, uint32_t n_limbs, uint32_t uf, uint32_t phase, std::vector<uint32_t>* ids,
                          const std::vector<uint32_t>* dep_a, const std::vector<uint32_t>* dep_b) -> int {
         const uint32_t n = 1u << L;
         UnitShape sh;
@@ -1172,11 +1206,15 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
             return fail(NTTB_ERR_INVALID_ARG, "batch job %u: log_n %u too large for tile %u", j, L, E);
         const uint32_t lg1 = sh.lg1, per = sh.per;
         const bool tcu = sh.tc;
+        if ((uf & UF_W64 || in) && !(tcu && lg1))
+            return fail(NTTB_ERR_UNSUPPORTED, "batch job %u: uint64 words or a separate source need tensor tiles", j);
+        const size_t es = (uf & UF_W64) ? 8 : 4;  // bytes per residue of data and in
         uint32_t k = 0;
         for (uint32_t l0 = 0; l0 < n_limbs; l0 += per, k++) {
             Pending p{};
             BUnit& u = p.u;
-            u.data = data + (size_t)l0 * n;
+            u.data = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(data) + (size_t)l0 * n * es);
+            u.in = in ? static_cast<const char*>(in) + (size_t)l0 * n * es : nullptr;
             u.pre_mul = pre_mul ? pre_mul + (size_t)l0 * n : nullptr;
             u.mod0 = first + l0;
             u.log_n = L;
@@ -1210,20 +1248,29 @@ int plan_batch(const BatchPlan& P, const nttb_batch_job* jobs, uint32_t n_jobs, 
         if ((J.flags & NTTB_NEGACYCLIC) && !P.negacyclic)
             return fail(NTTB_ERR_INVALID_ARG, "batch job %u: negacyclic job on a cyclic plan", j);
         const uint32_t nega = (J.flags & NTTB_NEGACYCLIC) ? UF_NEGA : 0u;
+        const uint32_t w64 = (J.flags & kJobW64) ? UF_W64 : 0u;
+        const void* in = (J.flags & kJobSrc) ? static_cast<const void*>(J.pointwise) : nullptr;
+        if ((J.flags & kJobSrc) && (!in || in == J.data))
+            return fail(NTTB_ERR_INVALID_ARG, "batch job %u: a separate source must be given and distinct", j);
+        if ((J.flags & NTTB_BATCH_POLYMUL) && (w64 || in))
+            return fail(NTTB_ERR_INVALID_ARG, "batch job %u: products take uint32 residues in place", j);
         if (J.flags & NTTB_BATCH_POLYMUL) {
             if (!J.pointwise || J.pointwise == J.data)
                 return fail(NTTB_ERR_INVALID_ARG, "batch job %u: a product needs a distinct second operand", j);
             std::vector<uint32_t> fa, fb;
-            if (int rc = add_units(j, J.data, nullptr, J.log_n, J.first_modulus, J.n_limbs, nega, 0, &fa, nullptr, nullptr)) return rc;
-            if (int rc = add_units(j, const_cast<uint32_t*>(J.pointwise), nullptr, J.log_n, J.first_modulus, J.n_limbs,
-                                   nega, 0, &fb, nullptr, nullptr))
+            if (int rc = add_units(j, J.data, nullptr, nullptr, J.log_n, J.first_modulus, J.n_limbs, nega, 0, &fa,
+                                   nullptr, nullptr))
                 return rc;
-            if (int rc = add_units(j, J.data, J.pointwise, J.log_n, J.first_modulus, J.n_limbs, nega | UF_INV, 1,
+            if (int rc = add_units(j, const_cast<uint32_t*>(J.pointwise), nullptr, nullptr, J.log_n, J.first_modulus,
+                                   J.n_limbs, nega, 0, &fb, nullptr, nullptr))
+                return rc;
+            if (int rc = add_units(j, J.data, nullptr, J.pointwise, J.log_n, J.first_modulus, J.n_limbs, nega | UF_INV, 1,
                                    nullptr, &fa, &fb))
                 return rc;
         } else {
-            const uint32_t uf = ((J.flags & NTTB_BATCH_INVERSE) ? UF_INV : 0u) | nega;
-            if (int rc = add_units(j, J.data, nullptr, J.log_n, J.first_modulus, J.n_limbs, uf, 0, nullptr, nullptr, nullptr))
+            const uint32_t uf = ((J.flags & NTTB_BATCH_INVERSE) ? UF_INV : 0u) | nega | w64;
+            if (int rc = add_units(j, J.data, in, nullptr, J.log_n, J.first_modulus, J.n_limbs, uf, 0, nullptr, nullptr,
+                                   nullptr))
                 return rc;
         }
     }
@@ -1525,6 +1572,101 @@ uint32_t batch_device_errors(bool clear) {
     return v;
 }
 
+// ---- plan transforms on the tensor tiles (NTTB_ENGINE_TILES) -----------------------
+// A transform of n_polys x n_limbs (polynomial, limb) units of 2^L residues,
+// 13 <= L <= 20, as one persistent launch of the queue's tensor tiles: a
+// batch plan over the plan's moduli at max_log = L (the same roots as the
+// plan's, so the results are the other engines'), and one queue per
+// (source, destination, count, direction, word size), built on first use and
+// then replayed: a counter reset and the launch, no host work.  The queue
+// reads the source in pass A and writes the destination in pass B (uint64
+// words for the drop-in's layout).  kTileQueues queues are kept per plan, the
+// least recently used one replaced; each owns its workspace ring (up to 16
+// slots of 2^L words).  Calls that share a plan are ordered on one stream.
+namespace {
+constexpr size_t kTileQueues = 4;
+struct TileEntry {
+    const void* src;
+    void* dst;
+    uint32_t n_polys;
+    bool inverse, u64;
+    Batch* b;
+    uint64_t used;
+};
+struct TileCache {
+    nttb_batch_plan* plan = nullptr;
+    std::vector<TileEntry> entries;
+    uint64_t clock = 0;
+};
+TileCache* tile_cache(Plan32& p) {
+    std::lock_guard<std::mutex> lock(p.engine_mu);
+    auto* c = static_cast<TileCache*>(p.engine_data[3]);
+    if (c) return c;
+    std::vector<uint64_t> q(p.n_limbs);
+    for (uint32_t l = 0; l < p.n_limbs; l++) q[l] = p.limbs[l].q;
+    nttb_batch_plan* h = nullptr;
+    if (nttb_batch_plan_create(q.data(), p.n_limbs, p.log_n, p.negacyclic ? NTTB_NEGACYCLIC : 0u, &h) != NTTB_OK)
+        return nullptr;
+    c = new TileCache();
+    c->plan = h;
+    p.engine_data[3] = c;
+    return c;
+}
+}  // namespace
+
+bool tiles_serve(const Plan32& p) { return p.log_n >= 13 && p.log_n <= 20; }
+
+int tiles_transform32(Plan32& p, const void* src, void* dst, bool u64, uint32_t n_polys, bool inverse,
+                      cudaStream_t s) {
+    if (!tiles_serve(p)) return 1;
+    TileCache* c = tile_cache(p);
+    if (!c) return 2;
+    TileEntry* e = nullptr;
+    for (TileEntry& t : c->entries)
+        if (t.src == src && t.dst == dst && t.n_polys == n_polys && t.inverse == inverse && t.u64 == u64) e = &t;
+    if (!e) {
+        const size_t es = u64 ? 8 : 4, poly = (size_t)p.n_limbs << p.log_n;
+        std::vector<nttb_batch_job> jobs(n_polys);
+        for (uint32_t i = 0; i < n_polys; i++) {
+            nttb_batch_job& J = jobs[i];
+            J.data = reinterpret_cast<uint32_t*>(static_cast<char*>(dst) + i * poly * es);
+            J.log_n = p.log_n;
+            J.n_limbs = p.n_limbs;
+            J.first_modulus = 0;
+            J.flags = (inverse ? NTTB_BATCH_INVERSE : 0u) | (p.negacyclic ? NTTB_NEGACYCLIC : 0u) | (u64 ? kJobW64 : 0u);
+            J.pointwise = nullptr;
+            if (src != dst) {
+                J.flags |= kJobSrc;
+                J.pointwise = reinterpret_cast<uint32_t*>(const_cast<char*>(static_cast<const char*>(src) + i * poly * es));
+            }
+        }
+        nttb_batch_config cfg = default_config();
+        cfg.tensor = 1;
+        Batch* b = nullptr;
+        if (create_batch(&c->plan->p, jobs.data(), n_polys, cfg, &b)) return 2;
+        if (c->entries.size() >= kTileQueues) {
+            auto lru = std::min_element(c->entries.begin(), c->entries.end(),
+                                        [](const TileEntry& x, const TileEntry& y) { return x.used < y.used; });
+            cudaStreamSynchronize(s);  // the evicted queue may still run on this stream
+            free_batch(lru->b);
+            c->entries.erase(lru);
+        }
+        c->entries.push_back({src, dst, n_polys, inverse, u64, b, 0});
+        e = &c->entries.back();
+    }
+    e->used = ++c->clock;
+    return launch_batch(e->b, s, true) ? 2 : 0;
+}
+
+void tiles_release(Plan32* p) {
+    auto* c = static_cast<TileCache*>(p->engine_data[3]);
+    if (!c) return;
+    for (TileEntry& t : c->entries) free_batch(t.b);
+    nttb_batch_plan_destroy(c->plan);
+    delete c;
+    p->engine_data[3] = nullptr;
+}
+
 }  // namespace nttb
 
 using nttb::Batch;
@@ -1534,6 +1676,15 @@ using nttb::fail;
 struct nttb_batch {
     Batch* b;
 };
+
+// Job flags a C-ABI caller may set (the rest are the plan-transform route's).
+static int check_public_flags(const nttb_batch_job* jobs, uint32_t n_jobs, const char* what) {
+    for (uint32_t j = 0; j < n_jobs; j++)
+        if (jobs[j].flags & ~nttb::kPublicJobFlags)
+            return fail(NTTB_ERR_INVALID_ARG, "%s: job %u has unknown flag bits 0x%x", what, j,
+                        jobs[j].flags & ~nttb::kPublicJobFlags);
+    return NTTB_OK;
+}
 
 extern "C" {
 
@@ -1677,6 +1828,7 @@ NTTB_API int nttb_batch_default_config(nttb_batch_config* out) {
 NTTB_API int nttb_batch_create(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs,
                                const nttb_batch_config* config, nttb_batch** out) {
     if (!plan || !out || (!jobs && n_jobs)) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_create: null argument");
+    if (int rc = check_public_flags(jobs, n_jobs, "nttb_batch_create")) return rc;
     const nttb_batch_config cfg = config ? *config : plan->p.have_tuned ? plan->p.tuned : nttb::default_config();
     Batch* b = nullptr;
     if (int rc = nttb::create_batch(&plan->p, jobs, n_jobs, cfg, &b)) return rc;
@@ -1757,6 +1909,7 @@ NTTB_API int nttb_batch_ctas(const nttb_batch* batch, uint32_t* ctas) {
 NTTB_API int nttb_batch_autotune(nttb_batch_plan* plan, const nttb_batch_job* jobs, uint32_t n_jobs, void* stream,
                                  nttb_batch_config* out) {
     if (!plan || !jobs || n_jobs == 0) return fail(NTTB_ERR_INVALID_ARG, "nttb_batch_autotune: no jobs");
+    if (int rc = check_public_flags(jobs, n_jobs, "nttb_batch_autotune")) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // Sample of the mix on scratch buffers (the caller's data is untouched):
     // up to two jobs per (log_n, direction, twist, product) with at most 8

@@ -302,6 +302,7 @@ static int wide_transform(Plan64& p, const void* src, void* dst, uint32_t n_poly
         engine = wide_tc_serves(p) && (uint64_t)n_polys * p.n_limbs < kWideTcMaxUnits ? NTTB_ENGINE_INT8
                                                                                        : NTTB_ENGINE_SCALAR;
     if (engine == NTTB_ENGINE_INT8) return wide_tc_transform64(p, src, dst, n_polys, inverse, s);
+    if (engine == NTTB_ENGINE_TILES) return 1;  // the batch queue's tiles take moduli < 2^31
     return scalar_transform64(p, src, dst, n_polys, inverse, s);  // the 31-bit engines do not serve 64-bit moduli
 }
 

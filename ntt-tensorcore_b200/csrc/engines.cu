@@ -13,6 +13,7 @@ static int env_engine() {
     if (!std::strcmp(e, "scalar")) return NTTB_ENGINE_SCALAR;
     if (!std::strcmp(e, "dmma")) return NTTB_ENGINE_DMMA;
     if (!std::strcmp(e, "int8")) return NTTB_ENGINE_INT8;
+    if (!std::strcmp(e, "tiles")) return NTTB_ENGINE_TILES;
     return NTTB_ENGINE_AUTO;
 }
 
@@ -21,9 +22,18 @@ static int env_engine() {
 // which spreads one polynomial over the whole GPU, is faster (uint64 words at
 // 2^16: 13 - 17 us for 1 - 4 polynomials against 21 us; 25 against 21 us for 8).
 constexpr uint64_t kInt8MinUnits = 8;
+// The batch queue's tensor tiles take sizes 2^17 .. 2^20 once a call holds
+// 2^20 residues: single forward transforms of BabyBear words, CUDA events
+// over 200 calls, tiles / CUDA-core engine in us: 1 x 2^20 26.4 / 33.8,
+// 4 x 2^18 23.6 / 32.7, 4 x 2^20 51.2 / 81.9; below that the CUDA-core
+// engine, which spreads a call over the whole GPU with less set-up, is as
+// fast or faster (4 x 2^17 22.5 / 22.6, 1 x 2^19 24.4 / 22.5).
+constexpr uint32_t kTilesMinLog = 17;
+constexpr uint64_t kTilesMinResidues = 1ull << 20;
 
 int auto_engine32(const Plan32& p, bool src_u64, uint64_t units) {
     if (int8_serves(p, src_u64) && units >= kInt8MinUnits) return NTTB_ENGINE_INT8;
+    if (tiles_serve(p) && p.log_n >= kTilesMinLog && (units << p.log_n) >= kTilesMinResidues) return NTTB_ENGINE_TILES;
     return NTTB_ENGINE_SCALAR;
 }
 
@@ -38,6 +48,8 @@ int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_
             return int8_transform32(p, src, dst, src_u64, n_polys, inverse, s);
         case NTTB_ENGINE_DMMA:
             return dmma_transform32(p, src, dst, src_u64, n_polys, inverse, s);
+        case NTTB_ENGINE_TILES:
+            return tiles_transform32(p, src, dst, src_u64, n_polys, inverse, s);
         default:
             return 1;
     }
@@ -46,6 +58,7 @@ int run_transform32(Plan32& p, const void* src, void* dst, bool src_u64, uint32_
 void engines_release32(Plan32* p) {
     int8_release(p);
     dmma_release(p);
+    tiles_release(p);
 }
 
 }  // namespace nttb

@@ -20,6 +20,11 @@ int auto_engine32(const Plan32& p, bool src_u64, uint64_t units);
 // Frees engine caches attached to a plan.
 void engines_release32(Plan32* p);
 
+// The batch queue's tensor tiles as a plan engine (batch.cu): 2^13 .. 2^20.
+bool tiles_serve(const Plan32& p);
+int tiles_transform32(Plan32& p, const void* src, void* dst, bool u64, uint32_t n_polys, bool inverse, cudaStream_t s);
+void tiles_release(Plan32* p);
+
 int fail(int code, const char* fmt, ...);
 
 // Byte-plane image of a 64 x 64 matrix W (mod q) as the INT8 contraction's

@@ -17,8 +17,9 @@ LIB_PATH = os.path.join(HERE, "libntt_b200_dbg.so" if os.environ.get("NTT_B200_L
 HEADER = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "ntt_b200.h")
 
 OK = 0
-ENGINE_AUTO, ENGINE_SCALAR, ENGINE_DMMA, ENGINE_INT8 = 0, 1, 2, 3
-ENGINES = {"auto": ENGINE_AUTO, "scalar": ENGINE_SCALAR, "dmma": ENGINE_DMMA, "int8": ENGINE_INT8}
+ENGINE_AUTO, ENGINE_SCALAR, ENGINE_DMMA, ENGINE_INT8, ENGINE_TILES = 0, 1, 2, 3, 4
+ENGINES = {"auto": ENGINE_AUTO, "scalar": ENGINE_SCALAR, "dmma": ENGINE_DMMA, "int8": ENGINE_INT8,
+           "tiles": ENGINE_TILES}
 NEGACYCLIC = 1
 ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_NO_MEMORY, ERR_TIMEOUT, ERR_BUDGET = 1, 2, 3, 4, 5, 6
 

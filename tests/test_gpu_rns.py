@@ -14,11 +14,14 @@ PRIMES21 = nb.generate_primes(31, 21, 8)
 
 
 def engines():
-    return ["scalar", "int8", "dmma", "auto"]
+    return ["scalar", "int8", "dmma", "tiles", "auto"]
 
 
 def serves(engine, lg):
-    """The tensor-core engines serve N = 2^16; AUTO falls back elsewhere."""
+    """The INT8 cluster and DMMA engines serve N = 2^16, the batch queue's
+    tensor tiles 2^13 .. 2^20; AUTO falls back elsewhere."""
+    if engine == "tiles":
+        return 13 <= lg <= 20
     return engine not in ("int8", "dmma") or lg == 16
 
 
@@ -38,8 +41,8 @@ def run(torch, plan, x, inverse, engine, out_of_place=False):
     return to_host(dst, np.uint32).reshape(x.shape)
 
 
-@pytest.mark.parametrize("engine,lg", [(e, lg) for e in engines() for lg in (1, 4, 6, 10, 12, 13, 16, 17)
-                                       if serves(e, lg)])
+@pytest.mark.parametrize("engine,lg", [(e, lg) for e in engines() for lg in (1, 4, 6, 10, 12, 13, 16, 17, 18, 20)
+                                       if serves(e, lg) and (lg < 18 or e in ("tiles", "auto"))])
 @pytest.mark.parametrize("negacyclic", [False, True])
 def test_rns_vs_oracle(torch_cuda, engine, negacyclic, lg):
     moduli = nb.generate_primes(31, max(17, lg + 1), 3)

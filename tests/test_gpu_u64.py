@@ -74,6 +74,61 @@ def test_auto_engine_for_uint64_batches(torch_cuda):
             assert (y[i] == O.ntt(x[i], BABYBEAR)).all()
 
 
+@pytest.mark.parametrize("lg", [13, 15, 17, 18, 19, 20])
+@pytest.mark.parametrize("batch", [1, 3])
+def test_tiles_engine_on_uint64_words(torch_cuda, lg, batch):
+    """The batch queue's tensor tiles as a plan engine (NTTB_ENGINE_TILES) on
+    the drop-in uint64-word layout, in place: pass A reads the words, pass B
+    writes them back.  Forward and inverse equal the oracle for every
+    polynomial; the high words of the results are zero."""
+    n = 1 << lg
+    x = np.stack([rand(n, BABYBEAR, 1300 + 7 * lg + i) for i in range(batch)])
+    plan = nb.Plan(n, BABYBEAR)
+    y = run_u64(torch_cuda, plan, x.reshape(-1), False, "tiles", batch).reshape(batch, n)
+    for i in range(batch):
+        assert (y[i] == O.ntt(x[i], BABYBEAR)).all(), "poly %d" % i
+    z = run_u64(torch_cuda, plan, y.reshape(-1), True, "tiles", batch).reshape(batch, n)
+    assert (z == x).all()
+    assert nb.device_errors() == 0
+
+
+def test_tiles_engine_queue_cache(torch_cuda):
+    """A plan keeps four tile queues (one per source / destination / count /
+    direction): six buffers in turn, twice over, replace queues in LRU order;
+    every call is exact."""
+    lg, n = 18, 1 << 18
+    plan = nb.Plan(n, BABYBEAR)
+    xs = [rand(n, BABYBEAR, 1400 + i) for i in range(6)]
+    ds = [to_dev(torch_cuda, x) for x in xs]
+    for rnd in range(2):
+        for i, d in enumerate(ds):
+            plan.transform(d, inverse=bool(rnd), engine="tiles")
+    torch_cuda.cuda.synchronize()
+    for x, d in zip(xs, ds):
+        assert (to_host(d, np.uint64) == x).all()
+    assert nb.device_errors() == 0
+
+
+def test_auto_engine_takes_tiles(torch_cuda):
+    """AUTO sends calls of 2^17 .. 2^20 residues per polynomial that hold at
+    least 2^20 residues to the tensor tiles (one launch of the batch queue),
+    smaller calls to the CUDA-core engine; both exact."""
+    for lg, batch, kernel in ((20, 1, "batch_queue"), (18, 4, "batch_queue"), (19, 1, "scalar_pass_col"),
+                              (17, 2, "scalar_pass_col")):
+        n = 1 << lg
+        x = np.stack([rand(n, BABYBEAR, 1500 + lg + i) for i in range(batch)])
+        plan = nb.Plan(n, BABYBEAR)
+        d = to_dev(torch_cuda, x.reshape(-1))
+        nb.profile_start()
+        plan.transform(d, batch=batch)
+        torch_cuda.cuda.synchronize()
+        ran = nb.profile_stop()
+        assert kernel in ran, (lg, batch, ran)
+        y = to_host(d, np.uint64).reshape(batch, n)
+        for i in range(batch):
+            assert (y[i] == O.ntt(x[i], BABYBEAR)).all()
+
+
 @pytest.mark.parametrize("n", [64, 256, 1024, 4096])
 def test_golden_seed42(torch_cuda, n):
     g = golden("babybear_seed42.npz")
