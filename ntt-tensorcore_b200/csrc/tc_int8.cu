@@ -95,28 +95,35 @@ constexpr uint32_t kOffImg = 4 * kTileBytes;            // DFT-64 image
 constexpr uint32_t kOffImg16 = kOffImg + kMatBytes64;   // DFT-16 images: forward, inverse
 constexpr uint32_t kOffTB1 = kOffImg16 + 2 * kMatBytes16;  // stage B level-1 twiddles: forward, inverse
 constexpr uint32_t kTB1Stride = 68;                         // words per b2 row (64 twiddles + padding)
-constexpr uint32_t kTB1Bytes = 16 * kTB1Stride * 4;         // one direction: 4352 B
-constexpr uint32_t kOffBar = kOffTB1 + 2 * kTB1Bytes;
+constexpr uint32_t kTB1Bytes = 16 * kTB1Stride * 4;         // one array of one direction: 4352 B
+constexpr uint32_t kTB1Dir = 2 * kTB1Bytes;                 // a direction's twiddles t, then their quotients t'
+constexpr uint32_t kOffBar = kOffTB1 + 2 * kTB1Dir;
 constexpr size_t kClSmem = kOffBar + 256 + 1024;
+static_assert(kClSmem <= 232448, "one CTA's dynamic shared memory (227 KB on sm_100)");
 constexpr uint32_t kPiece = 1024;            // DSMEM exchange granule
 constexpr uint32_t kBufBytes = 2 * kTileBytes;
 // per-limb device blob: DFT-16 images (8 KB), 3 DFT-64 images, twiddle tables
 constexpr uint32_t kImgSlots = 3;            // 0: stage A forward, 1: inverse (A and B), 2: stage B forward
 constexpr uint32_t kBlobImg = 2 * kMatBytes16;
 // twiddle table of one direction (words): a_st2[2048] a_ratio[1024] q qinv
-// (pad to 16 bytes) a_step[2048] b1[16][68]; the forward table, then the
+// (pad to 16 bytes) a_step[2048] b1[16][68] b1s[16][68]; the forward table, then the
 // inverse
 //   stage A:  t_A(b, d) = a_st2[2b + h] * a_ratio[b]^(d - 32h),   d in [32h, 32h + 32)
 //             (Montgomery form); a_step = (ratio^2 mod q, floor(ratio^2 * 2^32 / q))
 //             in plain form, the Shoup operands of the twiddle chains' step
 //             (every second output);
-//   stage B1: b1[b2][d2] = t_B1(b2, d2) = b_ratio[b2]^d2 itself (Montgomery form,
-//             canonical), row b2 padded to 68 words so that 16-byte loads of
-//             neighbouring rows hit distinct banks; bulk-copied into shared
-//             memory with the unit's constants, so that epilogue reads its
-//             twiddles instead of walking chains.
+//   stage B1: b1[b2][d2] = t_B1(b2, d2) = b_ratio[b2]^d2 (plain form,
+//             canonical), then b1s[b2][d2] = floor(t_B1 * 2^32 / q), the
+//             operands of a Shoup product (three single-width multiplies; a
+//             Montgomery product by a table entry takes more of the integer
+//             multiply pipe: 1.43e12 against 1.83e12 outputs/s for this
+//             epilogue's arithmetic on the whole GPU); rows b2 padded to 68
+//             words so that 16-byte loads of neighbouring rows hit distinct
+//             banks; bulk-copied into shared memory with the unit's
+//             constants, so that the epilogue reads its twiddles instead of
+//             walking chains.
 constexpr uint32_t kTabAst = 0, kTabArat = 2048, kTabQ = 3072, kTabAstep = 3076, kTabB1 = 5124;
-constexpr uint32_t kTabWords = kTabB1 + 16 * kTB1Stride;
+constexpr uint32_t kTabWords = kTabB1 + 2 * 16 * kTB1Stride;
 static_assert((kTabB1 * 4) % 16 == 0 && (kTabWords * 4) % 16 == 0, "bulk-copied table rows stay 16-byte aligned");
 constexpr uint32_t kBlobTab = kBlobImg + kImgSlots * kMatBytes64;
 constexpr uint32_t kBlobBytes = kBlobTab + 2 * kTabWords * 4;
@@ -312,7 +319,8 @@ template <class Gate>
 __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qinv, uint32_t dir, Gate gate) {
     const uint32_t mv = c.quarter * 32u + c.lane, b2 = mv & 15u, r = mv >> 4;
     // t_B1(b2, 32h + 16 part + i) from the shared-memory table
-    const uint32_t* tb = reinterpret_cast<const uint32_t*>(c.base + kOffTB1 + dir * kTB1Bytes) + b2 * kTB1Stride + 32u * c.h;
+    const uint32_t* tb = reinterpret_cast<const uint32_t*>(c.base + kOffTB1 + dir * kTB1Dir) + b2 * kTB1Stride + 32u * c.h;
+    const uint32_t* ts = tb + 16u * kTB1Stride;  // the Shoup quotients
     const uint32_t col = lane_cols(c);
     // sw64_offset(r + 8 (2h + part) + 32 i, 4 b2) = off + 512 (2h + part) + 2048 i
     const uint32_t off = r * 64u + (((b2 >> 2) ^ ((r >> 1) & 3u)) << 4) + 4u * (b2 & 3u);
@@ -324,14 +332,15 @@ __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qi
             uint32_t c0[8], c1[8], c2[8], c3[8];
             ld_planes8(col + 16u * part + 8u * sub, c0, c1, c2, c3);
 #pragma unroll
-            for (uint32_t g = 0; g < 2; g++) {  // four outputs per 16-byte twiddle load
-                const uint4 t = *reinterpret_cast<const uint4*>(tb + 16u * part + 8u * sub + 4u * g);
+            for (uint32_t g = 0; g < 2; g++) {  // four outputs per pair of 16-byte table loads
+                const uint32_t o = 16u * part + 8u * sub + 4u * g;
+                const uint4 t = *reinterpret_cast<const uint4*>(tb + o), u = *reinterpret_cast<const uint4*>(ts + o);
                 uint32_t* ys = y + 8 * sub + 4 * g;
                 const uint32_t i = 4 * g;
-                ys[0] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), t.x, q, qinv);
-                ys[1] = mont_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), t.y, q, qinv);
-                ys[2] = mont_lazy(combine_redc(c0[i + 2], c1[i + 2], c2[i + 2], c3[i + 2], q, qinv), t.z, q, qinv);
-                ys[3] = mont_lazy(combine_redc(c0[i + 3], c1[i + 3], c2[i + 3], c3[i + 3], q, qinv), t.w, q, qinv);
+                ys[0] = shoup_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), t.x, u.x, q);
+                ys[1] = shoup_lazy(combine_redc(c0[i + 1], c1[i + 1], c2[i + 1], c3[i + 1], q, qinv), t.y, u.y, q);
+                ys[2] = shoup_lazy(combine_redc(c0[i + 2], c1[i + 2], c2[i + 2], c3[i + 2], q, qinv), t.z, u.z, q);
+                ys[3] = shoup_lazy(combine_redc(c0[i + 3], c1[i + 3], c2[i + 3], c3[i + 3], q, qinv), t.w, u.w, q);
             }
         }
         if (part == 0) gate();
@@ -453,12 +462,12 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
         const uint8_t* limb_blob = args.consts + (unit % args.n_limbs) * args.const_stride;
         if (c.tid == 0) {
             const uint64_t pol = tc::l2_policy_evict_last();
-            tc::mbar_expect_tx(c.bar + kBarConst, kBlobImg + kMatBytes64 + 2 * kTB1Bytes);
+            tc::mbar_expect_tx(c.bar + kBarConst, kBlobImg + kMatBytes64 + 2 * kTB1Dir);
             tc::bulk_g2s_hint(c.base + kOffImg16, limb_blob, kBlobImg, c.bar + kBarConst, pol);
 #pragma unroll
             for (uint32_t dir = 0; dir < 2; dir++)
-                tc::bulk_g2s_hint(c.base + kOffTB1 + dir * kTB1Bytes, limb_blob + kBlobTab + (dir * kTabWords + kTabB1) * 4,
-                                  kTB1Bytes, c.bar + kBarConst, pol);
+                tc::bulk_g2s_hint(c.base + kOffTB1 + dir * kTB1Dir, limb_blob + kBlobTab + (dir * kTabWords + kTabB1) * 4,
+                                  kTB1Dir, c.bar + kBarConst, pol);
             copy_image(c, limb_blob, args.st[0].img, c.bar + kBarConst);
         }
     };
@@ -685,7 +694,11 @@ void fill_tables(uint32_t* t, uint64_t q, const uint64_t* start_a, const uint64_
         t[kTabAstep + 2 * b + 1] = (uint32_t)((r2 << 32) / q);
     }
     for (uint32_t b2 = 0; b2 < 16; b2++)
-        for (uint32_t d2 = 0; d2 < 64; d2++) t[kTabB1 + b2 * kTB1Stride + d2] = h_to_mont32(h_powmod(ratio_b[b2], d2, q), q);
+        for (uint32_t d2 = 0; d2 < 64; d2++) {
+            const uint64_t tw = h_powmod(ratio_b[b2], d2, q);
+            t[kTabB1 + b2 * kTB1Stride + d2] = (uint32_t)tw;
+            t[kTabB1 + (16 + b2) * kTB1Stride + d2] = (uint32_t)((tw << 32) / q);
+        }
 }
 
 // DFT-64 image slots: 0 stage A forward, 1 inverse (stage A and stage B
