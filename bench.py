@@ -53,7 +53,8 @@ def parse():
                          "q60: the 60-bit prime at N = 2^20, cyclic forward + inverse; aux: the helper "
                          "kernels (transposes, bit reversal, pointwise products) against the HBM roofline")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="seconds per load level (serve)")
-    ap.add_argument("--profile-case", choices=["int8", "dmma", "batch", "batch_tc", "q60", "move", "klimb"], default=None,
+    ap.add_argument("--profile-case", choices=["int8", "int8_phases", "dmma", "batch", "batch_tc", "q60", "move", "klimb"],
+                    default=None,
                     help="run one small profiling case and exit (the workloads the profiles/ captures use)")
     ap.add_argument("--no-compare", action="store_true", help="skip the per-engine comparison lines")
     ap.add_argument("--no-secondary", action="store_true",
@@ -1087,9 +1088,42 @@ def profile_case(name):
     60-bit prime, four times; move: the TMA tile kernels on 4096 x 4096
     words (transpose, in-place transpose, bit reversal), one launch each;
     klimb: the K-limb forward NTT over the BN254 field (K = 11) at 2^14,
-    three times (its field from the committed fixture)."""
+    three times (its field from the committed fixture); int8_phases: the
+    int8 case's step 100 times on the NTT_PHASE_PROFILE build
+    (NTT_B200_LIB=phase), printing where the epilogue warps spend a step."""
     import torch
     import ntt_b200 as nb
+    if name == "int8_phases":
+        qs = nb.generate_primes(31, TWO_ADICITY, N_LIMBS)
+        plan = nb.RnsPlan(LOG_N, qs, negacyclic=True)
+        x = make_batch(qs, 7)
+        d = torch.from_numpy(x.reshape(-1).view(np.int32)).cuda()
+        for _ in range(10):
+            plan.forward_inverse(d, 1, engine="int8")
+        torch.cuda.synchronize()
+        enabled, _ = nb.phase_profile(clear=True)
+        if not enabled:
+            sys.exit("int8_phases: load the NTT_PHASE_PROFILE build (NTT_B200_LIB=phase)")
+        steps = 100
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            plan.forward_inverse(d, 1, engine="int8")
+        e1.record()
+        torch.cuda.synchronize()
+        _, ph = nb.phase_profile(clear=True)
+        assert (d.cpu().numpy().view(np.uint32).reshape(x.shape) == x).all()
+        mhz = float(subprocess.run(["nvidia-smi", "--query-gpu=clocks.sm", "--format=csv,noheader,nounits", "-i", "0"],
+                                   capture_output=True, text=True).stdout.split()[0])
+        ctas = ph.pop("ctas")
+        warps = ctas * 16  # epilogue warps
+        out = {k: round(v / warps / mhz, 3) for k, v in ph.items() if not k.startswith("cta_")}
+        out.update({k: round(v / ctas / mhz, 3) for k, v in ph.items() if k.startswith("cta_")})
+        out["us_per_step_events"] = round(e0.elapsed_time(e1) / steps * 1e3, 3)
+        out["note"] = ("us per launch: epilogue-warp phases summed over the four stages (mean over warps), "
+                       "CTA lifetime and start-up per CTA; clock %d MHz" % mhz)
+        print(json.dumps(out))
+        return
     if name == "klimb":
         # BN254 (K = 11 limbs of 24 bits), Montgomery form R = 2^264.  The
         # twiddles are powers of the fixture's omega: the network does the same

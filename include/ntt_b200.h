@@ -80,6 +80,18 @@ NTTB_API int nttb_device_errors(uint32_t* flags, int clear);
  * reference's debug build is nvcc -G -g, CMakeLists.txt:10). */
 NTTB_API int nttb_bounds_errors(uint32_t* flags, int* enabled, int clear);
 
+/* Phase profile of the INT8 cluster kernel, in the NTT_PHASE_PROFILE build
+ * (libntt_b200_phase.so, `python ntt-tensorcore_b200/build.py
+ * --phase-profile`): out[0..15] receive clock() cycles summed over the
+ * epilogue warps of every launch since the last clear -- 0 waiting for the
+ * stage's MMA, 1 TMEM loads, 2 gates before staging stores, 3 part barriers
+ * and piece sends, 4 level-2 MMA, 5 end-of-stage barrier, 6 whole stages --
+ * and per CTA: 7 lifetime, 8 start-up (including the wait for the previous
+ * grid), 9 CTAs counted.  *enabled = 1 in that build; the release build
+ * has no probes (enabled 0, zeros).  Read after a device synchronize;
+ * clear != 0 resets the counters.  No reference counterpart. */
+NTTB_API int nttb_phase_profile(uint64_t* out16, int* enabled, int clear);
+
 /* ------------------------------------------------ modular parameters (host)
  * Field-for-field the reference's ModularParams
  * (include/modular_arith.cuh:11-19). */

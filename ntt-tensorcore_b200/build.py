@@ -1,11 +1,13 @@
 """Builds libntt_b200.so (in-tree) from csrc/*.cu and csrc/*.cpp with nvcc for sm_100a.
 
-Usage: python ntt-tensorcore_b200/build.py [--force] [--debug-bounds]
+Usage: python ntt-tensorcore_b200/build.py [--force] [--debug-bounds | --phase-profile]
 Objects go to ntt-tensorcore_b200/_build/, the library to
 ntt-tensorcore_b200/ntt_b200/libntt_b200.so.  Rebuilds only what changed
 (by modification time, headers included).  --debug-bounds builds the
 range-checked variant (-DNTT_DEBUG_BOUNDS, csrc/bounds.cuh) into _build_dbg/
-and ntt_b200/libntt_b200_dbg.so instead.
+and ntt_b200/libntt_b200_dbg.so instead; --phase-profile builds the INT8
+cluster kernel with its phase counters (-DNTT_PHASE_PROFILE, read by
+nttb_phase_profile) into _build_phase/ and ntt_b200/libntt_b200_phase.so.
 """
 import concurrent.futures as cf
 import glob
@@ -20,6 +22,8 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "ntt_b200", "libntt_b200.so")
 BUILD_DBG = os.path.join(HERE, "_build_dbg")
 LIB_DBG = os.path.join(HERE, "ntt_b200", "libntt_b200_dbg.so")
+BUILD_PHASE = os.path.join(HERE, "_build_phase")
+LIB_PHASE = os.path.join(HERE, "ntt_b200", "libntt_b200_phase.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -40,9 +44,13 @@ def _compile(src, obj, extra=()):
     return obj
 
 
-def build(force=False, verbose=False, debug_bounds=False):
-    build_dir, lib = (BUILD_DBG, LIB_DBG) if debug_bounds else (BUILD, LIB)
-    extra = ["-DNTT_DEBUG_BOUNDS"] if debug_bounds else []
+def build(force=False, verbose=False, debug_bounds=False, phase_profile=False):
+    if debug_bounds:
+        build_dir, lib, extra = BUILD_DBG, LIB_DBG, ["-DNTT_DEBUG_BOUNDS"]
+    elif phase_profile:
+        build_dir, lib, extra = BUILD_PHASE, LIB_PHASE, ["-DNTT_PHASE_PROFILE"]
+    else:
+        build_dir, lib, extra = BUILD, LIB, []
     os.makedirs(build_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     hdr_time = _headers()
@@ -68,4 +76,5 @@ def build(force=False, verbose=False, debug_bounds=False):
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True, debug_bounds="--debug-bounds" in sys.argv)
+    build(force="--force" in sys.argv, verbose=True, debug_bounds="--debug-bounds" in sys.argv,
+          phase_profile="--phase-profile" in sys.argv)

@@ -287,6 +287,17 @@ int nttb_bounds_errors(uint32_t* flags, int* enabled, int clear) {
     return cuda_status("bounds_errors");
 }
 
+int nttb_phase_profile(uint64_t* out16, int* enabled, int clear) {
+    if (!out16 || !enabled) return fail(NTTB_ERR_INVALID_ARG, "phase_profile: null argument");
+#ifdef NTT_PHASE_PROFILE
+    *enabled = 1;
+#else
+    *enabled = 0;
+#endif
+    int8_phase_profile(out16, clear != 0);
+    return cuda_status("phase_profile");
+}
+
 // A wide (64-bit modulus) transform: AUTO takes the INT8 engine where it
 // serves the plan (n = 2^20, cyclic) for fewer than 8 (polynomial, limb)
 // units, the CUDA-core Montgomery-64 engine otherwise.  Both spend about the

@@ -151,6 +151,8 @@ uint32_t int8_device_errors(bool clear);
 // Failed range checks of the NTT_DEBUG_BOUNDS build (bounds.cuh bits; 0 in the
 // release build), per kernel file.
 uint32_t int8_bounds_errors(bool clear);
+// The INT8 cluster kernel's phase counters (NTT_PHASE_PROFILE build; zeros otherwise).
+void int8_phase_profile(uint64_t* out16, bool clear);
 uint32_t dmma_bounds_errors(bool clear);
 uint32_t batch_bounds_errors(bool clear);
 // Forward then inverse, in place, in one persistent launch.

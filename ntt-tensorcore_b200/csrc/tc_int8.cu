@@ -78,6 +78,27 @@ __device__ uint32_t g_tc_error;
 // NTT_DEBUG_BOUNDS build: failed range checks (bounds.cuh bits)
 __device__ uint32_t g_tc_bounds;
 
+// NTT_PHASE_PROFILE build (build.py --phase-profile): clock() cycles spent
+// by the epilogue warps in each phase of a stage, summed over warps (lane 0
+// of each warp adds its own), plus per-CTA totals; read and cleared by
+// nttb_phase_profile.  The release build compiles every probe away.
+//   0 waiting for the stage's MMA   1 TMEM loads      2 gates before staging stores
+//   3 part barriers + piece sends   4 level-2 MMA     5 end-of-stage barrier
+//   6 whole stages                  7 CTA lifetime    8 CTA start-up   9 CTAs
+__device__ unsigned long long g_phase[16];
+#ifdef NTT_PHASE_PROFILE
+#define PHASE_T0 uint32_t phase_t0_ = (uint32_t)clock()
+#define PHASE_ADD(cat)                                                                       \
+    do {                                                                                     \
+        const uint32_t phase_t1_ = (uint32_t)clock();                                        \
+        if ((threadIdx.x & 31u) == 0) atomicAdd(c.phase + (cat), phase_t1_ - phase_t0_);     \
+        phase_t0_ = phase_t1_;                                                               \
+    } while (0)
+#else
+#define PHASE_T0 (void)0
+#define PHASE_ADD(cat) (void)0
+#endif
+
 namespace {
 
 using namespace tca;
@@ -183,6 +204,9 @@ struct Cl {
     uint32_t quarter, h, lane;  // TMEM sub-partition, output half, lane of this thread's warp
     uint32_t taddr;             // TMEM base (512 columns: tile w at + 256 w)
     uint64_t* bar;
+#ifdef NTT_PHASE_PROFILE
+    uint32_t* phase;            // shared-memory phase counters
+#endif
 };
 // Barriers (shared memory, after the images):
 //   [0, 1]  MMA of tile 0 / 1 (N = 256), issued in that order (N = 128
@@ -289,7 +313,9 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
 #pragma unroll
         for (uint32_t sub = 0; sub < 2; sub++) {
             uint32_t c0[8], c1[8], c2[8], c3[8];
+            PHASE_T0;
             ld_planes8(col + 16u * part + 8u * sub, c0, c1, c2, c3);
+            PHASE_ADD(1);
 #pragma unroll
             for (uint32_t i = 0; i < 8; i += 2) {
                 y[8 * sub + i] = mont_lazy(combine_redc(c0[i], c1[i], c2[i], c3[i], q, qinv), tw_e, q, qinv);
@@ -299,7 +325,11 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
                 tw_o = tw_norm<Lazy>(shoup_lazy(tw_o, step.x, step.y, q), q);
             }
         }
-        if (part == 0) gate();
+        if (part == 0) {
+            PHASE_T0;
+            gate();
+            PHASE_ADD(2);
+        }
         // d = 32h + 16 part + i: P = 2h + part, w' = i / 8, j = i % 8
         const uint32_t o0 = inpiece + (2u * c.h + part) * kPiece;
         uint8_t* o = c.base + kOffBuf0 + o0;
@@ -308,7 +338,9 @@ __device__ __forceinline__ void epilogue_a(const Cl& c, uint32_t q, uint32_t qin
             for (uint32_t i = 0; i < 16; i++)
                 *reinterpret_cast<uint32_t*>(o + (i >> 3) * kTileBytes + ((i >> 2) & 1u) * 16384u +
                                              4u * (i & 3u) * kPiece) = y[i];
+        PHASE_T0;
         part_done(part);
+        PHASE_ADD(3);
     }
 }
 
@@ -330,7 +362,9 @@ __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qi
 #pragma unroll
         for (uint32_t sub = 0; sub < 2; sub++) {
             uint32_t c0[8], c1[8], c2[8], c3[8];
+            PHASE_T0;
             ld_planes8(col + 16u * part + 8u * sub, c0, c1, c2, c3);
+            PHASE_ADD(1);
 #pragma unroll
             for (uint32_t g = 0; g < 2; g++) {  // four outputs per pair of 16-byte table loads
                 const uint32_t o = 16u * part + 8u * sub + 4u * g;
@@ -343,7 +377,11 @@ __device__ __forceinline__ void epilogue_b1(const Cl& c, uint32_t q, uint32_t qi
                 ys[3] = shoup_lazy(combine_redc(c0[i + 3], c1[i + 3], c2[i + 3], c3[i + 3], q, qinv), t.w, u.w, q);
             }
         }
-        if (part == 0) gate();
+        if (part == 0) {
+            PHASE_T0;
+            gate();
+            PHASE_ADD(2);
+        }
         const uint32_t o0 = off + 512u * (2u * c.h + part);
         uint8_t* o = c.base + kOffBuf1 + c.w * kTileBytes + o0;
         if (NTTB_CHECK(g_tc_bounds, kBoundsShared, o0 + 2048u * 15u + 4u <= kTileBytes))
@@ -373,11 +411,13 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
         for (uint32_t sub = 0; sub < 2; sub++) {
             const uint32_t col = base + t2 * 64u + 8u * sub;
             uint32_t c0[8], c1[8], c2[8], c3[8];
+            PHASE_T0;
             tc::ld_32x32b_x8(col + 0, c0);
             tc::ld_32x32b_x8(col + 16, c1);
             tc::ld_32x32b_x8(col + 32, c2);
             tc::ld_32x32b_x8(col + 48, c3);
             tc::ld_wait();
+            PHASE_ADD(1);
 #pragma unroll
             for (uint32_t k = 0; k < 8; k++) y[8 * sub + k] = combine_redc(c0[k], c1[k], c2[k], c3[k], q, qinv);
         }
@@ -398,7 +438,11 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
                 for (uint32_t k = 0; k < 16; k++) __stcs(g + 4096u * k, canon(y[k], q));
             }
         } else {
-            if (part == 0) gate();
+            if (part == 0) {
+                PHASE_T0;
+                gate();
+                PHASE_ADD(2);
+            }
             const uint32_t g = 2u * (c.quarter & 1u) + c.w;
             const uint32_t o0 = (c.quarter >> 1) * kTileBytes + t2 * 8u * kPiece + 2u * g * kPiece + r * 128u +
                                 4u * (c.lane >> 3);
@@ -407,7 +451,9 @@ __device__ __forceinline__ void epilogue_b2(const Cl& c, uint32_t q, uint32_t qi
 #pragma unroll
                 for (uint32_t k = 0; k < 16; k++)
                     *reinterpret_cast<uint32_t*>(o + (k >> 3) * kPiece + (((k & 7u) ^ r) << 4)) = y[k];
+            PHASE_T0;
             part_done(part);
+            PHASE_ADD(3);
         }
     }
 }
@@ -444,6 +490,12 @@ template <bool Lazy>
 __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_constant__ ClArgs args) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     Cl c;
+#ifdef NTT_PHASE_PROFILE
+    __shared__ uint32_t s_phase[16];
+    const uint32_t phase_k0_ = (uint32_t)clock();
+    if (threadIdx.x < 16) s_phase[threadIdx.x] = 0;
+    c.phase = s_phase;
+#endif
     c.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     c.rank = tc::cluster_rank();
     c.tid = threadIdx.x;
@@ -497,6 +549,9 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
     tc::cluster_sync();  // every CTA's barriers exist and are armed before any remote traffic
     tc::fence_after_sync();
     c.taddr = *slot;
+#ifdef NTT_PHASE_PROFILE
+    if (threadIdx.x == 0) atomicAdd(c.phase + 8, (uint32_t)clock() - phase_k0_);
+#endif
     uint32_t ph_mma = 0, ph_mma2 = 0, ph_ld = 0, ph_img = 0, ph_in0 = 0, ph_in1 = 0, ph_unit = 0;
     uint32_t iter = 0;
     for (uint32_t unit = tc::cluster_id(); unit < args.units; unit += tc::cluster_count(), iter++) {
@@ -516,6 +571,9 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
         __syncthreads();
         bool img_pending = false;  // issuing thread: a next-stage image copy is in flight
         for (uint32_t s = 0; s < args.n_stages; s++) {
+#ifdef NTT_PHASE_PROFILE
+            const uint32_t phase_stage_ = (uint32_t)clock();
+#endif
             const ClStage& S = args.st[s];
             const bool last = s + 1 == args.n_stages;
             const bool next_img = !last && args.st[s + 1].img != S.img;
@@ -568,7 +626,11 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                 __syncthreads();
                 continue;
             }
-            wait_parity(c.bar + kBarMma + c.w, ph_mma);
+            {
+                PHASE_T0;
+                wait_parity(c.bar + kBarMma + c.w, ph_mma);
+                PHASE_ADD(0);
+            }
             tc::fence_after_sync();
             // before the first stores: the MMAs reading the overwritten operand
             // are done (stage A stages into both tiles' operands: every MMA;
@@ -592,6 +654,7 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
             } else {
                 epilogue_b1(c, q, qinv, S.dir, mma_gate);
                 ph_mma ^= 1u;
+                PHASE_T0;
                 tc::fence_proxy_async_smem();
                 tc::fence_before_sync();
                 asm volatile("bar.sync %0, %1;" ::"r"(1u + c.w), "r"(256u) : "memory");
@@ -610,6 +673,7 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                 }
                 __syncwarp();
                 wait_parity(c.bar + kBarMma2 + c.w, ph_mma2);
+                PHASE_ADD(4);
                 tc::fence_after_sync();
                 // staging overwrites both tiles' level-2 operands
                 void* gout = nullptr;
@@ -620,9 +684,14 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
                             [&]() { wait_parity(c.bar + kBarMma2 + (c.w ^ 1u), ph_mma2); }, part_done);
                 ph_mma2 ^= 1u;
             }
+            PHASE_T0;
             tc::fence_proxy_async_smem();
             tc::fence_before_sync();
             __syncthreads();
+            PHASE_ADD(5);
+#ifdef NTT_PHASE_PROFILE
+            if ((threadIdx.x & 31u) == 0) atomicAdd(c.phase + 6, (uint32_t)clock() - phase_stage_);
+#endif
             if (last && c.tid == 0) {
                 // this CTA reads its buffers no more in this unit: re-arm the
                 // inboxes for the next one, then report done to every CTA
@@ -637,6 +706,14 @@ __global__ void __launch_bounds__(kClThreads, 1) int8_cluster_n16(const __grid_c
     tc::fence_before_sync();
     __syncthreads();
     if (c.tid < 32) tc::tmem_dealloc(c.taddr, 512);
+#ifdef NTT_PHASE_PROFILE
+    if (threadIdx.x == 0) {
+        atomicAdd(c.phase + 7, (uint32_t)clock() - phase_k0_);
+        atomicAdd(c.phase + 9, 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) atomicAdd(&g_phase[threadIdx.x], (unsigned long long)c.phase[threadIdx.x]);
+#endif
 }
 
 // ---- host: tables and byte-plane images ------------------------------------------------
@@ -904,6 +981,16 @@ void int8_release(Plan32* p) {
     if (c->d_blob) cudaFree(c->d_blob);
     delete c;
     p->engine_data[1] = nullptr;
+}
+
+void int8_phase_profile(uint64_t* out16, bool clear) {
+    unsigned long long v[16] = {};
+    cudaMemcpyFromSymbol(v, g_phase, sizeof v);
+    for (int i = 0; i < 16; i++) out16[i] = v[i];
+    if (clear) {
+        const unsigned long long z[16] = {};
+        cudaMemcpyToSymbol(g_phase, z, sizeof z);
+    }
 }
 
 uint32_t int8_bounds_errors(bool clear) {

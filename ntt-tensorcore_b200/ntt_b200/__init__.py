@@ -12,8 +12,10 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# NTT_B200_LIB=dbg selects the NTT_DEBUG_BOUNDS build (range-checked kernels)
-LIB_PATH = os.path.join(HERE, "libntt_b200_dbg.so" if os.environ.get("NTT_B200_LIB") == "dbg" else "libntt_b200.so")
+# NTT_B200_LIB=dbg selects the NTT_DEBUG_BOUNDS build (range-checked kernels),
+# NTT_B200_LIB=phase the NTT_PHASE_PROFILE build (the INT8 kernel's phase counters)
+LIB_PATH = os.path.join(HERE, {"dbg": "libntt_b200_dbg.so", "phase": "libntt_b200_phase.so"}.get(
+    os.environ.get("NTT_B200_LIB", ""), "libntt_b200.so"))
 HEADER = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "ntt_b200.h")
 
 OK = 0
@@ -147,6 +149,7 @@ def lib():
                                    ctypes.POINTER(BatchConfig)]),
         "nttb_device_errors": (_int, [ctypes.POINTER(_u32), _int]),
         "nttb_bounds_errors": (_int, [ctypes.POINTER(_u32), ctypes.POINTER(_int), _int]),
+        "nttb_phase_profile": (_int, [ctypes.POINTER(_u64), ctypes.POINTER(_int), _int]),
         "nttb_launch_count": (_int, [ctypes.POINTER(_u64)]),
         "nttb_profile_start": (_int, []),
         "nttb_profile_stop": (_int, [ctypes.POINTER(_u32)]),
@@ -409,6 +412,18 @@ def bounds_errors(clear=True):
     f, e = _u32(), _int()
     _check(lib().nttb_bounds_errors(ctypes.byref(f), ctypes.byref(e), int(clear)))
     return bool(e.value), int(f.value)
+
+
+PHASES = ["mma_wait", "tmem_load", "gate", "part_sync_send", "level2_mma", "stage_end_sync", "stages",
+          "cta_lifetime", "cta_startup", "ctas"]
+
+
+def phase_profile(clear=True):
+    """(enabled, {phase: cycles}) of the INT8 cluster kernel's phase counters
+    (nttb_phase_profile; the NTT_PHASE_PROFILE build, NTT_B200_LIB=phase)."""
+    v, e = (_u64 * 16)(), _int()
+    _check(lib().nttb_phase_profile(v, ctypes.byref(e), int(clear)))
+    return bool(e.value), {name: int(v[i]) for i, name in enumerate(PHASES)}
 
 
 def profile_start():

@@ -38,6 +38,19 @@ def test_debug_bounds_library_exports_every_header_symbol():
     assert nb.lib().nttb_bounds_errors(ctypes.byref(f), ctypes.byref(e), 0) == 0 and e.value == 0
 
 
+def test_phase_profile_library_exports_every_header_symbol():
+    """The NTT_PHASE_PROFILE build exports the same C ABI; null arguments are
+    refused in both builds without touching a device."""
+    ph = os.path.join(os.path.dirname(nb.LIB_PATH), "libntt_b200_phase.so")
+    assert os.path.exists(ph), "run `python ntt-tensorcore_b200/build.py --phase-profile`"
+    P = ctypes.CDLL(ph)
+    missing = [s for s in nb.header_symbols() if not hasattr(P, s)]
+    assert not missing, missing
+    P.nttb_phase_profile.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    assert P.nttb_phase_profile(None, None, 0) == 1
+    assert nb.lib().nttb_phase_profile(None, None, 0) == 1
+
+
 def test_library_exports_dropin_cpp_api():
     out = subprocess.run(["nm", "-DC", "--defined-only", nb.LIB_PATH], capture_output=True, text=True).stdout
     for name in ["ntt::ntt_init", "ntt::ntt_cleanup", "ntt::ntt_forward_basic", "ntt::ntt_inverse_basic",
