@@ -43,7 +43,7 @@ enum {
  * the INT8 tensor-core kernel at N = 2^16 from 8 (polynomial, limb) units
  * on; the batch queue's tensor tiles at N = 2^17 .. 2^20 once a call holds
  * 2^20 residues; the CUDA-core engine otherwise.  The tiles engine keeps up
- * to four prepared queues per plan (one per source, destination, count,
+ * to eight prepared queues per plan (one per source, destination, count,
  * direction), each with its own workspace ring of up to 16 x N words. */
 enum {
     NTTB_ENGINE_AUTO = 0,

@@ -1584,7 +1584,7 @@ uint32_t batch_device_errors(bool clear) {
 // least recently used one replaced; each owns its workspace ring (up to 16
 // slots of 2^L words).  Calls that share a plan are ordered on one stream.
 namespace {
-constexpr size_t kTileQueues = 4;
+constexpr size_t kTileQueues = 8;  // e.g. three staging buffers x two directions of a host stream
 struct TileEntry {
     const void* src;
     void* dst;

@@ -54,6 +54,30 @@ def test_stream_host_engines_and_small_batches(torch_cuda, lg, engine):
         assert (h_out.numpy().view(np.uint32).reshape(x.shape).astype(np.uint64) == want).all(), n_batches
 
 
+@pytest.mark.parametrize("mode", ["forward", "forward_inverse"])
+def test_stream_host_on_tensor_tiles(torch_cuda, mode):
+    """2^20 residues per batch route AUTO to the batch queue's tensor tiles:
+    each of the three staging buffers gets its own prepared queue, and five
+    batches in a row still give the oracle's transforms and round trips."""
+    torch = torch_cuda
+    rng = np.random.default_rng(73)
+    qs = nb.generate_primes(31, 21, 2)
+    plan = nb.RnsPlan(19, qs, negacyclic=True)  # 1 poly x 2 limbs x 2^19 = 2^20 residues
+    x, h_in = host_batches(torch, rng, qs, 19, 1, 5)
+    h_out = torch.empty_like(h_in).pin_memory()
+    nb.profile_start()
+    plan.stream_host(h_in, h_out, 1, 5, mode=mode)
+    torch.cuda.synchronize()
+    assert "batch_queue" in nb.profile_stop()
+    got = h_out.numpy().view(np.uint32).reshape(x.shape)
+    if mode == "forward_inverse":
+        assert (got == x).all()
+    else:
+        want = O.rns(x.astype(np.uint64), qs, negacyclic=True)
+        assert (got.astype(np.uint64) == want).all()
+    assert nb.device_errors() == 0
+
+
 def test_stream_host_rejects(torch_cuda):
     qs = nb.generate_primes(31, 17, 1)
     plan = nb.RnsPlan(12, qs)

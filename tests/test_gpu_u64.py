@@ -93,12 +93,12 @@ def test_tiles_engine_on_uint64_words(torch_cuda, lg, batch):
 
 
 def test_tiles_engine_queue_cache(torch_cuda):
-    """A plan keeps four tile queues (one per source / destination / count /
-    direction): six buffers in turn, twice over, replace queues in LRU order;
+    """A plan keeps eight tile queues (one per source / destination / count /
+    direction): ten buffers in turn, twice over, replace queues in LRU order;
     every call is exact."""
     lg, n = 18, 1 << 18
     plan = nb.Plan(n, BABYBEAR)
-    xs = [rand(n, BABYBEAR, 1400 + i) for i in range(6)]
+    xs = [rand(n, BABYBEAR, 1400 + i) for i in range(10)]
     ds = [to_dev(torch_cuda, x) for x in xs]
     for rnd in range(2):
         for i, d in enumerate(ds):
