@@ -204,29 +204,30 @@ namespace nttb {
 // copies split in two chunks on two copy streams per direction, so that the
 // host -> device copy of one batch, the transform of the previous one and the
 // device -> host copy of the one before overlap.  Events order every reuse.
+constexpr int kHsBufs = 3, kHsChunks = 2;  // device buffers in rotation; copy chunks (and streams) per direction
 struct HostStream {
     size_t words = 0;  // capacity of each buffer
-    uint32_t* dbuf[3] = {};
-    cudaStream_t in[2] = {}, out[2] = {};
-    cudaEvent_t start = nullptr, ev_in[3][2] = {}, ev_c[3] = {}, done[3][2] = {};
-    bool used[3] = {};
+    uint32_t* dbuf[kHsBufs] = {};
+    cudaStream_t in[kHsChunks] = {}, out[kHsChunks] = {};
+    cudaEvent_t start = nullptr, ev_in[kHsBufs][kHsChunks] = {}, ev_c[kHsBufs] = {}, done[kHsBufs][kHsChunks] = {};
+    bool used[kHsBufs] = {};
     uint32_t next = 0;  // buffer of the next batch: the rotation continues across calls
 };
 void host_stream_free(HostStream* h) {
     if (!h) return;
-    for (int c = 0; c < 2; c++) {
+    for (int c = 0; c < kHsChunks; c++) {
         if (h->in[c]) cudaStreamSynchronize(h->in[c]);
         if (h->out[c]) cudaStreamSynchronize(h->out[c]);
     }
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < kHsBufs; k++) {
         if (h->dbuf[k]) cudaFree(h->dbuf[k]);
         if (h->ev_c[k]) cudaEventDestroy(h->ev_c[k]);
-        for (int c = 0; c < 2; c++) {
+        for (int c = 0; c < kHsChunks; c++) {
             if (h->ev_in[k][c]) cudaEventDestroy(h->ev_in[k][c]);
             if (h->done[k][c]) cudaEventDestroy(h->done[k][c]);
         }
     }
-    for (int c = 0; c < 2; c++) {
+    for (int c = 0; c < kHsChunks; c++) {
         if (h->in[c]) cudaStreamDestroy(h->in[c]);
         if (h->out[c]) cudaStreamDestroy(h->out[c]);
     }
@@ -659,15 +660,15 @@ int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_ds
         nttb::host_stream_free(H);
         H = new nttb::HostStream();
         bool ok = true;
-        for (int k = 0; k < 3 && ok; k++) {
+        for (int k = 0; k < nttb::kHsBufs && ok; k++) {
             ok = cudaMalloc(&H->dbuf[k], bw * 4) == cudaSuccess;
             ok = ok && cudaEventCreateWithFlags(&H->ev_c[k], cudaEventDisableTiming) == cudaSuccess;
-            for (int c = 0; c < 2 && ok; c++) {
+            for (int c = 0; c < nttb::kHsChunks && ok; c++) {
                 ok = cudaEventCreateWithFlags(&H->ev_in[k][c], cudaEventDisableTiming) == cudaSuccess;
                 ok = ok && cudaEventCreateWithFlags(&H->done[k][c], cudaEventDisableTiming) == cudaSuccess;
             }
         }
-        for (int c = 0; c < 2 && ok; c++) {
+        for (int c = 0; c < nttb::kHsChunks && ok; c++) {
             ok = cudaStreamCreateWithFlags(&H->in[c], cudaStreamNonBlocking) == cudaSuccess;
             ok = ok && cudaStreamCreateWithFlags(&H->out[c], cudaStreamNonBlocking) == cudaSuccess;
         }
@@ -681,15 +682,21 @@ int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_ds
     }
     // everything after the caller's earlier work on `stream`
     cudaEventRecord(H->start, s);
-    for (int c = 0; c < 2; c++) {
+    for (int c = 0; c < nttb::kHsChunks; c++) {
         cudaStreamWaitEvent(H->in[c], H->start, 0);
         cudaStreamWaitEvent(H->out[c], H->start, 0);
     }
-    const size_t half = (bw / 2 + 63) & ~(size_t)63;  // chunk of a batch, 256-byte aligned
+    // chunk c of a batch: words [c chunk, min(bw, (c + 1) chunk)), 256-byte aligned
+    const size_t chunk = (bw / nttb::kHsChunks + 63) & ~(size_t)63;
+    auto span = [&](int c, size_t* off) {
+        *off = (size_t)c * chunk;
+        return *off < bw ? std::min(chunk, bw - *off) : (size_t)0;
+    };
     for (uint32_t i = 0; i < n_batches; i++) {
-        const int k = (int)(H->next++ % 3);
-        for (int c = 0; c < 2; c++) {
-            const size_t off = c ? half : 0, len = c ? (bw > half ? bw - half : 0) : std::min(half, bw);
+        const int k = (int)(H->next++ % nttb::kHsBufs);
+        for (int c = 0; c < nttb::kHsChunks; c++) {
+            size_t off;
+            const size_t len = span(c, &off);
             if (H->used[k]) cudaStreamWaitEvent(H->in[c], H->done[k][c], 0);
             if (len) cudaMemcpyAsync(H->dbuf[k] + off, h_src + i * bw + off, len * 4, cudaMemcpyHostToDevice, H->in[c]);
             cudaEventRecord(H->ev_in[k][c], H->in[c]);
@@ -706,8 +713,9 @@ int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_ds
         }
         if (rc) return engine_status(rc, "rns_stream_host");
         cudaEventRecord(H->ev_c[k], s);
-        for (int c = 0; c < 2; c++) {
-            const size_t off = c ? half : 0, len = c ? (bw > half ? bw - half : 0) : std::min(half, bw);
+        for (int c = 0; c < nttb::kHsChunks; c++) {
+            size_t off;
+            const size_t len = span(c, &off);
             cudaStreamWaitEvent(H->out[c], H->ev_c[k], 0);
             if (len) cudaMemcpyAsync(h_dst + i * bw + off, H->dbuf[k] + off, len * 4, cudaMemcpyDeviceToHost, H->out[c]);
             cudaEventRecord(H->done[k][c], H->out[c]);
@@ -715,9 +723,9 @@ int nttb_rns_stream_host(nttb_rns_plan* P, const uint32_t* h_src, uint32_t* h_ds
         H->used[k] = true;
     }
     // the caller's stream completes after the last copy back
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k < nttb::kHsBufs; k++)
         if (H->used[k])
-            for (int c = 0; c < 2; c++) cudaStreamWaitEvent(s, H->done[k][c], 0);
+            for (int c = 0; c < nttb::kHsChunks; c++) cudaStreamWaitEvent(s, H->done[k][c], 0);
     return cuda_status("rns_stream_host");
 }
 
