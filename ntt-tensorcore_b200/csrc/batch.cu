@@ -1595,6 +1595,7 @@ struct TileEntry {
 };
 struct TileCache {
     nttb_batch_plan* plan = nullptr;
+    std::mutex mu;  // guards entries and clock (host threads sharing a plan)
     std::vector<TileEntry> entries;
     uint64_t clock = 0;
 };
@@ -1621,6 +1622,7 @@ int tiles_transform32(Plan32& p, const void* src, void* dst, bool u64, uint32_t 
     if (!tiles_serve(p)) return 1;
     TileCache* c = tile_cache(p);
     if (!c) return 2;
+    std::lock_guard<std::mutex> lock(c->mu);
     TileEntry* e = nullptr;
     for (TileEntry& t : c->entries)
         if (t.src == src && t.dst == dst && t.n_polys == n_polys && t.inverse == inverse && t.u64 == u64) e = &t;
@@ -1647,7 +1649,7 @@ int tiles_transform32(Plan32& p, const void* src, void* dst, bool u64, uint32_t 
         if (c->entries.size() >= kTileQueues) {
             auto lru = std::min_element(c->entries.begin(), c->entries.end(),
                                         [](const TileEntry& x, const TileEntry& y) { return x.used < y.used; });
-            cudaStreamSynchronize(s);  // the evicted queue may still run on this stream
+            cudaDeviceSynchronize();  // the evicted queue may still run, on whichever stream it was given
             free_batch(lru->b);
             c->entries.erase(lru);
         }
