@@ -152,6 +152,18 @@ def test_batch_rejects_bad_jobs(torch_cuda):
         plan.batch([(d, 10, 1, 0, False, True)])  # negacyclic job, cyclic plan
     with pytest.raises(nb.NTTError):
         plan.batch([(d, 10, 1, 0, False, False)], {"tile_elems": 2048})
+    # flag bits other than inverse / negacyclic / product are refused at the C ABI
+    import ctypes
+    arr = (nb.BatchJob * 1)()
+    arr[0] = nb.BatchJob(d.data_ptr(), 10, 1, 0, 1 << 30, None)
+    h = ctypes.c_void_p()
+    assert nb.lib().nttb_batch_create(plan._h, arr, 1, None, ctypes.byref(h)) == nb.ERR_INVALID_ARG
+    # an empty job list is a batch that launches nothing
+    b = plan.batch([])
+    b.launch()
+    torch_cuda.cuda.synchronize()
+    b.close()
+    assert nb.device_errors() == 0
 
 
 def expect_product(a, b, moduli, nega):
