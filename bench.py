@@ -503,6 +503,9 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         ms2 = reduce_over_ranks(e0.elapsed_time(e1), world)
         barrier()
+        for i in range(min(pool_n, 4)):  # the concurrent round trips left every buffer intact
+            got = pool[i].cpu().numpy().view(np.uint32)
+            assert (got == host[i % 4].reshape(-1)).all(), "two-stream round trip mismatch in buffer %d" % i
         two_streams = {"value": world * coeffs_per_step * args.steps / (ms2 / 1e3), "unit": UNIT,
                        "ms_per_step": ms2 / args.steps,
                        "note": "steps alternate over two streams (each on its own batch); information only"}

@@ -203,3 +203,23 @@ def test_pointwise_mul_rows_and_alignment(torch_cuda, lg, polys, offset):
     q = np.array(moduli, dtype=np.uint64)[None, :, None]
     want = (a.astype(np.uint64) * b.astype(np.uint64)) % q
     assert (got == want).all()
+
+
+def test_int8_plan_on_two_streams(torch_cuda):
+    """One plan, launches alternating over two streams on independent
+    batches (the INT8 path keeps no per-plan workspace, so they may run at
+    the same time): every forward equals the oracle."""
+    torch = torch_cuda
+    qs = PRIMES17[:8]
+    plan = nb.RnsPlan(16, qs, negacyclic=True)
+    xs = [rand_batch(1, qs, 1 << 16, 900 + i) for i in range(6)]
+    ds = [to_dev(torch, x.reshape(-1)) for x in xs]
+    outs = [torch.empty_like(d) for d in ds]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for i in range(6):
+        plan.transform(outs[i], ds[i], 1, engine="int8", stream=streams[i & 1])
+    torch.cuda.synchronize()
+    for i in range(6):
+        want = O.rns(xs[i].astype(np.uint64), qs, negacyclic=True)
+        assert (to_host(outs[i], np.uint32).reshape(xs[i].shape).astype(np.uint64) == want).all(), i
+    assert nb.device_errors() == 0
